@@ -1,0 +1,385 @@
+"""Benchmark: radix-scale PK-FK hash join + aggregation on one B200.
+
+Workload (the configuration the headline metric is quoted on): build R =
+2^27 (int64 key, int64 payload) tuples with unique keys (a seeded
+permutation of 1..2^27, payload = key * 7); probe S = 2^30 (int64 fk,
+int64 payload) tuples, fk ~ Zipf(theta) over R's keys (theta = 0: uniform),
+payload ~ U[0, 2^20).  Output: match count and the wrapped int64 checksum
+sum(R.payload + S.payload) over the joined pairs.  A step = build the table
++ probe with the fused count/sum sink.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--theta T] [--impl pyg|reference]
+
+Prints one JSON line (rank 0).  `value` is device-resident throughput
+(inputs already in HBM); `e2e` goes through the same C-ABI calls with host
+buffers (host->device copies inside the timed region); `cpu_baseline` is
+the reference's own CPU engine on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "pythia-core_b200"))
+
+N_BUILD = 1 << 27
+N_PROBE = 1 << 30
+VMAX = 1 << 20
+SEED_KEYS, SEED_PROBE = 12345, 67890
+METRIC = "join+agg tuples/sec (R 2^27 PK, S 2^30 FK, hash join + count + checksum, bit-exact)"
+UNIT = "tuples/s"
+# Bounded CPU sample: 1/16 of both relations, same key distribution.
+CPU_SAMPLE_SHIFT = 4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--theta", type=float, default=0.0)
+    ap.add_argument("--impl", default="pyg", choices=["pyg", "reference"])
+    ap.add_argument("--load-factor", type=float, default=0.5)
+    ap.add_argument("--scale-shift", type=int, default=0, help="shrink both relations by 2^s (debug only)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- helpers
+
+class Clocks:
+    """Samples nvidia-smi clocks / throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                r = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                    "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if r.returncode == 0 and r.stdout.strip():
+                    self.samples.append([x.strip() for x in r.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[2 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def zipf_host(rng, n, nkeys, theta):
+    """Ranks in [0, nkeys) with P(r) ~ (r+1)^-theta (uniform at theta 0)."""
+    if theta == 0:
+        return rng.integers(0, nkeys, n)
+    w = np.arange(1, nkeys + 1, dtype=np.float64) ** (-theta)
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    return np.minimum(np.searchsorted(cdf, rng.random(n), side="right"), nkeys - 1)
+
+
+def cpu_sample(theta, shift=CPU_SAMPLE_SHIFT, seed=7):
+    """Host-generated sample with the bench's shapes scaled by 2^-shift."""
+    rng = np.random.default_rng(seed)
+    nR, nS = N_BUILD >> shift, N_PROBE >> shift
+    perm = rng.permutation(nR).astype(np.int64) + 1
+    R = np.empty((nR, 2), dtype=np.int64)
+    R[:, 0] = perm
+    R[:, 1] = perm * 7
+    S = np.empty((nS, 2), dtype=np.int64)
+    S[:, 0] = perm[zipf_host(rng, nS, nR, theta)]
+    S[:, 1] = rng.integers(0, VMAX, nS)
+    return R, S
+
+
+def run_reference_cpu(theta, steps, shift=CPU_SAMPLE_SHIFT):
+    """Times the reference engine (oracle/_ref/executequery) on the bounded
+    sample with all host cores; falls back to the C oracle port."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refrun
+    R, S = cpu_sample(theta, shift)
+    n_tuples = R.shape[0] + S.shape[0]
+    cores = os.cpu_count() or 1
+    sample = f"R=2^{27 - shift}, S=2^{30 - shift} (1/{1 << shift} of each relation), theta={theta}"
+    if refrun.available():
+        T = min(cores, 127)
+        times = []
+        with tempfile.TemporaryDirectory(dir=os.environ.get("PYG_TMP")) as d:
+            dt = np.dtype([("c0", np.int64), ("c1", np.int64)])
+            rf = refrun.write_rel(d, "R", R.view(dt).reshape(-1), T)
+            sf = refrun.write_rel(d, "S", S.view(dt).reshape(-1), T)
+            plan = refrun.plan_join_sum(T, rf, [2, 2], sf, [2, 2], [(0, 1), (1, 1)], 1, R.shape[0])
+            for _ in range(steps):
+                _, rt, _ = refrun.run(d, plan, timeout=900)
+                times.append(rt)
+        return {"kind": "reference", "cores": T, "sample": sample + f", executequery ResponseTimeInSec, {T} threads",
+                "times": times, "tuples": n_tuples}
+    import oracle as O
+    dt = O.dtype_of([2, 2])
+    Rs, Ss = R.view(dt).reshape(-1), S.view(dt).reshape(-1)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        O.hashjoin_agg(Rs, [2, 2], [0], Ss, [2, 2], [0], [(0, 1), (1, 1)], buckets=R.shape[0])
+        times.append(time.perf_counter() - t0)
+    return {"kind": "port", "cores": 1, "sample": sample + ", C oracle single thread", "times": times,
+            "tuples": n_tuples}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+# ------------------------------------------------------------ reference arm
+
+def main_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    steps = max(1, args.steps)
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        run_reference_cpu(args.theta, 1)
+    r = run_reference_cpu(args.theta, steps)
+    tot = sum(r["times"])
+    value = r["tuples"] * len(r["times"]) / tot
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * tot / len(r["times"]), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded, host-generated)",
+            "impl": "reference",
+            "config": {"workload": "hash join + count + checksum, R 2^27 PK / S 2^30 FK (CPU runs a 1/16 sample)",
+                       "theta": args.theta},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                             "sample": r["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def main_gpu(args):
+    import torch
+    import pyg
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    # One dedicated stream shared by torch and the library: the kernels and
+    # the timing events are on the same stream.
+    torch.cuda.set_stream(torch.cuda.Stream(local))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    nR, nS = N_BUILD >> args.scale_shift, N_PROBE >> args.scale_shift
+    ctx = pyg.Ctx(local)
+    stream = torch.cuda.current_stream(local)
+
+    # Each rank joins its own (R, S) pair: the per-GPU work is fixed (weak
+    # scaling); there is no data exchange between ranks.
+    R = torch.empty(nR * 2, dtype=torch.int64, device="cuda")
+    S = torch.empty(nS * 2, dtype=torch.int64, device="cuda")
+    ctx.gen_pk(R, nR, 7, SEED_KEYS)
+    ctx.gen_fk(S, nS, nR, args.theta, SEED_KEYS, VMAX, SEED_PROBE + rank)
+    torch.cuda.synchronize()
+    Rr = pyg.Rel(R, nR, [pyg.INT64, pyg.INT64])
+    Sr = pyg.Rel(S, nS, [pyg.INT64, pyg.INT64])
+    proj = [(0, 1), (1, 1)]
+
+    def step(rrel, srel, evs=None):
+        if evs:
+            evs[0].record(stream)
+        ht = ctx.hashjoin_build(rrel, [0], [1], pyg.HT_AGGREGATE, args.load_factor)
+        if evs:
+            evs[1].record(stream)
+        cnt, sums = ctx.hashjoin_probe_agg(ht, srel, [0], proj)
+        if evs:
+            evs[2].record(stream)
+        ht.free()
+        return cnt, (sums[0] + sums[1]) & 0xFFFFFFFFFFFFFFFF
+
+    # Size-independent check of the result (every fk matches exactly once;
+    # R.payload = 7 * key): count == |S| and checksum == sum(7 fk + val).
+    cnt, chk = step(Rr, Sr)
+    Sv = S.view(nS, 2)
+    expect = int((Sv[:, 0] * 7 + Sv[:, 1]).sum().item()) & 0xFFFFFFFFFFFFFFFF
+    if cnt != nS or chk != expect:
+        raise SystemExit(f"result mismatch: count {cnt} vs {nS}, checksum {chk} vs {expect}")
+
+    for _ in range(args.warmup):
+        step(Rr, Sr)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    launches0 = ctx.launches()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        t_start.record(stream)
+        for k in range(args.steps):
+            step(Rr, Sr, evs[k])
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    launches = ctx.launches() - launches0
+    ms = t_start.elapsed_time(t_end)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    build_ms = statistics.median(e[0].elapsed_time(e[1]) for e in evs)
+    probe_ms = statistics.median(e[1].elapsed_time(e[2]) for e in evs)
+    value = (nR + nS) * args.steps * world / (ms / 1000.0)
+
+    hbm, peak_kind = peaks()
+    probe_bytes = nS * 16  # every probe tuple read once
+    achieved = probe_bytes / (probe_ms / 1000.0) / 1e9
+    step_bytes = (nR + nS) * 16
+    roofline = {"bound": "hbm", "kernel": "probe_agg16_kernel", "achieved": round(achieved, 1), "peak": hbm,
+                "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_source": peak_kind,
+                "traffic": None,
+                "step_achieved_gbs": round(step_bytes / (ms / args.steps / 1000.0) / 1e9, 1),
+                "step_frac": round(step_bytes / (ms / args.steps / 1000.0) / 1e9 / hbm, 4),
+                "build_ms": round(build_ms, 3), "probe_ms": round(probe_ms, 3)}
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        key = f"theta={args.theta}"
+        if key in tj:
+            roofline["traffic"] = tj[key].get("probe_bytes_per_launch")
+
+    # End to end: the same C-ABI calls with host (pinned) buffers; the
+    # library copies each relation to the device inside the timed region.
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, torch, pyg, ctx, R, S, nR, nS, world, dist)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            r = run_reference_cpu(args.theta, 3)
+            cpu = {"value": r["tuples"] * len(r["times"]) / sum(r["times"]), "unit": UNIT, "cores": r["cores"],
+                   "kind": r["kind"], "sample": r["sample"]}
+        except Exception as ex:  # the CPU leg must not hide the GPU number
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "unavailable", "sample": str(ex)[:200]}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded, device-generated)",
+                "config": {"workload": "radix-scale PK-FK hash join + count + checksum", "build_tuples": nR,
+                           "probe_tuples": nS, "tuple_bytes": 16, "theta": args.theta,
+                           "load_factor": args.load_factor, "parallelism": f"replicas{world}",
+                           "l2": "inputs (19.3 GB) larger than L2; no flush needed"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_e2e(args, torch, pyg, ctx, R, S, nR, nS, world, dist):
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 0
+    need = (nR + nS) * 16
+    if avail and avail < 3 * need:
+        return {"value": None, "unit": UNIT, "skipped": f"host RAM {avail >> 30} GiB < 3x inputs"}
+    hR = pyg.HostBuf(nR * 16)
+    hS = pyg.HostBuf(nS * 16)
+    try:
+        ctx.d2h(hR.np, R)
+        ctx.d2h(hS.np, S)
+        Rh = pyg.Rel(hR.ptr, nR, [pyg.INT64, pyg.INT64], on_device=0)
+        Sh = pyg.Rel(hS.ptr, nS, [pyg.INT64, pyg.INT64], on_device=0)
+        proj = [(0, 1), (1, 1)]
+
+        def step():
+            ht = ctx.hashjoin_build(Rh, [0], [1], pyg.HT_AGGREGATE, args.load_factor)
+            cnt, sums = ctx.hashjoin_probe_agg(ht, Sh, [0], proj)
+            ht.free()
+            return cnt
+
+        step()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        steps = max(1, min(args.steps, 3))
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        stream = torch.cuda.current_stream()
+        t0.record(stream)
+        for _ in range(steps):
+            c = step()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        assert c == nS
+        ms = t0.elapsed_time(t1)
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return {"value": (nR + nS) * steps * world / (ms / 1000.0), "unit": UNIT,
+                "h2d_bytes_per_step": (nR + nS) * 16, "d2h_bytes_per_step": 2 * 8 * 4 + 9 * 8,
+                "ms_per_step": ms / steps, "host_buffers": "pinned"}
+    finally:
+        hR.free()
+        hS.free()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        main_reference(args)
+    else:
+        main_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,658 @@
+// Hash join on one B200: open-addressing table in HBM, atomicCAS inserts,
+// fused count/sum probe (16-byte vector loads, several independent probes
+// in flight per thread), and a materialising probe with warp-aggregated
+// output allocation.
+//
+// Semantics follow the reference's HashJoinOp (operators/join.cpp:367-903):
+// every (build, probe) pair with equal keys is one output tuple made of the
+// projected columns.  The bucket function of the reference only places
+// tuples; the join result does not depend on it, so the table here uses its
+// own hash (a 64-bit bijective mix + multiply-high range reduction) and
+// linear probing.
+#include <string.h>
+
+#include "pyg_internal.cuh"
+#include "hashtable.cuh"
+
+namespace pyg {
+
+// ---------------------------------------------------------------------------
+// Kernels
+
+__global__ void ht_init_kernel(uint64_t* __restrict__ slots, uint64_t cap, int W)
+{
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    if (W == 2) {
+        ulonglong2* s2 = reinterpret_cast<ulonglong2*>(slots);
+        for (; i < cap; i += stride) s2[i] = make_ulonglong2(kEmptyKey, 0ULL);
+        return;
+    }
+    uint64_t words = cap * (uint64_t)W;
+    for (; i < words; i += stride) slots[i] = (i % W == 0) ? kEmptyKey : 0ULL;
+}
+
+struct BuildArgs {
+    const uint8_t* base;
+    int64_t n;
+    int32_t tb;
+    KeySpec ks;
+    ColSpec pay;              // stored build columns
+    uint64_t* slots;
+    uint64_t cap;
+    int W;
+    int agg;                  // AGGREGATE mode
+    uint64_t* side;           // entries whose key word equals kEmptyKey
+    int64_t side_cap;
+    unsigned long long* flags;  // [0] dup, [1] full, [2] side count, [3] new entries
+};
+
+__global__ void ht_build_kernel(BuildArgs a)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    unsigned long long fresh = 0, dup = 0, full = 0;
+    for (; i < a.n; i += stride) {
+        const uint8_t* t = a.base + i * (int64_t)a.tb;
+        uint64_t k = load_key(t, a.ks);
+        if (k == kEmptyKey) {
+            unsigned long long e = atomicAdd(&a.flags[2], 1ULL);
+            if ((int64_t)e < a.side_cap) {
+                uint64_t* dst = a.side + e * a.W;
+                dst[0] = k;
+                for (int c = 0; c < a.pay.n; ++c) dst[1 + c] = (uint64_t)load_col(t, a.pay.off[c], a.pay.type[c]);
+            }
+            continue;
+        }
+        uint64_t s = reduce_range(mix64(k), a.cap);
+        uint64_t steps = 0;
+        for (;;) {
+            uint64_t* slot = a.slots + s * a.W;
+            unsigned long long prev = atomicCAS((unsigned long long*)slot, kEmptyKey, k);
+            if (prev == kEmptyKey) {
+                ++fresh;
+                if (a.agg) {
+                    for (int c = 0; c < a.pay.n; ++c)
+                        atomicAdd((unsigned long long*)&slot[1 + c],
+                                  (unsigned long long)load_col(t, a.pay.off[c], a.pay.type[c]));
+                } else {
+                    for (int c = 0; c < a.pay.n; ++c) slot[1 + c] = (uint64_t)load_col(t, a.pay.off[c], a.pay.type[c]);
+                }
+                break;
+            }
+            if (prev == k) {
+                dup = 1;
+                if (a.agg) {
+                    for (int c = 0; c < a.pay.n; ++c)
+                        atomicAdd((unsigned long long*)&slot[1 + c],
+                                  (unsigned long long)load_col(t, a.pay.off[c], a.pay.type[c]));
+                    break;
+                }
+            }
+            if (++steps >= a.cap) {
+                full = 1;
+                break;
+            }
+            s = (s + 1 == a.cap) ? 0 : s + 1;
+        }
+    }
+    // One atomic per warp for the counters.
+    fresh = warp_sum_u64(fresh);
+    dup = __any_sync(0xffffffffu, dup != 0);
+    full = __any_sync(0xffffffffu, full != 0);
+    if ((threadIdx.x & 31) == 0) {
+        if (fresh) atomicAdd(&a.flags[3], fresh);
+        if (dup) a.flags[0] = 1;
+        if (full) a.flags[1] = 1;
+    }
+}
+
+// Duplicate counts for an AGGREGATE table (run only when duplicates exist).
+__global__ void ht_count_kernel(BuildArgs a, unsigned long long* __restrict__ counts)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < a.n; i += stride) {
+        uint64_t k = load_key(a.base + i * (int64_t)a.tb, a.ks);
+        if (k == kEmptyKey) continue;
+        uint64_t s = reduce_range(mix64(k), a.cap);
+        for (uint64_t steps = 0; steps < a.cap; ++steps) {
+            uint64_t key = a.slots[s * a.W];
+            if (key == k) {
+                atomicAdd(&counts[s], 1ULL);
+                break;
+            }
+            if (key == kEmptyKey) break;
+            s = (s + 1 == a.cap) ? 0 : s + 1;
+        }
+    }
+}
+
+// Shared accumulation of probe results: [0] = count, [1 + p] = sum of
+// projected column p.
+__device__ __forceinline__ void block_flush(uint64_t* acc, int nacc, unsigned long long* out)
+{
+    __shared__ unsigned long long red[PYG_MAX_COLS + 1];
+    if (threadIdx.x <= PYG_MAX_COLS) red[threadIdx.x] = 0;
+    __syncthreads();
+    for (int j = 0; j < nacc; ++j) {
+        uint64_t v = warp_sum_u64(acc[j]);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&red[j], (unsigned long long)v);
+    }
+    __syncthreads();
+    if (threadIdx.x < nacc && red[threadIdx.x]) atomicAdd(&out[threadIdx.x], red[threadIdx.x]);
+}
+
+// Fast path: 16-byte (int64 key, int64 value) probe tuples against a
+// 16-byte-slot AGGREGATE table (one int64 build payload).  want_b / want_p
+// select which of the build sum and the probe sum are accumulated.
+template <int UNROLL>
+__global__ void __launch_bounds__(256) probe_agg16_kernel(const longlong2* __restrict__ S, int64_t n,
+                                                          const ulonglong2* __restrict__ slots, uint64_t cap,
+                                                          const unsigned long long* __restrict__ counts,
+                                                          const uint64_t* __restrict__ side, int64_t nside,
+                                                          unsigned long long* __restrict__ out)
+{
+    uint64_t cnt = 0, bsum = 0, psum = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t base = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; base < n; base += stride * UNROLL) {
+        longlong2 t[UNROLL];
+        uint64_t s[UNROLL];
+        ulonglong2 e[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            int64_t idx = base + u * stride;
+            t[u] = idx < n ? __ldcs(&S[idx]) : make_longlong2((long long)kEmptyKey, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            s[u] = reduce_range(mix64((uint64_t)t[u].x), cap);
+            e[u] = __ldg(&slots[s[u]]);
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            int64_t idx = base + u * stride;
+            if (idx >= n) continue;
+            uint64_t k = (uint64_t)t[u].x;
+            if (k == kEmptyKey) {
+                for (int64_t j = 0; j < nside; ++j)
+                    if (side[2 * j] == k) {
+                        ++cnt;
+                        bsum += side[2 * j + 1];
+                        psum += (uint64_t)t[u].y;
+                    }
+                continue;
+            }
+            uint64_t ss = s[u];
+            ulonglong2 ee = e[u];
+            uint64_t steps = 0;
+            while (ee.x != k && ee.x != kEmptyKey && ++steps < cap) {
+                ss = (ss + 1 == cap) ? 0 : ss + 1;
+                ee = __ldg(&slots[ss]);
+            }
+            if (ee.x == k) {
+                uint64_t c = counts ? (uint64_t)counts[ss] : 1ULL;
+                cnt += c;
+                bsum += ee.y;
+                psum += c * (uint64_t)t[u].y;
+            }
+        }
+    }
+    uint64_t acc[3] = {cnt, bsum, psum};
+    block_flush(acc, 3, out);
+}
+
+struct ProbeArgs {
+    const uint8_t* base;
+    int64_t n;
+    int32_t tb;
+    KeySpec ks;
+    const uint64_t* slots;
+    uint64_t cap;
+    int W;
+    int agg;
+    const unsigned long long* counts;
+    const uint64_t* side;
+    int64_t nside;
+    int nproj;
+    int32_t pside[PYG_MAX_COLS];   // 0 build, 1 probe
+    int32_t pidx[PYG_MAX_COLS];    // build: word index in slot (1..W-1); probe: unused
+    int32_t poff[PYG_MAX_COLS];    // probe column offset / output offset
+    int32_t ptype[PYG_MAX_COLS];   // column type
+    int32_t outoff[PYG_MAX_COLS];  // byte offset in the output tuple
+    int32_t out_tb;
+};
+
+// Generic fused count/sum probe (any layout, either table mode).
+__global__ void __launch_bounds__(256) probe_agg_kernel(ProbeArgs a, unsigned long long* __restrict__ out)
+{
+    uint64_t acc[PYG_MAX_COLS + 1];
+#pragma unroll
+    for (int j = 0; j <= PYG_MAX_COLS; ++j) acc[j] = 0;
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < a.n; i += stride) {
+        const uint8_t* t = a.base + i * (int64_t)a.tb;
+        uint64_t k = load_key(t, a.ks);
+        uint64_t pv[PYG_MAX_COLS];
+        for (int p = 0; p < a.nproj; ++p)
+            pv[p] = a.pside[p] ? (uint64_t)load_col(t, a.poff[p], a.ptype[p]) : 0;
+        if (k == kEmptyKey) {
+            for (int64_t j = 0; j < a.nside; ++j) {
+                const uint64_t* e = a.side + j * a.W;
+                if (e[0] != k) continue;
+                acc[0] += 1;
+                for (int p = 0; p < a.nproj; ++p) acc[1 + p] += a.pside[p] ? pv[p] : e[a.pidx[p]];
+            }
+            continue;
+        }
+        uint64_t s = reduce_range(mix64(k), a.cap);
+        for (uint64_t steps = 0; steps < a.cap; ++steps) {
+            const uint64_t* e = a.slots + s * a.W;
+            uint64_t key = e[0];
+            if (key == kEmptyKey) break;
+            if (key == k) {
+                uint64_t c = a.counts ? (uint64_t)a.counts[s] : 1ULL;
+                acc[0] += c;
+                for (int p = 0; p < a.nproj; ++p) acc[1 + p] += a.pside[p] ? c * pv[p] : e[a.pidx[p]];
+                if (a.agg) break;
+            }
+            s = (s + 1 == a.cap) ? 0 : s + 1;
+        }
+    }
+    block_flush(acc, a.nproj + 1, out);
+}
+
+__device__ __forceinline__ void store_col(uint8_t* dst, uint64_t v, int32_t type)
+{
+    if (type == PYG_INT32) {
+        uint32_t w = (uint32_t)v;
+        memcpy(dst, &w, 4);
+    } else {
+        memcpy(dst, &v, 8);
+    }
+}
+
+// Materialising probe.  Each lane first counts its matches, the warp
+// reserves one contiguous output range with a single atomic, then every lane
+// walks its chain again writing its pairs.  Pairs past the capacity are
+// counted but not written.
+__global__ void __launch_bounds__(256) probe_mat_kernel(ProbeArgs a, uint8_t* __restrict__ out, int64_t out_cap,
+                                                        unsigned long long* __restrict__ cursor)
+{
+    const unsigned lane = threadIdx.x & 31;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t first = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u);
+    // Whole warps iterate together so the warp-wide scan stays converged.
+    for (int64_t wbase = first; wbase < a.n; wbase += stride) {
+        int64_t i = wbase + lane;
+        bool valid = i < a.n;
+        const uint8_t* t = valid ? a.base + i * (int64_t)a.tb : nullptr;
+        uint64_t k = valid ? load_key(t, a.ks) : 0;
+        uint64_t s0 = valid ? reduce_range(mix64(k), a.cap) : 0;
+        unsigned long long m = 0;
+        if (valid) {
+            if (k == kEmptyKey) {
+                for (int64_t j = 0; j < a.nside; ++j) m += (a.side[j * a.W] == k);
+            } else {
+                uint64_t s = s0;
+                for (uint64_t steps = 0; steps < a.cap; ++steps) {
+                    uint64_t key = a.slots[s * a.W];
+                    if (key == kEmptyKey) break;
+                    m += (key == k);
+                    s = (s + 1 == a.cap) ? 0 : s + 1;
+                }
+            }
+        }
+        // Warp-inclusive scan of match counts.
+        unsigned long long incl = m;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (unsigned)o) incl += v;
+        }
+        unsigned long long total = __shfl_sync(0xffffffffu, incl, 31);
+        unsigned long long wstart = 0;
+        if (lane == 31 && total) wstart = atomicAdd(cursor, total);
+        wstart = __shfl_sync(0xffffffffu, wstart, 31);
+        if (!valid || m == 0) continue;
+        int64_t pos = (int64_t)(wstart + incl - m);
+        auto emit = [&](const uint64_t* e) {
+            if (pos < out_cap) {
+                uint8_t* dst = out + pos * (int64_t)a.out_tb;
+                for (int p = 0; p < a.nproj; ++p) {
+                    uint64_t v = a.pside[p] ? (uint64_t)load_col(t, a.poff[p], a.ptype[p]) : e[a.pidx[p]];
+                    store_col(dst + a.outoff[p], v, a.ptype[p]);
+                }
+            }
+            ++pos;
+        };
+        if (k == kEmptyKey) {
+            for (int64_t j = 0; j < a.nside; ++j)
+                if (a.side[j * a.W] == k) emit(a.side + j * a.W);
+        } else {
+            uint64_t s = s0;
+            for (uint64_t steps = 0; steps < a.cap; ++steps) {
+                const uint64_t* e = a.slots + s * a.W;
+                if (e[0] == kEmptyKey) break;
+                if (e[0] == k) emit(e);
+                s = (s + 1 == a.cap) ? 0 : s + 1;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+
+static int fill_probe_args(pyg_ctx* ctx, const pyg_hashtable* ht, const pyg_rel* S, const int32_t* key_cols,
+                           const pyg_proj* proj, int32_t nproj, ProbeArgs* a)
+{
+    (void)ctx;
+    memset(a, 0, sizeof(*a));
+    if (nproj < 0 || nproj > PYG_MAX_COLS || (nproj > 0 && !proj)) {
+        set_error("probe: nproj must be in [0, %d]", PYG_MAX_COLS);
+        return PYG_ERR_ARG;
+    }
+    int rc = make_keyspec(S, key_cols, ht->nkeys, &a->ks);
+    if (rc) return rc;
+    if (a->ks.nkeys != ht->ks.nkeys) {
+        set_error("probe: key arity differs from the build side");
+        return PYG_ERR_ARG;
+    }
+    a->base = (const uint8_t*)S->base;
+    a->n = S->ntuples;
+    a->tb = S->tuple_bytes;
+    a->slots = ht->slots;
+    a->cap = ht->cap;
+    a->W = ht->W;
+    a->agg = ht->mode == PYG_HT_AGGREGATE;
+    a->counts = ht->counts;
+    a->side = ht->side;
+    a->nside = ht->nside;
+    a->nproj = nproj;
+    int off = 0;
+    for (int p = 0; p < nproj; ++p) {
+        a->pside[p] = proj[p].side ? 1 : 0;
+        if (proj[p].side) {
+            if (proj[p].col < 0 || proj[p].col >= S->ncols) {
+                set_error("probe: projection P$%d out of range", proj[p].col);
+                return PYG_ERR_ARG;
+            }
+            a->poff[p] = S->col_offset[proj[p].col];
+            a->ptype[p] = S->col_type[proj[p].col];
+        } else {
+            int w = -1;
+            for (int c = 0; c < ht->npay; ++c)
+                if (ht->pay_cols[c] == proj[p].col) w = c;
+            if (w < 0) {
+                set_error("probe: projection B$%d is not a stored build column", proj[p].col);
+                return PYG_ERR_ARG;
+            }
+            a->pidx[p] = 1 + w;
+            a->ptype[p] = ht->pay_types[w];
+        }
+        a->outoff[p] = off;
+        off += a->ptype[p] == PYG_INT32 ? 4 : 8;
+    }
+    a->out_tb = off;
+    return PYG_OK;
+}
+
+}  // namespace pyg
+
+using namespace pyg;
+
+extern "C" {
+
+int pyg_hashjoin_build(pyg_ctx* ctx, const pyg_rel* build, const int32_t* key_cols, int32_t nkeys,
+                       const int32_t* payload_cols, int32_t npayload, int32_t mode, float load_factor,
+                       pyg_hashtable** out)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out) {
+        set_error("pyg_hashjoin_build: null out");
+        return PYG_ERR_ARG;
+    }
+    *out = nullptr;
+    if ((rc = check_rel(build, "build"))) return rc;
+    if (mode != PYG_HT_AGGREGATE && mode != PYG_HT_MATERIALIZE) {
+        set_error("pyg_hashjoin_build: bad mode %d", mode);
+        return PYG_ERR_ARG;
+    }
+    if (!(load_factor > 0.f && load_factor <= 0.95f)) {
+        set_error("pyg_hashjoin_build: load factor %f outside (0, 0.95]", (double)load_factor);
+        return PYG_ERR_ARG;
+    }
+    if (npayload < 0 || npayload > PYG_MAX_COLS - 1 || (npayload > 0 && !payload_cols)) {
+        set_error("pyg_hashjoin_build: npayload must be in [0, %d]", PYG_MAX_COLS - 1);
+        return PYG_ERR_ARG;
+    }
+    pyg_hashtable* ht = new pyg_hashtable();
+    ht->mode = mode;
+    ht->nkeys = nkeys;
+    if ((rc = make_keyspec(build, key_cols, nkeys, &ht->ks))) {
+        delete ht;
+        return rc;
+    }
+    ht->npay = npayload;
+    BuildArgs a;
+    memset(&a, 0, sizeof(a));
+    a.pay.n = npayload;
+    for (int c = 0; c < npayload; ++c) {
+        if (payload_cols[c] < 0 || payload_cols[c] >= build->ncols) {
+            set_error("pyg_hashjoin_build: payload column %d out of range", payload_cols[c]);
+            delete ht;
+            return PYG_ERR_ARG;
+        }
+        ht->pay_cols[c] = payload_cols[c];
+        ht->pay_types[c] = build->col_type[payload_cols[c]];
+        a.pay.off[c] = build->col_offset[payload_cols[c]];
+        a.pay.type[c] = build->col_type[payload_cols[c]];
+    }
+    ht->W = 1 + npayload;
+    uint64_t cap = (uint64_t)((double)build->ntuples / (double)load_factor) + 1;
+    if (cap < 64) cap = 64;
+    ht->cap = cap;
+
+    DevRel R;
+    if ((rc = R.stage(ctx, build))) {
+        delete ht;
+        return rc;
+    }
+    int64_t side_cap = build->ntuples < 1024 ? (build->ntuples > 0 ? build->ntuples : 1) : 1024;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        if ((rc = dalloc(ctx, (void**)&ht->slots, cap * ht->W * sizeof(uint64_t)))) break;
+        if ((rc = dalloc(ctx, (void**)&ht->side, side_cap * ht->W * sizeof(uint64_t)))) break;
+        int threads = 256;
+        int grid = grid_for(ctx, (int64_t)cap * (ht->W == 2 ? 1 : ht->W), threads, 4, 8);
+        ht_init_kernel<<<grid, threads, 0, ctx->stream>>>(ht->slots, cap, ht->W);
+        PYG_LAUNCHED(ctx);
+        unsigned long long* flags = ctx->dcounters;
+        PYG_CUDA(cudaMemsetAsync(flags, 0, 8 * sizeof(unsigned long long), ctx->stream));
+        a.base = (const uint8_t*)R.rel.base;
+        a.n = build->ntuples;
+        a.tb = build->tuple_bytes;
+        a.ks = ht->ks;
+        a.slots = ht->slots;
+        a.cap = cap;
+        a.W = ht->W;
+        a.agg = mode == PYG_HT_AGGREGATE;
+        a.side = ht->side;
+        a.side_cap = side_cap;
+        a.flags = flags;
+        if (a.n > 0) {
+            grid = grid_for(ctx, a.n, threads, 1, 8);
+            ht_build_kernel<<<grid, threads, 0, ctx->stream>>>(a);
+            PYG_LAUNCHED(ctx);
+        }
+        unsigned long long* h = (unsigned long long*)ctx->pinned;
+        PYG_CUDA(cudaMemcpyAsync(h, flags, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (h[1]) {
+            set_error("pyg_hashjoin_build: table full (capacity %llu)", (unsigned long long)cap);
+            rc = PYG_ERR_TABLE_FULL;
+            break;
+        }
+        ht->has_dups = h[0] ? 1 : 0;
+        ht->entries = (int64_t)h[3];
+        ht->nside = (int64_t)h[2];
+        if (ht->nside > side_cap) {
+            // More keys equal to the empty marker than the side list holds:
+            // rebuild once with an exact side list.
+            dfree(ctx, ht->slots);
+            dfree(ctx, ht->side);
+            ht->slots = nullptr;
+            ht->side = nullptr;
+            side_cap = ht->nside;
+            continue;
+        }
+        ht->entries += ht->nside;  // side entries are kept per tuple
+        if (ht->has_dups && mode == PYG_HT_AGGREGATE && a.n > 0) {
+            if ((rc = dalloc(ctx, (void**)&ht->counts, cap * sizeof(unsigned long long)))) break;
+            PYG_CUDA(cudaMemsetAsync(ht->counts, 0, cap * sizeof(unsigned long long), ctx->stream));
+            grid = grid_for(ctx, a.n, threads, 1, 8);
+            ht_count_kernel<<<grid, threads, 0, ctx->stream>>>(a, ht->counts);
+            PYG_LAUNCHED(ctx);
+        }
+        rc = PYG_OK;
+        break;
+    }
+    R.release(ctx);
+    if (rc) {
+        pyg_hashtable_free(ctx, ht);
+        return rc;
+    }
+    *out = ht;
+    return PYG_OK;
+}
+
+int pyg_hashtable_free(pyg_ctx* ctx, pyg_hashtable* ht)
+{
+    if (!ht) return PYG_OK;
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    dfree(ctx, ht->slots);
+    dfree(ctx, ht->side);
+    dfree(ctx, ht->counts);
+    delete ht;
+    return PYG_OK;
+}
+
+int pyg_hashtable_stats(pyg_ctx* ctx, const pyg_hashtable* ht, int64_t* entries, int64_t* capacity,
+                        int32_t* has_duplicates)
+{
+    (void)ctx;
+    if (!ht) {
+        set_error("pyg_hashtable_stats: null table");
+        return PYG_ERR_ARG;
+    }
+    if (entries) *entries = ht->entries;
+    if (capacity) *capacity = (int64_t)ht->cap;
+    if (has_duplicates) *has_duplicates = ht->has_dups;
+    return PYG_OK;
+}
+
+int pyg_hashjoin_probe_agg(pyg_ctx* ctx, const pyg_hashtable* ht, const pyg_rel* probe, const int32_t* key_cols,
+                           const pyg_proj* proj, int32_t nproj, pyg_join_result* out)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!ht || !out) {
+        set_error("pyg_hashjoin_probe_agg: null table or out");
+        return PYG_ERR_ARG;
+    }
+    if ((rc = check_rel(probe, "probe"))) return rc;
+    ProbeArgs a;
+    if ((rc = fill_probe_args(ctx, ht, probe, key_cols, proj, nproj, &a))) return rc;
+    DevRel S;
+    if ((rc = S.stage(ctx, probe))) return rc;
+    a.base = (const uint8_t*)S.rel.base;
+    unsigned long long* acc = ctx->dcounters + 8;
+    PYG_CUDA(cudaMemsetAsync(acc, 0, (PYG_MAX_COLS + 1) * sizeof(unsigned long long), ctx->stream));
+    int threads = 256;
+    // 16-byte fast path: (int64 key @0, int64 value @8) probe tuples, a
+    // one-payload AGGREGATE table, projection over {B$payload, P$1}.
+    bool fast = a.agg && ht->W == 2 && probe->tuple_bytes == 16 && a.ks.nkeys == 1 && a.ks.off0 == 0 &&
+                a.ks.type0 == PYG_INT64 && ((uintptr_t)a.base % 16 == 0) && nproj <= 2;
+    int fb = -1, fp = -1;
+    for (int p = 0; fast && p < nproj; ++p) {
+        if (a.pside[p] == 0 && a.ptype[p] == PYG_INT64 && fb < 0) fb = p;
+        else if (a.pside[p] == 1 && a.poff[p] == 8 && a.ptype[p] == PYG_INT64 && fp < 0) fp = p;
+        else fast = false;
+    }
+    if (a.n > 0) {
+        if (fast) {
+            int grid = grid_for(ctx, a.n, threads, 4, 8);
+            probe_agg16_kernel<4><<<grid, threads, 0, ctx->stream>>>(
+                (const longlong2*)a.base, a.n, (const ulonglong2*)a.slots, a.cap, a.counts, a.side, a.nside, acc);
+        } else {
+            int grid = grid_for(ctx, a.n, threads, 1, 8);
+            probe_agg_kernel<<<grid, threads, 0, ctx->stream>>>(a, acc);
+        }
+        PYG_LAUNCHED(ctx);
+    }
+    unsigned long long* h = (unsigned long long*)ctx->pinned;
+    PYG_CUDA(cudaMemcpyAsync(h, acc, (PYG_MAX_COLS + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    S.release(ctx);
+    PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+    memset(out, 0, sizeof(*out));
+    out->count = (int64_t)h[0];
+    for (int p = 0; p < nproj; ++p) {
+        uint64_t v;
+        if (fast) v = (p == fb) ? h[1] : h[2];
+        else v = h[1 + p];
+        out->sums[p] = a.ptype[p] == PYG_INT32 ? (int64_t)(int32_t)(uint32_t)v : (int64_t)v;
+    }
+    return PYG_OK;
+}
+
+int pyg_hashjoin_probe_materialize(pyg_ctx* ctx, const pyg_hashtable* ht, const pyg_rel* probe,
+                                   const int32_t* key_cols, const pyg_proj* proj, int32_t nproj, void* out,
+                                   int64_t out_capacity, int64_t* out_count)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!ht || !out_count || (out_capacity > 0 && !out)) {
+        set_error("pyg_hashjoin_probe_materialize: null argument");
+        return PYG_ERR_ARG;
+    }
+    if (ht->mode != PYG_HT_MATERIALIZE) {
+        set_error("pyg_hashjoin_probe_materialize: table was built in AGGREGATE mode");
+        return PYG_ERR_ARG;
+    }
+    if ((rc = check_rel(probe, "probe"))) return rc;
+    ProbeArgs a;
+    if ((rc = fill_probe_args(ctx, ht, probe, key_cols, proj, nproj, &a))) return rc;
+    if (nproj < 1) {
+        set_error("pyg_hashjoin_probe_materialize: empty projection");
+        return PYG_ERR_ARG;
+    }
+    DevRel S;
+    if ((rc = S.stage(ctx, probe))) return rc;
+    a.base = (const uint8_t*)S.rel.base;
+    unsigned long long* cursor = ctx->dcounters + 24;
+    PYG_CUDA(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), ctx->stream));
+    if (a.n > 0) {
+        int threads = 256;
+        int grid = grid_for(ctx, a.n, threads, 1, 8);
+        probe_mat_kernel<<<grid, threads, 0, ctx->stream>>>(a, (uint8_t*)out, out_capacity, cursor);
+        PYG_LAUNCHED(ctx);
+    }
+    unsigned long long* h = (unsigned long long*)ctx->pinned;
+    PYG_CUDA(cudaMemcpyAsync(h, cursor, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+    S.release(ctx);
+    PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+    *out_count = (int64_t)h[0];
+    if (*out_count > out_capacity) {
+        set_error("pyg_hashjoin_probe_materialize: %lld pairs exceed capacity %lld", (long long)*out_count,
+                  (long long)out_capacity);
+        return PYG_ERR_CAPACITY;
+    }
+    return PYG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,135 @@
+// Internal definitions shared by the libpyg CUDA sources (sm_100a only).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string>
+
+#include "../../include/pyg.h"
+
+struct pyg_ctx {
+    int device;
+    int sm_count;
+    cudaStream_t own_stream;
+    cudaStream_t stream;
+    int64_t launches;
+    // Small pinned host staging area for scalar results read back per call.
+    void* pinned;
+    size_t pinned_bytes;
+    // Device scratch for scalar counters (zeroed per use).
+    unsigned long long* dcounters;
+};
+
+namespace pyg {
+
+void set_error(const char* fmt, ...);
+
+// Records the error (if any) of the last CUDA call and maps it to a status.
+int cuda_status(cudaError_t e, const char* what);
+
+#define PYG_CUDA(call)                                                  \
+    do {                                                                \
+        cudaError_t _e = (call);                                        \
+        if (_e != cudaSuccess) return ::pyg::cuda_status(_e, #call);    \
+    } while (0)
+
+#define PYG_LAUNCHED(ctx)                                               \
+    do {                                                                \
+        (ctx)->launches++;                                              \
+        cudaError_t _e = cudaGetLastError();                            \
+        if (_e != cudaSuccess) return ::pyg::cuda_status(_e, "launch"); \
+    } while (0)
+
+int check_ctx(pyg_ctx* ctx);
+int check_rel(const pyg_rel* r, const char* name);
+
+// Device memory from the stream-ordered pool.
+int dalloc(pyg_ctx* ctx, void** p, size_t bytes);
+void dfree(pyg_ctx* ctx, void* p);
+
+// A relation staged on the device: either the caller's device buffer or a
+// temporary copy of a host buffer (freed by release()).
+struct DevRel {
+    pyg_rel rel;
+    void* owned = nullptr;
+    int stage(pyg_ctx* ctx, const pyg_rel* in);
+    void release(pyg_ctx* ctx);
+};
+
+// Key of up to 8 bytes packed into one 64-bit word.  A single int64 column
+// is the value itself; a single int32 column is sign-extended; a pair of
+// int32 columns is (first << 32) | (uint32)second, so the packed word's
+// signed order is the lexicographic order of the pair.
+struct KeySpec {
+    int32_t nkeys;
+    int32_t off0, off1;
+    int32_t type0, type1;
+};
+int make_keyspec(const pyg_rel* r, const int32_t* cols, int32_t nkeys, KeySpec* ks);
+
+// Column reader description for up to PYG_MAX_COLS value columns.
+struct ColSpec {
+    int32_t n;
+    int32_t off[PYG_MAX_COLS];
+    int32_t type[PYG_MAX_COLS];
+};
+
+__device__ __forceinline__ int64_t load_col(const uint8_t* t, int32_t off, int32_t type)
+{
+    if (type == PYG_INT32) {
+        int32_t v;
+        memcpy(&v, t + off, 4);
+        return (int64_t)v;
+    }
+    int64_t v;
+    memcpy(&v, t + off, 8);
+    return v;
+}
+
+__device__ __forceinline__ uint64_t load_key(const uint8_t* t, const KeySpec& ks)
+{
+    if (ks.nkeys == 1) return (uint64_t)load_col(t, ks.off0, ks.type0);
+    uint32_t a, b;
+    memcpy(&a, t + ks.off0, 4);
+    memcpy(&b, t + ks.off1, 4);
+    return ((uint64_t)a << 32) | (uint64_t)b;
+}
+
+// 64-bit finaliser (the MurmurHash3 fmix64 mixing function).  It is a
+// bijection, so distinct keys never share a mixed value.
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t k)
+{
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdULL;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ULL;
+    k ^= k >> 33;
+    return k;
+}
+
+// Slot index in [0, cap) from a mixed hash: multiply-high range reduction.
+__device__ __forceinline__ uint64_t reduce_range(uint64_t h, uint64_t cap)
+{
+    return __umul64hi(h, cap);
+}
+
+constexpr uint64_t kEmptyKey = 0x8000000000000000ULL;
+
+inline int grid_for(pyg_ctx* ctx, int64_t work, int threads, int per_thread, int blocks_per_sm)
+{
+    int64_t need = (work + (int64_t)threads * per_thread - 1) / ((int64_t)threads * per_thread);
+    int64_t cap = (int64_t)ctx->sm_count * blocks_per_sm;
+    if (need < 1) need = 1;
+    return (int)(need < cap ? need : cap);
+}
+
+// Warp-level 64-bit sum.
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace pyg

@@ -1,0 +1,97 @@
+"""Group-by aggregation on the GPU vs the oracle and the reference's golden
+outputs (bit-exact sums and counts, output ordered by key)."""
+import numpy as np
+import pytest
+
+import oracle as O
+import pyg
+from util import I32, I64, alloc, dev_rel, from_device, host_rel, rows, struct
+
+pytestmark = pytest.mark.gpu
+
+
+def run_groupby(ctx, torch, A, types, keys, flags, sum_col, expected, on_device=True, sort=True):
+    rel = dev_rel(torch, A, types) if on_device else host_rel(A, types)
+    dt = O.groupby_dtype(types, keys, flags, sum_col)
+    cap = max(1, A.shape[0])
+    out = alloc(torch, cap * dt.itemsize)
+    rc, g = ctx.groupby(rel, keys, flags, sum_col, sort, expected, out, cap)
+    assert rc == pyg.PYG_OK
+    return from_device(torch, out, g, dt)
+
+
+@pytest.mark.parametrize("expected", [1024, 0, 16])
+def test_groupby_int64_golden(ctx, torch_cuda, golden, expected):
+    g = golden("groupby_int64")
+    out = run_groupby(ctx, torch_cuda, g["A"], [I64, I64], [0], 3, 1, expected)
+    assert [(r[0], r[1]) for r in rows(out)] == rows(g["sum_rows"])
+    assert [(r[0], r[2]) for r in rows(out)] == rows(g["count_rows"])
+
+
+@pytest.mark.parametrize("on_device", [True, False])
+def test_groupby_composite_golden(ctx, torch_cuda, golden, on_device):
+    g = golden("groupby_composite")
+    out = run_groupby(ctx, torch_cuda, g["A"], [I32, I32, I32], [0, 1], 3, 2, 256, on_device)
+    assert [(r[0], r[1], r[3]) for r in rows(out)] == rows(g["count_rows"])
+    assert [(r[0], r[1], r[2]) for r in rows(out)] == rows(g["sum_rows"])
+
+
+@pytest.mark.parametrize("G,expected", [(16, 16), (1 << 10, 1 << 10), (1 << 16, 1 << 16), (1 << 16, 0)])
+@pytest.mark.parametrize("zipf", [False, True])
+def test_groupby_random_vs_oracle(ctx, torch_cuda, G, expected, zipf):
+    rng = np.random.default_rng(G + zipf)
+    n = 1 << 20
+    if zipf:
+        gid = (rng.zipf(1.1, n) - 1) % G
+    else:
+        gid = rng.integers(0, G, n)
+    perm = rng.permutation(G).astype(np.int64) * 1000003 - (1 << 40)
+    A = struct([perm[gid], rng.integers(0, 1 << 20, n)], [I64, I64])
+    out = run_groupby(ctx, torch_cuda, A, [I64, I64], [0], 3, 1, expected)
+    ref = O.groupby(A, [I64, I64], [0], 3, 1, buckets=G)
+    assert rows(out) == rows(ref)
+
+
+def test_groupby_edge_cases(ctx, torch_cuda):
+    mn = np.iinfo(np.int64).min
+    A = struct([np.array([mn, 3, mn, 3, 9, -1], dtype=np.int64), np.array([1, 2, 3, 4, 5, 6], dtype=np.int64)],
+               [I64, I64])
+    for exp in (0, 4):
+        out = run_groupby(ctx, torch_cuda, A, [I64, I64], [0], 3, 1, exp)
+        assert rows(out) == rows(O.groupby(A, [I64, I64], [0], 3, 1))
+    # Unordered output is the same multiset.
+    out = run_groupby(ctx, torch_cuda, A, [I64, I64], [0], 3, 1, 0, sort=False)
+    assert sorted(rows(out)) == rows(O.groupby(A, [I64, I64], [0], 3, 1))
+    # No GROUP BY, and empty input.
+    out = run_groupby(ctx, torch_cuda, A, [I64, I64], [], 3, 1, 0)
+    assert rows(out) == [(int(A["c1"].sum()), 6)]
+    E = A[:0]
+    assert run_groupby(ctx, torch_cuda, E, [I64, I64], [0], 3, 1, 0).shape[0] == 0
+    assert run_groupby(ctx, torch_cuda, E, [I64, I64], [], 3, 1, 0).shape[0] == 0
+    # Count only, sum only.
+    assert rows(run_groupby(ctx, torch_cuda, A, [I64, I64], [0], 2, 1, 0)) == rows(O.groupby(A, [I64, I64], [0], 2, 1))
+    assert rows(run_groupby(ctx, torch_cuda, A, [I64, I64], [0], 1, 1, 0)) == rows(O.groupby(A, [I64, I64], [0], 1, 1))
+
+
+def test_groupby_capacity_error(ctx, torch_cuda):
+    A = struct([np.arange(100, dtype=np.int64)] * 2, [I64, I64])
+    out = alloc(torch_cuda, 10 * 24)
+    rc, g = ctx.groupby(dev_rel(torch_cuda, A, [I64, I64]), [0], 3, 1, True, 100, out, 10)
+    assert rc == pyg.PYG_ERR_CAPACITY and g == 100
+
+
+def test_groupby_full_size_property(ctx, torch_cuda):
+    """2^26 tuples over 2^20 groups: counts sum to n, sums sum to the total."""
+    torch = torch_cuda
+    n, G = 1 << 26, 1 << 20
+    S = torch.empty(n * 2, dtype=torch.int64, device="cuda")
+    ctx.gen_fk(S, n, G, 1.0, 3, 1 << 20, 4)
+    rel = pyg.Rel(S, n, [I64, I64])
+    out = torch.empty(G * 3, dtype=torch.int64, device="cuda")
+    rc, g = ctx.groupby(rel, [0], 3, 1, True, G, out, G)
+    assert rc == pyg.PYG_OK and 0 < g <= G
+    o = out[: 3 * g].view(g, 3)
+    assert int(o[:, 2].sum().item()) == n
+    assert int(o[:, 1].sum().item()) == int(S.view(n, 2)[:, 1].sum().item())
+    assert bool((o[1:, 0] > o[:-1, 0]).all().item())
+    assert int(torch.unique(S.view(n, 2)[:, 0]).numel()) == g
