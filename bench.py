@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--theta", type=float, default=0.0)
     ap.add_argument("--impl", default="pyg", choices=["pyg", "reference"])
     ap.add_argument("--load-factor", type=float, default=0.5)
+    ap.add_argument("--algo", default="radix", choices=["radix", "direct", "auto"])
+    ap.add_argument("--radix-bits", type=int, default=0, help="log2 partition fan-out (0 = automatic)")
     ap.add_argument("--scale-shift", type=int, default=0, help="shrink both relations by 2^s (debug only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -94,7 +96,7 @@ class Clocks:
         sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
         mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[2 + i]})
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
 
@@ -228,21 +230,16 @@ def main_gpu(args):
     Sr = pyg.Rel(S, nS, [pyg.INT64, pyg.INT64])
     proj = [(0, 1), (1, 1)]
 
-    def step(rrel, srel, evs=None):
-        if evs:
-            evs[0].record(stream)
-        ht = ctx.hashjoin_build(rrel, [0], [1], pyg.HT_AGGREGATE, args.load_factor)
-        if evs:
-            evs[1].record(stream)
-        cnt, sums = ctx.hashjoin_probe_agg(ht, srel, [0], proj)
-        if evs:
-            evs[2].record(stream)
-        ht.free()
-        return cnt, (sums[0] + sums[1]) & 0xFFFFFFFFFFFFFFFF
+    algo = {"radix": pyg.JOIN_RADIX, "direct": pyg.JOIN_DIRECT, "auto": pyg.JOIN_AUTO}[args.algo]
+
+    def step(rrel, srel, stats=False):
+        r = ctx.hashjoin_agg(rrel, [0], srel, [0], proj, algo, args.radix_bits, args.load_factor, stats=stats)
+        (cnt, sums), st = r if stats else (r, None)
+        return cnt, (sums[0] + sums[1]) & 0xFFFFFFFFFFFFFFFF, st
 
     # Size-independent check of the result (every fk matches exactly once;
     # R.payload = 7 * key): count == |S| and checksum == sum(7 fk + val).
-    cnt, chk = step(Rr, Sr)
+    cnt, chk, _ = step(Rr, Sr)
     Sv = S.view(nS, 2)
     expect = int((Sv[:, 0] * 7 + Sv[:, 1]).sum().item()) & 0xFFFFFFFFFFFFFFFF
     if cnt != nS or chk != expect:
@@ -250,7 +247,9 @@ def main_gpu(args):
 
     for _ in range(args.warmup):
         step(Rr, Sr)
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    # Phase timings (CUDA events inside the library, on the same stream)
+    # from separate untimed steps, so the timed steps carry no extra events.
+    phase = [step(Rr, Sr, stats=True)[2] for _ in range(3)]
     launches0 = ctx.launches()
     if dist:
         dist.barrier()
@@ -260,7 +259,7 @@ def main_gpu(args):
     with Clocks(local) as clk:
         t_start.record(stream)
         for k in range(args.steps):
-            step(Rr, Sr, evs[k])
+            step(Rr, Sr)
         t_end.record(stream)
         torch.cuda.synchronize()
     launches = ctx.launches() - launches0
@@ -269,27 +268,37 @@ def main_gpu(args):
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    build_ms = statistics.median(e[0].elapsed_time(e[1]) for e in evs)
-    probe_ms = statistics.median(e[1].elapsed_time(e[2]) for e in evs)
     value = (nR + nS) * args.steps * world / (ms / 1000.0)
 
     hbm, peak_kind = peaks()
-    probe_bytes = nS * 16  # every probe tuple read once
-    achieved = probe_bytes / (probe_ms / 1000.0) / 1e9
+    med = lambda f: statistics.median(getattr(p, f) for p in phase)  # noqa: E731
+    # Algorithmic bytes per phase: every tuple read once (and written once
+    # by a partition pass).
+    phases = {
+        "build_partition": (med("build_partition_ms"), nR * 16 * 2),
+        "build": (med("build_ms"), nR * 16),
+        "probe_partition": (med("probe_partition_ms"), nS * 16 * 2),
+        "probe": (med("probe_ms"), nS * 16),
+    }
+    ph = {k: {"ms": round(v[0], 3), "bytes": v[1],
+              "gbs": round(v[1] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else None,
+              "frac": round(v[1] / (v[0] / 1e3) / 1e9 / hbm, 4) if v[0] > 0 else None} for k, v in phases.items()}
+    top = max((k for k in ph if ph[k]["ms"] > 0), key=lambda k: ph[k]["ms"])
+    kernel_name = {"probe": "probe_agg16_kernel", "probe_partition": "tile_partition16_kernel",
+                   "build": "ht_build_kernel", "build_partition": "pt_scatter_kernel"}[top]
     step_bytes = (nR + nS) * 16
-    roofline = {"bound": "hbm", "kernel": "probe_agg16_kernel", "achieved": round(achieved, 1), "peak": hbm,
-                "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_source": peak_kind,
-                "traffic": None,
+    roofline = {"bound": "hbm", "kernel": kernel_name, "phase": top, "achieved": ph[top]["gbs"], "peak": hbm,
+                "unit": "GB/s", "frac": ph[top]["frac"], "peak_source": peak_kind, "traffic": None,
+                "phases": ph, "algorithm": int(phase[0].algorithm), "radix_bits": int(phase[0].radix_bits),
                 "step_achieved_gbs": round(step_bytes / (ms / args.steps / 1000.0) / 1e9, 1),
-                "step_frac": round(step_bytes / (ms / args.steps / 1000.0) / 1e9 / hbm, 4),
-                "build_ms": round(build_ms, 3), "probe_ms": round(probe_ms, 3)}
+                "step_frac": round(step_bytes / (ms / args.steps / 1000.0) / 1e9 / hbm, 4)}
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
             tj = json.load(f)
-        key = f"theta={args.theta}"
+        key = f"{kernel_name}@theta={args.theta}"
         if key in tj:
-            roofline["traffic"] = tj[key].get("probe_bytes_per_launch")
+            roofline["traffic"] = tj[key]
 
     # End to end: the same C-ABI calls with host (pinned) buffers; the
     # library copies each relation to the device inside the timed region.
@@ -341,9 +350,7 @@ def run_e2e(args, torch, pyg, ctx, R, S, nR, nS, world, dist):
         proj = [(0, 1), (1, 1)]
 
         def step():
-            ht = ctx.hashjoin_build(Rh, [0], [1], pyg.HT_AGGREGATE, args.load_factor)
-            cnt, sums = ctx.hashjoin_probe_agg(ht, Sh, [0], proj)
-            ht.free()
+            cnt, sums = ctx.hashjoin_agg(Rh, [0], Sh, [0], proj, pyg.JOIN_AUTO, 0, args.load_factor)
             return cnt
 
         step()

@@ -135,6 +135,42 @@ int pyg_hashjoin_probe_materialize(pyg_ctx* ctx, const pyg_hashtable* ht, const 
                                    const int32_t* key_cols, const pyg_proj* proj, int32_t nproj,
                                    void* out, int64_t out_capacity, int64_t* out_count);
 
+/* One-shot join + aggregate (build and probe in one call), the plan
+ * hashjoin -> aggregate_sum of the reference (HashJoinOp::scanStart +
+ * getNext, operators/join.cpp:548-757, feeding GenericAggregate).
+ * PYG_JOIN_DIRECT: one table in HBM, probed in input order.
+ * PYG_JOIN_RADIX: both sides partitioned by the top radix_bits bits of the
+ * key hash first, so each partition's probes hit one L2-sized slice of the
+ * table (16-byte (int64, int64) device relations, projection over
+ * {B$1, P$1}; other shapes use DIRECT).  PYG_JOIN_AUTO picks RADIX for
+ * large eligible inputs.  stats (optional) receives phase timings. */
+#define PYG_JOIN_AUTO   0
+#define PYG_JOIN_DIRECT 1
+#define PYG_JOIN_RADIX  2
+
+typedef struct pyg_join_opts {
+    int32_t algorithm;     /* PYG_JOIN_*                               */
+    int32_t radix_bits;    /* log2 partition fan-out (0 = automatic)   */
+    float load_factor;     /* table load factor (0 = 0.5)              */
+    int32_t reserved;
+} pyg_join_opts;
+
+typedef struct pyg_join_stats {
+    int32_t algorithm;
+    int32_t radix_bits;
+    double build_partition_ms;  /* partition the build side (RADIX)     */
+    double build_ms;            /* table init + inserts                 */
+    double probe_partition_ms;  /* partition the probe side (RADIX)     */
+    double probe_ms;            /* probes + fused aggregation           */
+    int64_t overflow_tuples;
+    int64_t padded_tuples;
+} pyg_join_stats;
+
+int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_keys,
+                     const pyg_rel* probe, const int32_t* probe_keys, int32_t nkeys,
+                     const pyg_proj* proj, int32_t nproj, const pyg_join_opts* opts,
+                     pyg_join_result* out, pyg_join_stats* stats);
+
 /* ---- group-by aggregation ------------------------------------------ */
 #define PYG_AGG_SUM    1
 #define PYG_AGG_COUNT  2

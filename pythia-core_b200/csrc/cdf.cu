@@ -1,0 +1,622 @@
+// Learned CDF splitter: a two-level piecewise-linear model trained on the
+// GPU with the library's own forward / backward kernels.
+//
+// Model (all formulas also in include/pyg_learned.h):
+//   x = (key - lo) * scale                      normalised key in [0, 1]
+//   r = a0 * x + b0                             root line (monotone: a0 >= 0)
+//   l = clamp(floor(L * r), 0, L - 1)           leaf
+//   u = clamp(L * r - l, 0, 1)                  leaf-local coordinate
+//   cdf = ylo_l + (yhi_l - ylo_l) * clamp(a_l * u + b_l, 0, 1)
+// The root is fitted to y_i = i / n of the sorted sample, then each leaf to
+// its samples' targets normalised to the leaf's y range.  Training is full
+// batch, projected Adam (slopes kept >= 0 so the model stays monotone),
+// with the step size decayed to 1% over the epochs.  Residual arithmetic
+// is fp64; parameters are fp32.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/pyg_learned.h"
+#include "primitives.cuh"
+
+struct pyg_cdf {
+    int L = 0;
+    double key_lo = 0, key_scale = 0;
+    int64_t kmin = 0, kmax = 0;
+    float a0 = 1, b0 = 0;
+    std::vector<float> la, lb;      // leaf slope / intercept
+    std::vector<double> ylo, yhi;   // leaf target range
+    float* d_params = nullptr;      // device: a0, b0, then (a, b) per leaf
+    double* d_yr = nullptr;         // device: (ylo, yhi) per leaf
+    int64_t n_sample = 0, distinct = 0, f1 = 0;
+};
+
+namespace pyg {
+
+constexpr int CDF_THREADS = 256;
+
+struct LeafStat {
+    unsigned long long lo, hi;  // first index, last index + 1 (lo = ~0 when empty)
+};
+
+__device__ __forceinline__ double norm_key(int64_t k, double lo, double scale)
+{
+    return (double)(float)(((double)k - lo) * scale);
+}
+
+// Root forward + backward over the sorted sample: acc[0] += e^2,
+// acc[1] += e*x, acc[2] += e with e = a0*x + b0 - y.
+__global__ void __launch_bounds__(CDF_THREADS) root_fwd_bwd_kernel(const int64_t* __restrict__ keys, int64_t n,
+                                                                   double lo, double scale,
+                                                                   const float* __restrict__ params,
+                                                                   double* __restrict__ acc)
+{
+    const double a0 = params[0], b0 = params[1];
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double x = norm_key(keys[i], lo, scale);
+        double y = (double)i / (double)n;
+        double e = a0 * x + b0 - y;
+        s0 += e * e;
+        s1 += e * x;
+        s2 += e;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&acc[0], s0);
+        atomicAdd(&acc[1], s1);
+        atomicAdd(&acc[2], s2);
+    }
+}
+
+// Adam step on `count` parameters with gradient g[i] = gscale[i/2] * raw[i]
+// (raw accumulated by a backward kernel); slopes (even i) projected to >= 0.
+// Zeroes the raw gradient for the next epoch.
+__global__ void adam_kernel(float* __restrict__ p, double* __restrict__ raw, const double* __restrict__ gscale,
+                            float* __restrict__ m, float* __restrict__ v, int count, float lr, int t)
+{
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        double gs = gscale[i >> 1];
+        float g = (float)(raw[i] * gs);
+        raw[i] = 0;
+        if (gs == 0) continue;
+        float mi = b1 * m[i] + (1 - b1) * g;
+        float vi = b2 * v[i] + (1 - b2) * g * g;
+        m[i] = mi;
+        v[i] = vi;
+        float mh = mi / (1 - powf(b1, (float)t));
+        float vh = vi / (1 - powf(b2, (float)t));
+        float q = p[i] - lr * mh / (sqrtf(vh) + eps);
+        if ((i & 1) == 0 && q < 0) q = 0;
+        p[i] = q;
+    }
+}
+
+// Leaf of every sample and each leaf's index range.
+__global__ void assign_kernel(const int64_t* __restrict__ keys, int64_t n, double lo, double scale,
+                              const float* __restrict__ params, int L, int* __restrict__ leaf, double* __restrict__ u,
+                              LeafStat* __restrict__ st)
+{
+    const double a0 = params[0], b0 = params[1];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double x = norm_key(keys[i], lo, scale);
+        double r = a0 * x + b0;
+        double fl = floor(L * r);
+        int l = fl < 0 ? 0 : (fl > L - 1 ? L - 1 : (int)fl);
+        double uu = L * r - l;
+        uu = uu < 0 ? 0 : (uu > 1 ? 1 : uu);
+        leaf[i] = l;
+        u[i] = uu;
+        atomicMin(&st[l].lo, (unsigned long long)i);
+        atomicMax(&st[l].hi, (unsigned long long)(i + 1));
+    }
+}
+
+__global__ void leaf_range_kernel(const LeafStat* __restrict__ st, int64_t n, int L, double* __restrict__ yr,
+                                  double* __restrict__ gscale)
+{
+    for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < L; l += gridDim.x * blockDim.x) {
+        bool empty = st[l].lo == ~0ULL;
+        double ylo = empty ? 0 : (double)st[l].lo / (double)n;
+        double yhi = empty ? 0 : (double)st[l].hi / (double)n;
+        yr[2 * l] = ylo;
+        yr[2 * l + 1] = yhi;
+        // d/dparam of (1/L) * mean over the leaf: (1/L) * 2 / n_l.
+        gscale[1 + l] = empty ? 0 : 2.0 / ((double)(st[l].hi - st[l].lo) * (double)L);
+    }
+}
+
+// Leaf forward: residual g_i = a_l u_i + b_l - t_i and loss sum per leaf.
+__global__ void __launch_bounds__(CDF_THREADS) leaf_forward_kernel(int64_t n, const int* __restrict__ leaf,
+                                                                   const double* __restrict__ u,
+                                                                   const double* __restrict__ yr,
+                                                                   const float* __restrict__ params,
+                                                                   double* __restrict__ g, double* __restrict__ lsum)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int l = leaf[i];
+        double y = (double)i / (double)n;
+        double ylo = yr[2 * l], yhi = yr[2 * l + 1];
+        double t = yhi > ylo ? (y - ylo) / (yhi - ylo) : 0.0;
+        double e = (double)params[2 + 2 * l] * u[i] + (double)params[3 + 2 * l] - t;
+        g[i] = e;
+        if (lsum) atomicAdd(&lsum[l], e * e);
+    }
+}
+
+// Leaf backward: raw[2l] += g u, raw[2l+1] += g (summed per leaf; samples
+// are sorted so a warp is usually inside one leaf and reduces first).
+__global__ void __launch_bounds__(CDF_THREADS) leaf_backward_kernel(int64_t n, const int* __restrict__ leaf,
+                                                                    const double* __restrict__ u,
+                                                                    const double* __restrict__ g,
+                                                                    double* __restrict__ raw)
+{
+    const unsigned lane = threadIdx.x & 31;
+    for (int64_t wb = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u); wb < n;
+         wb += (int64_t)gridDim.x * blockDim.x) {
+        int64_t i = wb + lane;
+        bool valid = i < n;
+        int l = valid ? leaf[i] : -1;
+        double ga = valid ? g[i] * u[i] : 0, gb = valid ? g[i] : 0;
+        int l0 = __shfl_sync(0xffffffffu, l, 0);
+        bool uniform = __all_sync(0xffffffffu, !valid || l == l0);
+        if (uniform) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                ga += __shfl_xor_sync(0xffffffffu, ga, o);
+                gb += __shfl_xor_sync(0xffffffffu, gb, o);
+            }
+            if (lane == 0) {
+                atomicAdd(&raw[2 + 2 * l0], ga);
+                atomicAdd(&raw[3 + 2 * l0], gb);
+            }
+        } else if (valid) {
+            atomicAdd(&raw[2 + 2 * l], ga);
+            atomicAdd(&raw[3 + 2 * l], gb);
+        }
+    }
+}
+
+__global__ void root_to_raw_kernel(const double* __restrict__ acc, double* __restrict__ raw)
+{
+    raw[0] = acc[1];
+    raw[1] = acc[2];
+}
+
+__global__ void predict_kernel(const int64_t* __restrict__ keys, int64_t n, double lo, double scale,
+                               const float* __restrict__ params, const double* __restrict__ yr, int L,
+                               float* __restrict__ out)
+{
+    const double a0 = params[0], b0 = params[1];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double x = norm_key(keys[i], lo, scale);
+        double r = a0 * x + b0;
+        double fl = floor(L * r);
+        int l = fl < 0 ? 0 : (fl > L - 1 ? L - 1 : (int)fl);
+        double uu = L * r - l;
+        uu = uu < 0 ? 0 : (uu > 1 ? 1 : uu);
+        double f = (double)params[2 + 2 * l] * uu + (double)params[3 + 2 * l];
+        f = f < 0 ? 0 : (f > 1 ? 1 : f);
+        out[i] = (float)(yr[2 * l] + (yr[2 * l + 1] - yr[2 * l]) * f);
+    }
+}
+
+__global__ void run_stats_kernel(const int64_t* __restrict__ k, int64_t n, unsigned long long* out)
+{
+    unsigned long long d = 0, f1 = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        bool start = i == 0 || k[i] != k[i - 1];
+        bool end = i == n - 1 || k[i] != k[i + 1];
+        d += start;
+        f1 += start && end;
+    }
+    d = warp_sum_u64(d);
+    f1 = warp_sum_u64(f1);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&out[0], d);
+        atomicAdd(&out[1], f1);
+    }
+}
+
+__global__ void to_signed_kernel(const uint64_t* __restrict__ in, int64_t n, int64_t* __restrict__ out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = from_sortable(in[i]);
+}
+
+__global__ void to_sortable_kernel(const int64_t* __restrict__ in, int64_t n, uint64_t* __restrict__ out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = to_sortable(in[i]);
+}
+
+// Sorted copy of n device keys into *sorted (device, caller frees).
+int sort_keys(pyg_ctx* ctx, const int64_t* keys, int64_t n, int64_t** sorted)
+{
+    uint64_t* buf;
+    int rc = dalloc(ctx, (void**)&buf, (size_t)2 * (n > 0 ? n : 1) * 8);
+    if (rc) return rc;
+    int g = grid_for(ctx, n, 256, 4, 8);
+    if (n > 0) {
+        to_sortable_kernel<<<g, 256, 0, ctx->stream>>>(keys, n, buf);
+        PYG_LAUNCHED(ctx);
+    }
+    int b = 0, e = 0, alt = 0;
+    if (!(rc = key_bit_range(ctx, buf, n, &b, &e))) rc = radix_sort_pairs(ctx, buf, nullptr, buf + n, nullptr, n, b, e, &alt);
+    if (rc) {
+        dfree(ctx, buf);
+        return rc;
+    }
+    if ((rc = dalloc(ctx, (void**)sorted, (size_t)(n > 0 ? n : 1) * 8))) {
+        dfree(ctx, buf);
+        return rc;
+    }
+    if (n > 0) {
+        to_signed_kernel<<<g, 256, 0, ctx->stream>>>(alt ? buf + n : buf, n, *sorted);
+        PYG_LAUNCHED(ctx);
+    }
+    dfree(ctx, buf);
+    return PYG_OK;
+}
+
+// Device workspace for one forward/backward pass over a sorted sample.
+struct CdfWork {
+    int* leaf = nullptr;
+    double* u = nullptr;
+    double* g = nullptr;
+    double* raw = nullptr;     // 2 + 2L raw gradient sums
+    double* gscale = nullptr;  // 1 + L gradient scales (root, leaves)
+    double* acc = nullptr;     // root: e^2, e x, e ; then per-leaf loss sums (L)
+    LeafStat* st = nullptr;
+    void release(pyg_ctx* ctx)
+    {
+        dfree(ctx, leaf); dfree(ctx, u); dfree(ctx, g); dfree(ctx, raw); dfree(ctx, gscale); dfree(ctx, acc);
+        dfree(ctx, st);
+    }
+    int alloc(pyg_ctx* ctx, int64_t n, int L)
+    {
+        int rc;
+        if ((rc = dalloc(ctx, (void**)&leaf, (size_t)n * 4))) return rc;
+        if ((rc = dalloc(ctx, (void**)&u, (size_t)n * 8))) return rc;
+        if ((rc = dalloc(ctx, (void**)&g, (size_t)n * 8))) return rc;
+        if ((rc = dalloc(ctx, (void**)&raw, (size_t)(2 + 2 * L) * 8))) return rc;
+        if ((rc = dalloc(ctx, (void**)&gscale, (size_t)(1 + L) * 8))) return rc;
+        if ((rc = dalloc(ctx, (void**)&acc, (size_t)(3 + L) * 8))) return rc;
+        if ((rc = dalloc(ctx, (void**)&st, (size_t)L * sizeof(LeafStat)))) return rc;
+        PYG_CUDA(cudaMemsetAsync(raw, 0, (size_t)(2 + 2 * L) * 8, ctx->stream));
+        return PYG_OK;
+    }
+};
+
+// Assigns leaves with the current root and computes leaf target ranges and
+// gradient scales.
+static int cdf_assign(pyg_ctx* ctx, CdfWork& w, const int64_t* keys, int64_t n, int L, double lo, double scale,
+                      const float* d_params, double* d_yr)
+{
+    PYG_CUDA(cudaMemsetAsync(w.st, 0xFF, (size_t)L * sizeof(LeafStat), ctx->stream));
+    // hi must start at 0 for atomicMax: set every second word to zero.
+    std::vector<LeafStat> init(L);
+    for (auto& s : init) { s.lo = ~0ULL; s.hi = 0; }
+    PYG_CUDA(cudaMemcpyAsync(w.st, init.data(), (size_t)L * sizeof(LeafStat), cudaMemcpyHostToDevice, ctx->stream));
+    int gr = grid_for(ctx, n, CDF_THREADS, 4, 8);
+    assign_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(keys, n, lo, scale, d_params, L, w.leaf, w.u, w.st);
+    PYG_LAUNCHED(ctx);
+    leaf_range_kernel<<<grid_for(ctx, L, 256, 1, 4), 256, 0, ctx->stream>>>(w.st, n, L, d_yr, w.gscale);
+    PYG_LAUNCHED(ctx);
+    PYG_CUDA(cudaStreamSynchronize(ctx->stream));  // keeps `init` alive until the copy ran
+    return PYG_OK;
+}
+
+}  // namespace pyg
+
+using namespace pyg;
+
+extern "C" {
+
+int pyg_cdf_train(pyg_ctx* ctx, const int64_t* sample_keys, int64_t n, const pyg_cdf_train_opts* opts, pyg_cdf** out)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out || !opts || n < 2 || !sample_keys || opts->leaves < 1 || opts->leaves > (1 << 20) || opts->epochs < 1) {
+        set_error("pyg_cdf_train: need >= 2 sample keys, 1..2^20 leaves, >= 1 epoch");
+        return PYG_ERR_ARG;
+    }
+    *out = nullptr;
+    const int L = opts->leaves;
+    int64_t* sorted = nullptr;
+    if ((rc = sort_keys(ctx, sample_keys, n, &sorted))) return rc;
+    pyg_cdf* m = new pyg_cdf();
+    m->L = L;
+    m->n_sample = n;
+    CdfWork w;
+    float* adam = nullptr;  // m and v for 2 + 2L params
+    int64_t ends[2];
+    unsigned long long* hs = (unsigned long long*)ctx->pinned + 128;
+    do {
+        if ((rc = w.alloc(ctx, n, L))) break;
+        if ((rc = dalloc(ctx, (void**)&m->d_params, (size_t)(2 + 2 * L) * 4))) break;
+        if ((rc = dalloc(ctx, (void**)&m->d_yr, (size_t)2 * L * 8))) break;
+        if ((rc = dalloc(ctx, (void**)&adam, (size_t)2 * (2 + 2 * L) * 4))) break;
+        PYG_CUDA(cudaMemcpyAsync(ends, sorted, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(ends + 1, sorted + n - 1, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        unsigned long long* dstat = ctx->dcounters + 80;
+        PYG_CUDA(cudaMemsetAsync(dstat, 0, 16, ctx->stream));
+        run_stats_kernel<<<grid_for(ctx, n, 256, 4, 8), 256, 0, ctx->stream>>>(sorted, n, dstat);
+        PYG_LAUNCHED(ctx);
+        PYG_CUDA(cudaMemcpyAsync(hs, dstat, 16, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        m->kmin = ends[0];
+        m->kmax = ends[1];
+        m->distinct = (int64_t)hs[0];
+        m->f1 = (int64_t)hs[1];
+        m->key_lo = (double)m->kmin;
+        m->key_scale = m->kmax > m->kmin ? 1.0 / ((double)m->kmax - (double)m->kmin) : 0.0;
+
+        // Initial parameters: root y = x, leaves t = u.
+        std::vector<float> p(2 + 2 * L);
+        p[0] = 1.f;
+        p[1] = 0.f;
+        for (int l = 0; l < L; ++l) {
+            p[2 + 2 * l] = 1.f;
+            p[3 + 2 * l] = 0.f;
+        }
+        PYG_CUDA(cudaMemcpyAsync(m->d_params, p.data(), p.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+        PYG_CUDA(cudaMemsetAsync(adam, 0, (size_t)2 * (2 + 2 * L) * 4, ctx->stream));
+        double root_scale = 2.0 / (double)n;
+        PYG_CUDA(cudaMemcpyAsync(w.gscale, &root_scale, 8, cudaMemcpyHostToDevice, ctx->stream));
+        int gr = grid_for(ctx, n, CDF_THREADS, 4, 8);
+        const int E = opts->epochs;
+        // Root: forward+backward, then Adam on (a0, b0).
+        for (int e = 1; e <= E; ++e) {
+            float lr = opts->lr * powf(0.01f, (float)(e - 1) / (float)E);
+            PYG_CUDA(cudaMemsetAsync(w.acc, 0, 24, ctx->stream));
+            root_fwd_bwd_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(sorted, n, m->key_lo, m->key_scale, m->d_params, w.acc);
+            root_to_raw_kernel<<<1, 1, 0, ctx->stream>>>(w.acc, w.raw);
+            adam_kernel<<<1, 32, 0, ctx->stream>>>(m->d_params, w.raw, w.gscale, adam, adam + 2 + 2 * L, 2, lr, e);
+            ctx->launches += 3;
+        }
+        PYG_CUDA(cudaGetLastError());
+        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        if ((rc = cdf_assign(ctx, w, sorted, n, L, m->key_lo, m->key_scale, m->d_params, m->d_yr))) break;
+        // Leaves: forward (residuals), backward (per-leaf gradient sums), Adam.
+        int ga = grid_for(ctx, 2 + 2 * L, 256, 1, 4);
+        for (int e = 1; e <= E; ++e) {
+            float lr = opts->lr * powf(0.01f, (float)(e - 1) / (float)E);
+            leaf_forward_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(n, w.leaf, w.u, m->d_yr, m->d_params, w.g, nullptr);
+            leaf_backward_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(n, w.leaf, w.u, w.g, w.raw);
+            // Root gradient entries are zero here; Adam skips scale-0 params.
+            adam_kernel<<<ga, 256, 0, ctx->stream>>>(m->d_params + 2, w.raw + 2, w.gscale + 1, adam + 2,
+                                                     adam + 2 + 2 * L + 2, 2 * L, lr, e);
+            ctx->launches += 3;
+        }
+        PYG_CUDA(cudaGetLastError());
+        // Host copies for splitter inversion.
+        PYG_CUDA(cudaMemcpyAsync(p.data(), m->d_params, p.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        std::vector<double> yr(2 * L);
+        PYG_CUDA(cudaMemcpyAsync(yr.data(), m->d_yr, yr.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        m->a0 = p[0];
+        m->b0 = p[1];
+        m->la.resize(L);
+        m->lb.resize(L);
+        m->ylo.resize(L);
+        m->yhi.resize(L);
+        for (int l = 0; l < L; ++l) {
+            m->la[l] = p[2 + 2 * l];
+            m->lb[l] = p[3 + 2 * l];
+            m->ylo[l] = yr[2 * l];
+            m->yhi[l] = yr[2 * l + 1];
+        }
+        rc = PYG_OK;
+    } while (0);
+    w.release(ctx);
+    dfree(ctx, adam);
+    dfree(ctx, sorted);
+    if (rc) {
+        pyg_cdf_free(ctx, m);
+        return rc;
+    }
+    *out = m;
+    return PYG_OK;
+}
+
+int pyg_cdf_free(pyg_ctx* ctx, pyg_cdf* m)
+{
+    if (!m) return PYG_OK;
+    if (ctx) {
+        dfree(ctx, m->d_params);
+        dfree(ctx, m->d_yr);
+    }
+    delete m;
+    return PYG_OK;
+}
+
+int pyg_cdf_splitters(pyg_ctx* ctx, const pyg_cdf* m, int32_t fanout, int64_t* out)
+{
+    (void)ctx;
+    if (!m || fanout < 1 || (fanout > 1 && !out)) {
+        set_error("pyg_cdf_splitters: bad arguments");
+        return PYG_ERR_ARG;
+    }
+    const int L = m->L;
+    // Non-empty leaves in order (their y ranges are ordered and disjoint).
+    std::vector<int> ne;
+    for (int l = 0; l < L; ++l)
+        if (m->yhi[l] > m->ylo[l]) ne.push_back(l);
+    const int64_t past = m->kmax == INT64_MAX ? INT64_MAX : m->kmax + 1;  // past the largest sample key
+    int64_t prev = m->kmin;
+    for (int j = 1; j < fanout; ++j) {
+        double q = (double)j / (double)fanout;
+        int64_t key;
+        if (ne.empty() || m->key_scale == 0) {
+            key = past;
+        } else {
+            // Leaf whose y range contains q.
+            size_t lo = 0, hi = ne.size();
+            while (lo + 1 < hi) {
+                size_t mid = (lo + hi) / 2;
+                if (m->ylo[ne[mid]] <= q) lo = mid;
+                else hi = mid;
+            }
+            int l = ne[lo];
+            double t = (q - m->ylo[l]) / (m->yhi[l] - m->ylo[l]);
+            double a = m->la[l], b = m->lb[l];
+            double uu = a > 0 ? (t - b) / a : 0.0;
+            uu = std::min(1.0, std::max(0.0, uu));
+            double r = ((double)l + uu) / (double)L;
+            double x = m->a0 > 0 ? (r - (double)m->b0) / (double)m->a0 : 0.0;
+            double kf = m->key_lo + x / m->key_scale;
+            if (!(kf > (double)m->kmin)) key = m->kmin;
+            else if (kf >= (double)m->kmax) key = past;
+            else key = (int64_t)ceil(kf);
+        }
+        if (key < prev) key = prev;
+        out[j - 1] = key;
+        prev = key;
+    }
+    return PYG_OK;
+}
+
+int pyg_cdf_predict(pyg_ctx* ctx, const pyg_cdf* m, const int64_t* keys, int64_t n, float* out)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!m || n < 0 || (n > 0 && (!keys || !out))) {
+        set_error("pyg_cdf_predict: bad arguments");
+        return PYG_ERR_ARG;
+    }
+    if (n == 0) return PYG_OK;
+    predict_kernel<<<grid_for(ctx, n, 256, 4, 8), 256, 0, ctx->stream>>>(keys, n, m->key_lo, m->key_scale,
+                                                                        m->d_params, m->d_yr, m->L, out);
+    PYG_LAUNCHED(ctx);
+    return PYG_OK;
+}
+
+int pyg_cdf_params(pyg_ctx* ctx, const pyg_cdf* m, float* params, int32_t cap, double* key_lo, double* key_scale)
+{
+    (void)ctx;
+    if (!m || !params || cap < 2 + 2 * m->L) {
+        set_error("pyg_cdf_params: need room for %d floats", m ? 2 + 2 * m->L : 0);
+        return PYG_ERR_ARG;
+    }
+    params[0] = m->a0;
+    params[1] = m->b0;
+    for (int l = 0; l < m->L; ++l) {
+        params[2 + 2 * l] = m->la[l];
+        params[3 + 2 * l] = m->lb[l];
+    }
+    if (key_lo) *key_lo = m->key_lo;
+    if (key_scale) *key_scale = m->key_scale;
+    return PYG_OK;
+}
+
+int pyg_cdf_loss_grad(pyg_ctx* ctx, const int64_t* sorted_keys, int64_t n, int32_t L, const float* params_host,
+                      double key_lo, double key_scale, double* loss, float* grad_host)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!sorted_keys || n < 1 || L < 1 || !params_host || !loss || !grad_host) {
+        set_error("pyg_cdf_loss_grad: bad arguments");
+        return PYG_ERR_ARG;
+    }
+    CdfWork w;
+    float* dp = nullptr;
+    double* dyr = nullptr;
+    do {
+        if ((rc = w.alloc(ctx, n, L))) break;
+        if ((rc = dalloc(ctx, (void**)&dp, (size_t)(2 + 2 * L) * 4))) break;
+        if ((rc = dalloc(ctx, (void**)&dyr, (size_t)2 * L * 8))) break;
+        PYG_CUDA(cudaMemcpyAsync(dp, params_host, (size_t)(2 + 2 * L) * 4, cudaMemcpyHostToDevice, ctx->stream));
+        PYG_CUDA(cudaMemsetAsync(w.acc, 0, (size_t)(3 + L) * 8, ctx->stream));
+        int gr = grid_for(ctx, n, CDF_THREADS, 4, 8);
+        root_fwd_bwd_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(sorted_keys, n, key_lo, key_scale, dp, w.acc);
+        PYG_LAUNCHED(ctx);
+        if ((rc = cdf_assign(ctx, w, sorted_keys, n, L, key_lo, key_scale, dp, dyr))) break;
+        leaf_forward_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(n, w.leaf, w.u, dyr, dp, w.g, w.acc + 3);
+        PYG_LAUNCHED(ctx);
+        leaf_backward_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(n, w.leaf, w.u, w.g, w.raw);
+        PYG_LAUNCHED(ctx);
+        std::vector<double> acc(3 + L), raw(2 + 2 * L), gs(1 + L);
+        PYG_CUDA(cudaMemcpyAsync(acc.data(), w.acc, acc.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(raw.data(), w.raw, raw.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(gs.data(), w.gscale, gs.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        double total = acc[0] / (double)n;
+        grad_host[0] = (float)(2.0 / n * acc[1]);
+        grad_host[1] = (float)(2.0 / n * acc[2]);
+        for (int l = 0; l < L; ++l) {
+            // gs[1+l] = 2 / (n_l L); the leaf loss mean is (gs/2) * sum e^2.
+            total += 0.5 * gs[1 + l] * acc[3 + l];
+            grad_host[2 + 2 * l] = (float)(gs[1 + l] * raw[2 + 2 * l]);
+            grad_host[3 + 2 * l] = (float)(gs[1 + l] * raw[3 + 2 * l]);
+        }
+        *loss = total;
+        rc = PYG_OK;
+    } while (0);
+    w.release(ctx);
+    dfree(ctx, dp);
+    dfree(ctx, dyr);
+    return rc;
+}
+
+__global__ void gather_quantiles_kernel(const int64_t* __restrict__ sorted, int64_t n, int fanout,
+                                        int64_t* __restrict__ out)
+{
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x + 1; j < fanout; j += gridDim.x * blockDim.x) {
+        int64_t idx = (int64_t)(((__int128)j * n + fanout - 1) / fanout);  // ceil(j n / F)
+        int64_t last = sorted[n - 1];
+        out[j - 1] = idx < n ? sorted[idx] : (last == INT64_MAX ? last : last + 1);
+    }
+}
+
+int pyg_sampled_splitters(pyg_ctx* ctx, const int64_t* sample_keys, int64_t n, int32_t fanout, int64_t* out)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!sample_keys || n < 1 || fanout < 1 || (fanout > 1 && !out)) {
+        set_error("pyg_sampled_splitters: bad arguments");
+        return PYG_ERR_ARG;
+    }
+    if (fanout == 1) return PYG_OK;
+    int64_t* sorted = nullptr;
+    if ((rc = sort_keys(ctx, sample_keys, n, &sorted))) return rc;
+    int64_t* d;
+    if ((rc = dalloc(ctx, (void**)&d, (size_t)(fanout - 1) * 8))) {
+        dfree(ctx, sorted);
+        return rc;
+    }
+    gather_quantiles_kernel<<<grid_for(ctx, fanout, 256, 1, 4), 256, 0, ctx->stream>>>(sorted, n, fanout, d);
+    PYG_LAUNCHED(ctx);
+    PYG_CUDA(cudaMemcpyAsync(out, d, (size_t)(fanout - 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+    dfree(ctx, d);
+    dfree(ctx, sorted);
+    return PYG_OK;
+}
+
+int pyg_cdf_estimate_distinct(pyg_ctx* ctx, const pyg_cdf* m, int64_t population, int64_t* out)
+{
+    (void)ctx;
+    if (!m || !out || population < 0) {
+        set_error("pyg_cdf_estimate_distinct: bad arguments");
+        return PYG_ERR_ARG;
+    }
+    // GEE (Charikar, Chaudhuri, Motwani, Narasayya, PODS 2000):
+    // D = sqrt(N / n) * f1 + (d - f1).
+    double r = m->n_sample > 0 ? sqrt((double)population / (double)m->n_sample) : 1.0;
+    double est = r * (double)m->f1 + (double)(m->distinct - m->f1);
+    if (est > (double)population) est = (double)population;
+    if (est < (double)m->distinct) est = (double)m->distinct;
+    *out = (int64_t)ceil(est);
+    return PYG_OK;
+}
+
+}  // extern "C"

@@ -162,6 +162,7 @@ int pyg_ctx_create(int device, pyg_ctx** out)
         return PYG_ERR_NO_DEVICE;
     }
     pyg_ctx* c = new pyg_ctx();
+    memset(c, 0, sizeof(*c));
     c->device = device;
     c->sm_count = prop.multiProcessorCount;
     c->launches = 0;
@@ -176,6 +177,11 @@ int pyg_ctx_create(int device, pyg_ctx** out)
     c->pinned_bytes = 1 << 16;
     e = cudaMallocHost(&c->pinned, c->pinned_bytes);
     if (e == cudaSuccess) e = cudaMalloc((void**)&c->dcounters, 4096);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+        e = cudaEventCreateWithFlags(&c->copied[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->consumed[i], cudaEventDisableTiming);
+    }
     if (e != cudaSuccess) {
         cudaStreamDestroy(c->own_stream);
         if (c->pinned) cudaFreeHost(c->pinned);
@@ -197,6 +203,12 @@ int pyg_ctx_destroy(pyg_ctx* ctx)
     if (!ctx) return PYG_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    cudaStreamSynchronize(ctx->copy_stream);
+    for (int i = 0; i < 2; ++i) {
+        cudaEventDestroy(ctx->copied[i]);
+        cudaEventDestroy(ctx->consumed[i]);
+    }
+    cudaStreamDestroy(ctx->copy_stream);
     cudaFree(ctx->dcounters);
     cudaFreeHost(ctx->pinned);
     cudaStreamDestroy(ctx->own_stream);

@@ -11,8 +11,11 @@
 // linear probing.
 #include <string.h>
 
+#include <vector>
+
 #include "pyg_internal.cuh"
 #include "hashtable.cuh"
+#include "partition.cuh"
 
 namespace pyg {
 
@@ -144,9 +147,11 @@ __device__ __forceinline__ void block_flush(uint64_t* acc, int nacc, unsigned lo
 }
 
 // Fast path: 16-byte (int64 key, int64 value) probe tuples against a
-// 16-byte-slot AGGREGATE table (one int64 build payload).  want_b / want_p
-// select which of the build sum and the probe sum are accumulated.
-template <int UNROLL>
+// 16-byte-slot AGGREGATE table (one int64 build payload); accumulates the
+// match count, the build-payload sum and the probe-value sum.  FILLERS:
+// tuples whose key is the empty marker are padding (skipped) rather than
+// real keys (matched against the side list).
+template <int UNROLL, bool FILLERS>
 __global__ void __launch_bounds__(256) probe_agg16_kernel(const longlong2* __restrict__ S, int64_t n,
                                                           const ulonglong2* __restrict__ slots, uint64_t cap,
                                                           const unsigned long long* __restrict__ counts,
@@ -176,6 +181,7 @@ __global__ void __launch_bounds__(256) probe_agg16_kernel(const longlong2* __res
             if (idx >= n) continue;
             uint64_t k = (uint64_t)t[u].x;
             if (k == kEmptyKey) {
+                if (FILLERS) continue;
                 for (int64_t j = 0; j < nside; ++j)
                     if (side[2 * j] == k) {
                         ++cnt;
@@ -400,6 +406,258 @@ static int fill_probe_args(pyg_ctx* ctx, const pyg_hashtable* ht, const pyg_rel*
     return PYG_OK;
 }
 
+
+// 16-byte fast layout: (int64 key @0, int64 value @8) probe tuples, a
+// one-payload AGGREGATE table, projection over {B$payload, P$1}.
+static bool fast16_layout(const pyg_hashtable* ht, const ProbeArgs& a, const pyg_rel* probe, int nproj, int* fb,
+                          int* fp)
+{
+    bool fast = a.agg && ht->W == 2 && probe->tuple_bytes == 16 && a.ks.nkeys == 1 && a.ks.off0 == 0 &&
+                a.ks.type0 == PYG_INT64 && nproj <= 2 && ht->pay_types[0] == PYG_INT64;
+    *fb = *fp = -1;
+    for (int p = 0; fast && p < nproj; ++p) {
+        if (a.pside[p] == 0 && a.ptype[p] == PYG_INT64 && *fb < 0) *fb = p;
+        else if (a.pside[p] == 1 && a.poff[p] == 8 && a.ptype[p] == PYG_INT64 && *fp < 0) *fp = p;
+        else fast = false;
+    }
+    return fast;
+}
+
+static void fill_result(pyg_join_result* out, const unsigned long long* h, const ProbeArgs& a, int nproj, bool fast,
+                        int fb)
+{
+    memset(out, 0, sizeof(*out));
+    out->count = (int64_t)h[0];
+    for (int p = 0; p < nproj; ++p) {
+        uint64_t v;
+        if (fast) v = (p == fb) ? h[1] : h[2];
+        else v = h[1 + p];
+        out->sums[p] = a.ptype[p] == PYG_INT32 ? (int64_t)(int32_t)(uint32_t)v : (int64_t)v;
+    }
+}
+
+static int launch_probe16(pyg_ctx* ctx, const pyg_hashtable* ht, const longlong2* S, int64_t n, bool fillers,
+                          unsigned long long* acc)
+{
+    if (n <= 0) return PYG_OK;
+    int threads = 256;
+    int grid = grid_for(ctx, n, threads, 4, 8);
+    if (fillers)
+        probe_agg16_kernel<4, true><<<grid, threads, 0, ctx->stream>>>(S, n, (const ulonglong2*)ht->slots, ht->cap,
+                                                                       ht->counts, ht->side, ht->nside, acc);
+    else
+        probe_agg16_kernel<4, false><<<grid, threads, 0, ctx->stream>>>(S, n, (const ulonglong2*)ht->slots, ht->cap,
+                                                                        ht->counts, ht->side, ht->nside, acc);
+    PYG_LAUNCHED(ctx);
+    return PYG_OK;
+}
+
+static int probe16_stream_host(pyg_ctx* ctx, const pyg_hashtable* ht, const longlong2* host, int64_t n,
+                               unsigned long long* acc)
+{
+    const int64_t chunk = (int64_t)1 << 25;  // 512 MiB of tuples per buffer
+    int64_t per = n < chunk ? n : chunk;
+    longlong2* buf[2] = {nullptr, nullptr};
+    int rc = dalloc(ctx, (void**)&buf[0], (size_t)per * 16);
+    if (!rc) rc = dalloc(ctx, (void**)&buf[1], (size_t)per * 16);
+    if (!rc) {
+        // Buffers become usable on the copy stream once allocated.
+        cudaEventRecord(ctx->consumed[0], ctx->stream);
+        cudaEventRecord(ctx->consumed[1], ctx->stream);
+        int64_t i = 0;
+        for (int64_t off = 0; off < n && !rc; off += per, ++i) {
+            int b = (int)(i & 1);
+            int64_t len = n - off < per ? n - off : per;
+            cudaStreamWaitEvent(ctx->copy_stream, ctx->consumed[b], 0);
+            cudaError_t e = cudaMemcpyAsync(buf[b], host + off, (size_t)len * 16, cudaMemcpyHostToDevice,
+                                            ctx->copy_stream);
+            if (e != cudaSuccess) {
+                rc = cuda_status(e, "probe chunk copy");
+                break;
+            }
+            cudaEventRecord(ctx->copied[b], ctx->copy_stream);
+            cudaStreamWaitEvent(ctx->stream, ctx->copied[b], 0);
+            rc = launch_probe16(ctx, ht, buf[b], len, false, acc);
+            cudaEventRecord(ctx->consumed[b], ctx->stream);
+        }
+    }
+    dfree(ctx, buf[0]);
+    dfree(ctx, buf[1]);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Hash-ordered radix join.  Build and probe relations are partitioned by
+// the top bits of mix64(key); the table's slot function (multiply-high of
+// the same hash) maps partition p to the p-th slice of the table, so a
+// partition's inserts and probes touch one L2-sized slice at a time.
+// The probe relation is partitioned in one pass (no histogram pass):
+// partition capacities come from a sample, each CTA stages a 4096-tuple
+// tile in shared memory grouped by partition and reserves space with one
+// atomic per (tile, partition), so runs are written contiguously.  Tuples
+// that do not fit (or carry the empty-marker key) go to an overflow area
+// probed separately; unused capacity is filled with empty-marker padding.
+
+constexpr int TP_THREADS = 512;
+constexpr int TP_TILE = 4096;
+
+__global__ void sample_part_hist_kernel(const longlong2* __restrict__ S, int64_t n, int64_t stride, int pbits,
+                                        unsigned long long* __restrict__ hist)
+{
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j * stride < n; j += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t k = (uint64_t)S[j * stride].x;
+        atomicAdd(&hist[mix64(k) >> (64 - pbits)], 1ULL);
+    }
+}
+
+__global__ void __launch_bounds__(TP_THREADS) tile_partition16_kernel(
+    const longlong2* __restrict__ S, int64_t n, int pbits, const unsigned long long* __restrict__ pstart,
+    const unsigned long long* __restrict__ pcap, unsigned long long* __restrict__ cursor, longlong2* __restrict__ out,
+    longlong2* __restrict__ ovf, unsigned long long* __restrict__ ovf_cursor, int64_t ovf_cap)
+{
+    extern __shared__ __align__(16) unsigned char tp_smem[];
+    const int P = 1 << pbits;
+    longlong2* stage = (longlong2*)tp_smem;
+    unsigned* hist = (unsigned*)(stage + TP_TILE);
+    unsigned* loff = hist + P;
+    unsigned long long* gbase = (unsigned long long*)(loff + P + (P & 1));
+    __shared__ unsigned warp_tot[TP_THREADS / 32];
+    __shared__ unsigned tile_n;
+    const int64_t ntiles = (n + TP_TILE - 1) / TP_TILE;
+    constexpr int PER = TP_TILE / TP_THREADS;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        for (int b = threadIdx.x; b < P; b += TP_THREADS) hist[b] = 0;
+        __syncthreads();
+        const int64_t base = tile * TP_TILE;
+        longlong2 t[PER];
+        unsigned bin[PER], rank[PER];
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            int64_t i = base + j * TP_THREADS + threadIdx.x;
+            bin[j] = 0xFFFFFFFFu;
+            if (i < n) {
+                t[j] = __ldcs(&S[i]);
+                uint64_t k = (uint64_t)t[j].x;
+                if (k == kEmptyKey) {
+                    unsigned long long o = atomicAdd(ovf_cursor, 1ULL);
+                    if ((int64_t)o < ovf_cap) ovf[o] = t[j];
+                } else {
+                    bin[j] = (unsigned)(mix64(k) >> (64 - pbits));
+                    rank[j] = atomicAdd(&hist[bin[j]], 1u);
+                }
+            }
+        }
+        __syncthreads();
+        // Exclusive scan of the tile histogram; each thread owns a run of
+        // consecutive bins.  Reserve global space per non-empty bin.
+        const int per = (P + TP_THREADS - 1) / TP_THREADS;
+        const int b0 = threadIdx.x * per;
+        unsigned local = 0;
+        for (int b = b0; b < b0 + per && b < P; ++b) local += hist[b];
+        unsigned incl = local;
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) warp_tot[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            unsigned x = lane < TP_THREADS / 32 ? warp_tot[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                unsigned v = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += v;
+            }
+            if (lane < TP_THREADS / 32) warp_tot[lane] = x;
+            if (lane == TP_THREADS / 32 - 1) tile_n = x;
+        }
+        __syncthreads();
+        unsigned run = incl - local + (w > 0 ? warp_tot[w - 1] : 0);
+        for (int b = b0; b < b0 + per && b < P; ++b) {
+            unsigned c = hist[b];
+            loff[b] = run;
+            run += c;
+            if (c) gbase[b] = atomicAdd(&cursor[b], (unsigned long long)c);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < PER; ++j)
+            if (bin[j] != 0xFFFFFFFFu) stage[loff[bin[j]] + rank[j]] = t[j];
+        __syncthreads();
+        const unsigned cnt = tile_n;
+        for (unsigned i = threadIdx.x; i < cnt; i += TP_THREADS) {
+            longlong2 v = stage[i];
+            unsigned b = (unsigned)(mix64((uint64_t)v.x) >> (64 - pbits));
+            unsigned long long g = gbase[b] + (i - loff[b]);
+            if (g < pcap[b]) {
+                __stcs(&out[pstart[b] + g], v);
+            } else {
+                unsigned long long o = atomicAdd(ovf_cursor, 1ULL);
+                if ((int64_t)o < ovf_cap) ovf[o] = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Pads [start + min(cursor, cap), start + cap) of every partition with
+// empty-marker tuples.
+__global__ void fill_gaps_kernel(longlong2* __restrict__ out, int P, const unsigned long long* __restrict__ pstart,
+                                 const unsigned long long* __restrict__ pcap,
+                                 const unsigned long long* __restrict__ cursor)
+{
+    for (int b = blockIdx.x; b < P; b += gridDim.x) {
+        unsigned long long used = cursor[b] < pcap[b] ? cursor[b] : pcap[b];
+        for (unsigned long long i = used + threadIdx.x; i < pcap[b]; i += blockDim.x)
+            out[pstart[b] + i] = make_longlong2((long long)kEmptyKey, 0);
+    }
+}
+
+// Exact partitioning of the build relation by the same hash bits (the
+// histogram / scan / scatter partitioner).
+static int partition_by_hash(pyg_ctx* ctx, const pyg_rel* r, int pbits, void* out, unsigned long long* offs)
+{
+    BucketFn f;
+    memset(&f, 0, sizeof(f));
+    f.kind = PYG_SPLIT_HASH;
+    f.fanout = 1u << pbits;
+    f.log2f = pbits;
+    return partition_device(ctx, r, 0, f, out, offs);
+}
+
+struct PhaseTimer {
+    static constexpr int N = 5;
+    cudaEvent_t ev[N] = {};
+    bool on = false;
+    void start(pyg_ctx* ctx, bool enable)
+    {
+        on = enable;
+        if (!on) return;
+        for (auto& e : ev) cudaEventCreate(&e);
+        for (auto& e : ev) cudaEventRecord(e, ctx->stream);
+    }
+    void mark(pyg_ctx* ctx, int i)
+    {
+        if (on) cudaEventRecord(ev[i], ctx->stream);
+    }
+    // Phases between consecutive marks: build-side partition, build,
+    // probe-side partition, probe.
+    void finish(pyg_join_stats* st)
+    {
+        if (!on) return;
+        cudaEventSynchronize(ev[N - 1]);
+        float ms[N - 1];
+        for (int i = 0; i + 1 < N; ++i) cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+        st->build_partition_ms = ms[0];
+        st->build_ms = ms[1];
+        st->probe_partition_ms = ms[2];
+        st->probe_ms = ms[3];
+        for (auto& e : ev) cudaEventDestroy(e);
+    }
+};
+
 }  // namespace pyg
 
 using namespace pyg;
@@ -567,46 +825,39 @@ int pyg_hashjoin_probe_agg(pyg_ctx* ctx, const pyg_hashtable* ht, const pyg_rel*
     if ((rc = check_rel(probe, "probe"))) return rc;
     ProbeArgs a;
     if ((rc = fill_probe_args(ctx, ht, probe, key_cols, proj, nproj, &a))) return rc;
-    DevRel S;
-    if ((rc = S.stage(ctx, probe))) return rc;
-    a.base = (const uint8_t*)S.rel.base;
     unsigned long long* acc = ctx->dcounters + 8;
     PYG_CUDA(cudaMemsetAsync(acc, 0, (PYG_MAX_COLS + 1) * sizeof(unsigned long long), ctx->stream));
-    int threads = 256;
-    // 16-byte fast path: (int64 key @0, int64 value @8) probe tuples, a
-    // one-payload AGGREGATE table, projection over {B$payload, P$1}.
-    bool fast = a.agg && ht->W == 2 && probe->tuple_bytes == 16 && a.ks.nkeys == 1 && a.ks.off0 == 0 &&
-                a.ks.type0 == PYG_INT64 && ((uintptr_t)a.base % 16 == 0) && nproj <= 2;
     int fb = -1, fp = -1;
-    for (int p = 0; fast && p < nproj; ++p) {
-        if (a.pside[p] == 0 && a.ptype[p] == PYG_INT64 && fb < 0) fb = p;
-        else if (a.pside[p] == 1 && a.poff[p] == 8 && a.ptype[p] == PYG_INT64 && fp < 0) fp = p;
-        else fast = false;
-    }
-    if (a.n > 0) {
-        if (fast) {
-            int grid = grid_for(ctx, a.n, threads, 4, 8);
-            probe_agg16_kernel<4><<<grid, threads, 0, ctx->stream>>>(
-                (const longlong2*)a.base, a.n, (const ulonglong2*)a.slots, a.cap, a.counts, a.side, a.nside, acc);
-        } else {
-            int grid = grid_for(ctx, a.n, threads, 1, 8);
-            probe_agg_kernel<<<grid, threads, 0, ctx->stream>>>(a, acc);
+    bool fast = fast16_layout(ht, a, probe, nproj, &fb, &fp);
+    if (fast && !probe->on_device && a.n > 0) {
+        // Host probe relation: stream it through two device buffers, the
+        // copy of chunk i+1 overlapping the probe of chunk i.
+        if ((rc = probe16_stream_host(ctx, ht, (const longlong2*)probe->base, a.n, acc))) return rc;
+    } else {
+        DevRel S;
+        if ((rc = S.stage(ctx, probe))) return rc;
+        a.base = (const uint8_t*)S.rel.base;
+        if (fast && (uintptr_t)a.base % 16) fast = false;
+        if (a.n > 0) {
+            if (fast) {
+                if ((rc = launch_probe16(ctx, ht, (const longlong2*)a.base, a.n, false, acc))) {
+                    S.release(ctx);
+                    return rc;
+                }
+            } else {
+                int threads = 256;
+                int grid = grid_for(ctx, a.n, threads, 1, 8);
+                probe_agg_kernel<<<grid, threads, 0, ctx->stream>>>(a, acc);
+                PYG_LAUNCHED(ctx);
+            }
         }
-        PYG_LAUNCHED(ctx);
+        S.release(ctx);
     }
     unsigned long long* h = (unsigned long long*)ctx->pinned;
     PYG_CUDA(cudaMemcpyAsync(h, acc, (PYG_MAX_COLS + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                              ctx->stream));
-    S.release(ctx);
     PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-    memset(out, 0, sizeof(*out));
-    out->count = (int64_t)h[0];
-    for (int p = 0; p < nproj; ++p) {
-        uint64_t v;
-        if (fast) v = (p == fb) ? h[1] : h[2];
-        else v = h[1 + p];
-        out->sums[p] = a.ptype[p] == PYG_INT32 ? (int64_t)(int32_t)(uint32_t)v : (int64_t)v;
-    }
+    fill_result(out, h, a, nproj, fast, fb);
     return PYG_OK;
 }
 
@@ -653,6 +904,165 @@ int pyg_hashjoin_probe_materialize(pyg_ctx* ctx, const pyg_hashtable* ht, const 
         return PYG_ERR_CAPACITY;
     }
     return PYG_OK;
+}
+
+int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_keys, const pyg_rel* probe,
+                     const int32_t* probe_keys, int32_t nkeys, const pyg_proj* proj, int32_t nproj,
+                     const pyg_join_opts* opts, pyg_join_result* out, pyg_join_stats* stats)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out || (nproj > 0 && !proj) || nproj < 0 || nproj > PYG_MAX_COLS) {
+        set_error("pyg_hashjoin_agg: bad arguments");
+        return PYG_ERR_ARG;
+    }
+    if ((rc = check_rel(build, "build")) || (rc = check_rel(probe, "probe"))) return rc;
+    int algorithm = opts ? opts->algorithm : PYG_JOIN_AUTO;
+    float lf = (opts && opts->load_factor > 0) ? opts->load_factor : 0.5f;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    // Build columns referenced by the projection.
+    int32_t pay[PYG_MAX_COLS];
+    int npay = 0;
+    for (int p = 0; p < nproj; ++p) {
+        if (proj[p].side) continue;
+        bool seen = false;
+        for (int c = 0; c < npay; ++c) seen |= pay[c] == proj[p].col;
+        if (!seen) pay[npay++] = proj[p].col;
+    }
+    // The radix path covers 16-byte (int64 key @0, int64 payload @8)
+    // device relations with a projection over {B$1, P$1}.
+    auto is16 = [](const pyg_rel* r, const int32_t* k) {
+        return r->on_device && r->tuple_bytes == 16 && r->ncols == 2 && k && k[0] == 0 && r->col_offset[0] == 0 &&
+               r->col_type[0] == PYG_INT64 && r->col_offset[1] == 8 && r->col_type[1] == PYG_INT64 &&
+               (uintptr_t)r->base % 16 == 0;
+    };
+    bool eligible = nkeys == 1 && is16(build, build_keys) && is16(probe, probe_keys) && nproj <= 2 && npay <= 1;
+    for (int p = 0; eligible && p < nproj; ++p) eligible = proj[p].col == 1;
+    if (eligible && nproj == 2) eligible = proj[0].side != proj[1].side;
+    bool radix = eligible && (algorithm == PYG_JOIN_RADIX ||
+                              (algorithm == PYG_JOIN_AUTO && probe->ntuples >= ((int64_t)1 << 24)));
+    PhaseTimer tm;
+    if (!radix) {
+        tm.start(ctx, stats != nullptr);
+        pyg_hashtable* ht = nullptr;
+        if ((rc = pyg_hashjoin_build(ctx, build, build_keys, nkeys, pay, npay, PYG_HT_AGGREGATE, lf, &ht))) return rc;
+        tm.mark(ctx, 2);
+        tm.mark(ctx, 3);
+        rc = pyg_hashjoin_probe_agg(ctx, ht, probe, probe_keys, proj, nproj, out);
+        tm.mark(ctx, 4);
+        pyg_hashtable_free(ctx, ht);
+        if (stats) {
+            tm.finish(stats);
+            stats->algorithm = PYG_JOIN_DIRECT;
+        }
+        return rc;
+    }
+    const int64_t nR = build->ntuples, nS = probe->ntuples;
+    int pbits = opts ? opts->radix_bits : 0;
+    if (pbits <= 0) {
+        // About 8 MiB of table per partition.
+        double table = (double)nR / lf * 16.0;
+        pbits = 4;
+        while (pbits < 12 && table / (double)(1 << pbits) > 8.0 * (1 << 20)) ++pbits;
+    }
+    if (pbits < 1 || pbits > 12) {
+        set_error("pyg_hashjoin_agg: radix bits must be in [1, 12]");
+        return PYG_ERR_ARG;
+    }
+    const int P = 1 << pbits;
+    tm.start(ctx, stats != nullptr);
+    void* Rp = nullptr;
+    unsigned long long* meta = nullptr;  // roffs[P+1] | hist[P] | pstart[P] | pcap[P] | cursor[P] | ovf
+    longlong2 *Sp = nullptr, *ovf = nullptr;
+    pyg_hashtable* ht = nullptr;
+    unsigned long long* acc = ctx->dcounters + 8;
+    std::vector<unsigned long long> hh(3 * P);
+    do {
+        if ((rc = dalloc(ctx, &Rp, (size_t)(nR > 0 ? nR : 1) * 16))) break;
+        if ((rc = dalloc(ctx, (void**)&meta, (size_t)(6 * P + 2) * 8))) break;
+        unsigned long long *roffs = meta, *hist = meta + P + 1, *pstart = hist + P, *pcap = pstart + P,
+                           *cursor = pcap + P, *ovf_cursor = cursor + P;
+        if (nR > 0 && (rc = partition_by_hash(ctx, build, pbits, Rp, roffs))) break;
+        // Sample histogram of the probe side (about 2^20 samples).
+        int64_t stride = nS >> 20;
+        if (stride < 1) stride = 1;
+        PYG_CUDA(cudaMemsetAsync(hist, 0, (size_t)P * 8, ctx->stream));
+        PYG_CUDA(cudaMemsetAsync(cursor, 0, (size_t)(P + 1) * 8, ctx->stream));
+        if (nS > 0) {
+            sample_part_hist_kernel<<<grid_for(ctx, (nS + stride - 1) / stride, 256, 4, 4), 256, 0, ctx->stream>>>(
+                (const longlong2*)probe->base, nS, stride, pbits, hist);
+            PYG_LAUNCHED(ctx);
+        }
+        tm.mark(ctx, 1);
+        pyg_rel Rrel = *build;
+        Rrel.base = Rp;
+        if ((rc = pyg_hashjoin_build(ctx, &Rrel, build_keys, 1, pay, npay, PYG_HT_AGGREGATE, lf, &ht))) break;
+        tm.mark(ctx, 2);
+        // pyg_hashjoin_build synchronised the stream: the sample is ready.
+        PYG_CUDA(cudaMemcpyAsync(hh.data(), hist, (size_t)P * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        unsigned long long total = 0;
+        for (int b = 0; b < P; ++b) {
+            double est = (double)hh[b] * (double)stride;
+            unsigned long long cap = (unsigned long long)(est * 1.06) + 2048;
+            hh[P + b] = total;
+            hh[2 * P + b] = cap;
+            total += cap;
+        }
+        int64_t ovf_cap = nS / 64 + (1 << 20);
+        if ((rc = dalloc(ctx, (void**)&Sp, (size_t)total * 16))) break;
+        if ((rc = dalloc(ctx, (void**)&ovf, (size_t)ovf_cap * 16))) break;
+        PYG_CUDA(cudaMemcpyAsync(pstart, hh.data() + P, (size_t)2 * P * 8, cudaMemcpyHostToDevice, ctx->stream));
+        PYG_CUDA(cudaMemsetAsync(acc, 0, (PYG_MAX_COLS + 1) * 8, ctx->stream));
+        size_t smem = (size_t)TP_TILE * 16 + (size_t)(2 * P + 2) * 4 + (size_t)P * 8;
+        PYG_CUDA(cudaFuncSetAttribute(tile_partition16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (nS > 0) {
+            int grid = grid_for(ctx, (nS + TP_TILE - 1) / TP_TILE, 1, 1, smem > 100000 ? 1 : 2);  // one tile per unit
+            tile_partition16_kernel<<<grid, TP_THREADS, smem, ctx->stream>>>(
+                (const longlong2*)probe->base, nS, pbits, pstart, pcap, cursor, Sp, ovf, ovf_cursor, ovf_cap);
+            PYG_LAUNCHED(ctx);
+            fill_gaps_kernel<<<P < 4 * ctx->sm_count ? P : 4 * ctx->sm_count, 256, 0, ctx->stream>>>(Sp, P, pstart, pcap,
+                                                                                                    cursor);
+            PYG_LAUNCHED(ctx);
+        }
+        tm.mark(ctx, 3);
+        if (nS > 0) {
+            if ((rc = launch_probe16(ctx, ht, Sp, (int64_t)total, true, acc))) break;
+        }
+        unsigned long long* h = (unsigned long long*)ctx->pinned;
+        PYG_CUDA(cudaMemcpyAsync(h + 16, ovf_cursor, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        int64_t novf = (int64_t)h[16];
+        if (novf > ovf_cap) {
+            // The sample badly under-estimated some partitions: probe the
+            // original relation instead (same table, exact result).
+            PYG_CUDA(cudaMemsetAsync(acc, 0, (PYG_MAX_COLS + 1) * 8, ctx->stream));
+            rc = launch_probe16(ctx, ht, (const longlong2*)probe->base, nS, false, acc);
+        } else if (novf > 0) {
+            rc = launch_probe16(ctx, ht, ovf, novf, false, acc);
+        }
+        if (rc) break;
+        tm.mark(ctx, 4);
+        PYG_CUDA(cudaMemcpyAsync(h, acc, 3 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        memset(out, 0, sizeof(*out));
+        out->count = (int64_t)h[0];
+        for (int p = 0; p < nproj; ++p) out->sums[p] = (int64_t)(proj[p].side ? h[2] : h[1]);
+        if (stats) {
+            tm.finish(stats);
+            stats->algorithm = PYG_JOIN_RADIX;
+            stats->radix_bits = pbits;
+            stats->overflow_tuples = novf;
+            stats->padded_tuples = (int64_t)total;
+        }
+        rc = PYG_OK;
+    } while (0);
+    if (ht) pyg_hashtable_free(ctx, ht);
+    dfree(ctx, Rp);
+    dfree(ctx, meta);
+    dfree(ctx, Sp);
+    dfree(ctx, ovf);
+    return rc;
 }
 
 }  // extern "C"

@@ -19,6 +19,10 @@ struct pyg_ctx {
     size_t pinned_bytes;
     // Device scratch for scalar counters (zeroed per use).
     unsigned long long* dcounters;
+    // Second stream and events for overlapping host->device copies with
+    // kernels when an input relation lives in host memory.
+    cudaStream_t copy_stream;
+    cudaEvent_t copied[2], consumed[2];
 };
 
 namespace pyg {

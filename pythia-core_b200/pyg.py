@@ -39,6 +39,10 @@ SPLIT_SPLITTERS = 1
 SPLIT_RADIX = 2
 SPLIT_HASH = 3
 
+JOIN_AUTO = 0
+JOIN_DIRECT = 1
+JOIN_RADIX = 2
+
 MPSM_EXACTRANGE = 0
 MPSM_SAMPLED = 1
 MPSM_LEARNED = 2
@@ -62,6 +66,17 @@ class pyg_proj(C.Structure):
 
 class pyg_join_result(C.Structure):
     _fields_ = [("count", C.c_int64), ("sums", C.c_int64 * MAX_COLS)]
+
+
+class pyg_join_opts(C.Structure):
+    _fields_ = [("algorithm", C.c_int32), ("radix_bits", C.c_int32), ("load_factor", C.c_float),
+                ("reserved", C.c_int32)]
+
+
+class pyg_join_stats(C.Structure):
+    _fields_ = [("algorithm", C.c_int32), ("radix_bits", C.c_int32), ("build_partition_ms", C.c_double),
+                ("build_ms", C.c_double), ("probe_partition_ms", C.c_double), ("probe_ms", C.c_double), ("overflow_tuples", C.c_int64),
+                ("padded_tuples", C.c_int64)]
 
 
 class pyg_splitter(C.Structure):
@@ -123,6 +138,9 @@ SIGNATURES = [
                                          C.POINTER(pyg_join_result)]),
     ("pyg_hashjoin_probe_materialize", C.c_int, [_P, _P, C.POINTER(pyg_rel), _PI32, C.POINTER(pyg_proj), _I32, _P,
                                                  _I64, _PI64]),
+    ("pyg_hashjoin_agg", C.c_int, [_P, C.POINTER(pyg_rel), _PI32, C.POINTER(pyg_rel), _PI32, _I32, C.POINTER(pyg_proj),
+                                   _I32, C.POINTER(pyg_join_opts), C.POINTER(pyg_join_result),
+                                   C.POINTER(pyg_join_stats)]),
     ("pyg_groupby", C.c_int, [_P, C.POINTER(pyg_rel), _PI32, _I32, _I32, _I32, _I32, _I64, _P, _I64, _PI64]),
     ("pyg_partition", C.c_int, [_P, C.POINTER(pyg_rel), _I32, C.POINTER(pyg_splitter), _P, _PI64]),
     ("pyg_sort", C.c_int, [_P, C.POINTER(pyg_rel), _I32, _P]),
@@ -343,6 +361,20 @@ class Ctx:
         if rc not in (PYG_OK, PYG_ERR_CAPACITY):
             check(rc)
         return rc, cnt.value
+
+    def hashjoin_agg(self, R, rkeys, S, skeys, proj, algorithm=JOIN_AUTO, radix_bits=0, load_factor=0.5,
+                     stats=False):
+        rk = (C.c_int32 * len(rkeys))(*rkeys)
+        sk = (C.c_int32 * len(skeys))(*skeys)
+        pj = (pyg_proj * max(1, len(proj)))(*[pyg_proj(s, c) for s, c in proj])
+        o = pyg_join_opts(algorithm, radix_bits, load_factor, 0)
+        out = pyg_join_result()
+        st = pyg_join_stats()
+        r, s = R.c(), S.c()
+        check(lib().pyg_hashjoin_agg(self.h, C.byref(r), rk, C.byref(s), sk, len(rkeys), pj, len(proj), C.byref(o),
+                                     C.byref(out), C.byref(st) if stats else None))
+        res = (out.count, [out.sums[i] for i in range(len(proj))])
+        return (res, st) if stats else res
 
     # -- group-by -----------------------------------------------------
     def groupby(self, rel, key_cols, flags, sum_col, sort_by_key, expected_groups, out, capacity):

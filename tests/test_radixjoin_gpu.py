@@ -1,0 +1,77 @@
+"""One-shot join + aggregate (pyg_hashjoin_agg): the hash-ordered radix
+path and the direct path must give bit-identical count and sums, equal to
+the oracle; plus the streamed host-input probe."""
+import numpy as np
+import pytest
+
+import oracle as O
+import pyg
+from util import I64, dev_rel, host_rel, struct
+
+pytestmark = pytest.mark.gpu
+PROJ = [(0, 1), (1, 1)]
+
+
+def zipf_keys(rng, n, keys, theta):
+    if theta == 0:
+        return keys[rng.integers(0, len(keys), n)]
+    w = np.arange(1, len(keys) + 1, dtype=np.float64) ** -theta
+    c = np.cumsum(w)
+    c /= c[-1]
+    return keys[np.minimum(np.searchsorted(c, rng.random(n)), len(keys) - 1)]
+
+
+@pytest.mark.parametrize("theta", [0.0, 0.75, 1.25])
+@pytest.mark.parametrize("bits", [0, 3, 8, 12])
+def test_radix_equals_direct_equals_oracle(ctx, torch_cuda, theta, bits):
+    rng = np.random.default_rng(int(theta * 100) + bits)
+    n, m = 1 << 17, 1 << 21
+    k = rng.permutation(n).astype(np.int64) * 5 + 11
+    R = struct([k, rng.integers(-(1 << 60), 1 << 60, n)], [I64, I64])
+    fk = zipf_keys(rng, m, k, theta) + (rng.random(m) < 0.05)  # a few misses
+    S = struct([fk, rng.integers(-(1 << 60), 1 << 60, m)], [I64, I64])
+    Rd, Sd = dev_rel(torch_cuda, R, [I64, I64]), dev_rel(torch_cuda, S, [I64, I64])
+    want = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ)
+    got_r, st = ctx.hashjoin_agg(Rd, [0], Sd, [0], PROJ, pyg.JOIN_RADIX, bits, stats=True)
+    assert st.algorithm == pyg.JOIN_RADIX
+    got_d = ctx.hashjoin_agg(Rd, [0], Sd, [0], PROJ, pyg.JOIN_DIRECT)
+    assert got_r == want and got_d == want
+
+
+def test_radix_sentinel_keys_and_duplicates(ctx, torch_cuda):
+    rng = np.random.default_rng(3)
+    mn = np.iinfo(np.int64).min
+    n, m = 50000, 400000
+    k = rng.integers(-1000, 1000, n)
+    k[:7] = mn
+    R = struct([k, rng.integers(0, 1 << 40, n)], [I64, I64])
+    fk = rng.integers(-1100, 1100, m)
+    fk[::1000] = mn
+    S = struct([fk, rng.integers(0, 1 << 40, m)], [I64, I64])
+    Rd, Sd = dev_rel(torch_cuda, R, [I64, I64]), dev_rel(torch_cuda, S, [I64, I64])
+    want = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ)
+    for proj in (PROJ, [(1, 1), (0, 1)], [(1, 1)], [(0, 1)], []):
+        w = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], proj)
+        assert ctx.hashjoin_agg(Rd, [0], Sd, [0], proj, pyg.JOIN_RADIX, 6) == w
+    assert ctx.hashjoin_agg(Rd, [0], Sd, [0], PROJ, pyg.JOIN_RADIX) == want
+
+
+def test_empty_sides(ctx, torch_cuda):
+    R = struct([np.arange(100, dtype=np.int64)] * 2, [I64, I64])
+    E = R[:0]
+    for a, b in ((R, E), (E, R), (E, E)):
+        got = ctx.hashjoin_agg(dev_rel(torch_cuda, a, [I64, I64]), [0], dev_rel(torch_cuda, b, [I64, I64]), [0], PROJ,
+                               pyg.JOIN_RADIX, 4)
+        assert got == (0, [0, 0])
+
+
+def test_host_probe_streams_in_chunks(ctx, torch_cuda):
+    """Host-resident probe relation larger than one 2^25-tuple staging chunk
+    (the end-to-end path): same result as the oracle."""
+    rng = np.random.default_rng(8)
+    n, m = 1 << 16, (1 << 25) + 12345
+    k = rng.permutation(n).astype(np.int64)
+    R = struct([k, k * 3], [I64, I64])
+    S = struct([rng.integers(0, n + 100, m), rng.integers(0, 1 << 20, m)], [I64, I64])
+    got = ctx.hashjoin_agg(host_rel(R, [I64, I64]), [0], host_rel(S, [I64, I64]), [0], PROJ, pyg.JOIN_AUTO)
+    assert got == O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ, buckets=n)
