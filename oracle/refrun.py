@@ -151,14 +151,15 @@ def plan_mpsm(T, rfiles, rtypes, sfiles, stypes, proj, mn, mx, maxb, maxp):
 _ROW = re.compile(r"^-?\d+(\|-?\d+)*$")
 
 
-def run(workdir, plan_text, timeout=600):
-    """Runs a plan; returns (rows as list of int tuples, ResponseTimeInSec,
-    tuple count printed by printer_tuplecount or None)."""
+def run(workdir, plan_text, timeout=600, exe=None):
+    """Runs a plan with the reference engine (or another driver with the
+    same output format, `exe`); returns (rows as list of int tuples,
+    ResponseTimeInSec, tuple count printed by printer_tuplecount or None)."""
     p = os.path.join(workdir, "plan.conf")
     with open(p, "w") as f:
         f.write(plan_text)
     t0 = time.time()
-    r = subprocess.run([EXE, "plan.conf"], cwd=workdir, capture_output=True, text=True, timeout=timeout)
+    r = subprocess.run([exe or EXE, "plan.conf"], cwd=workdir, capture_output=True, text=True, timeout=timeout)
     wall = time.time() - t0
     out = r.stdout.splitlines()
     rows, rt, total = [], None, None

@@ -31,6 +31,10 @@ struct pyg_cdf {
     float* d_params = nullptr;      // device: a0, b0, then (a, b) per leaf
     double* d_yr = nullptr;         // device: (ylo, yhi) per leaf
     int64_t n_sample = 0, distinct = 0, f1 = 0;
+    // Heavy keys: sample runs of at least n/4096 equal keys, kept as exact
+    // point masses [lo, hi) of the sample CDF next to the linear leaves.
+    std::vector<int64_t> heavy_key;
+    std::vector<double> heavy_lo, heavy_hi;
 };
 
 namespace pyg {
@@ -226,6 +230,27 @@ __global__ void run_stats_kernel(const int64_t* __restrict__ k, int64_t n, unsig
     }
 }
 
+// Runs of at least `thr` equal keys in the sorted sample: (key, first, end).
+__global__ void heavy_runs_kernel(const int64_t* __restrict__ k, int64_t n, int64_t thr, longlong2* __restrict__ out,
+                                  long long* __restrict__ ends, unsigned long long* count, int cap)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i > 0 && k[i] == k[i - 1]) continue;
+        if (i + thr - 1 >= n || k[i + thr - 1] != k[i]) continue;
+        int64_t lo = i + thr - 1, hi = n;  // upper bound of k[i]
+        while (lo < hi) {
+            int64_t mid = lo + ((hi - lo) >> 1);
+            if (k[mid] <= k[i]) lo = mid + 1;
+            else hi = mid;
+        }
+        unsigned long long e = atomicAdd(count, 1ULL);
+        if ((int)e < cap) {
+            out[e] = make_longlong2(k[i], i);
+            ends[e] = lo;
+        }
+    }
+}
+
 __global__ void to_signed_kernel(const uint64_t* __restrict__ in, int64_t n, int64_t* __restrict__ out)
 {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -357,6 +382,38 @@ int pyg_cdf_train(pyg_ctx* ctx, const int64_t* sample_keys, int64_t n, const pyg
         m->kmax = ends[1];
         m->distinct = (int64_t)hs[0];
         m->f1 = (int64_t)hs[1];
+        {
+            const int cap = 4096;
+            int64_t thr = n / 4096 > 2 ? n / 4096 : 2;
+            longlong2* runs;
+            long long* rend;
+            if ((rc = dalloc(ctx, (void**)&runs, (size_t)cap * 16))) break;
+            if ((rc = dalloc(ctx, (void**)&rend, (size_t)cap * 8))) {
+                dfree(ctx, runs);
+                break;
+            }
+            PYG_CUDA(cudaMemsetAsync(dstat, 0, 8, ctx->stream));
+            heavy_runs_kernel<<<grid_for(ctx, n, 256, 4, 8), 256, 0, ctx->stream>>>(sorted, n, thr, runs, rend, dstat, cap);
+            PYG_LAUNCHED(ctx);
+            PYG_CUDA(cudaMemcpyAsync(hs, dstat, 8, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+            int nh = (int)std::min<unsigned long long>(hs[0], (unsigned long long)cap);
+            std::vector<longlong2> hr(nh);
+            std::vector<long long> he(nh);
+            PYG_CUDA(cudaMemcpyAsync(hr.data(), runs, (size_t)nh * 16, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaMemcpyAsync(he.data(), rend, (size_t)nh * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+            dfree(ctx, runs);
+            dfree(ctx, rend);
+            std::vector<int> ord(nh);
+            for (int i = 0; i < nh; ++i) ord[i] = i;
+            std::sort(ord.begin(), ord.end(), [&](int a, int b) { return hr[a].x < hr[b].x; });
+            for (int i : ord) {
+                m->heavy_key.push_back(hr[i].x);
+                m->heavy_lo.push_back((double)hr[i].y / (double)n);
+                m->heavy_hi.push_back((double)he[i] / (double)n);
+            }
+        }
         m->key_lo = (double)m->kmin;
         m->key_scale = m->kmax > m->kmin ? 1.0 / ((double)m->kmax - (double)m->kmin) : 0.0;
 
@@ -481,6 +538,24 @@ int pyg_cdf_splitters(pyg_ctx* ctx, const pyg_cdf* m, int32_t fanout, int64_t* o
         if (key < prev) key = prev;
         out[j - 1] = key;
         prev = key;
+    }
+    // Point masses: every splitter whose target quantile falls inside a
+    // heavy key's CDF step becomes that key, the last of them key + 1, so
+    // the heavy key gets a partition of its own (as exact quantiles do);
+    // neighbours are clamped to keep the splitters non-decreasing.
+    for (size_t h = 0; h < m->heavy_key.size(); ++h) {
+        const int64_t k = m->heavy_key[h];
+        int j0 = (int)floor(m->heavy_lo[h] * fanout) + 1;  // first j with j/F > lo
+        int j1 = (int)floor(m->heavy_hi[h] * fanout);      // last j with j/F <= hi
+        if (j1 > fanout - 1) j1 = fanout - 1;
+        if (j0 < 1) j0 = 1;
+        if (j0 > j1) continue;
+        for (int j = j0; j <= j1; ++j) out[j - 1] = k;
+        const int64_t k1 = k == INT64_MAX ? k : k + 1;
+        if (j1 > j0) out[j1 - 1] = k1;
+        for (int j = j0 - 1; j >= 1 && out[j - 1] > k; --j) out[j - 1] = k;
+        const int64_t after = j1 > j0 ? k1 : k;
+        for (int j = j1 + 1; j <= fanout - 1 && out[j - 1] < after; ++j) out[j - 1] = after;
     }
     return PYG_OK;
 }

@@ -170,26 +170,13 @@ struct OutSpec {
 __device__ __forceinline__ void write_group(uint8_t* dst, const OutSpec& o, uint64_t k, uint64_t sum, uint64_t cnt)
 {
     if (o.nkeys == 2) {
-        uint32_t a = (uint32_t)(k >> 32), b = (uint32_t)k;
-        memcpy(dst, &a, 4);
-        memcpy(dst + 4, &b, 4);
+        store_col(dst, 0, PYG_INT32, k >> 32);
+        store_col(dst, 4, PYG_INT32, k);
     } else if (o.nkeys == 1) {
-        if (o.key_type0 == PYG_INT32) {
-            uint32_t w = (uint32_t)k;
-            memcpy(dst, &w, 4);
-        } else {
-            memcpy(dst, &k, 8);
-        }
+        store_col(dst, 0, o.key_type0, k);
     }
-    if (o.want_sum) {
-        if (o.sum_type == PYG_INT32) {
-            uint32_t w = (uint32_t)sum;
-            memcpy(dst + o.sum_off, &w, 4);
-        } else {
-            memcpy(dst + o.sum_off, &sum, 8);
-        }
-    }
-    if (o.want_count) memcpy(dst + o.cnt_off, &cnt, 8);
+    if (o.want_sum) store_col(dst, o.sum_off, o.sum_type, sum);
+    if (o.want_count) store_col(dst, o.cnt_off, PYG_INT64, cnt);
 }
 
 // Compaction: occupied slots -> output rows (unordered), or -> (sortable

@@ -11,6 +11,7 @@
 // linear probing.
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "pyg_internal.cuh"
@@ -110,6 +111,85 @@ __global__ void ht_build_kernel(BuildArgs a)
     }
 }
 
+// Fast build for 16-byte (int64 key @0, int64 payload @8) tuples into a
+// one-payload AGGREGATE table.  A fresh insert is one 16-byte CAS of the
+// whole slot ({empty, 0} -> {key, payload}); only a duplicate key adds its
+// payload with a second atomic.  Each thread keeps UNROLL independent
+// insert chains in flight (loads, then the first CAS of every chain, then
+// resolution).
+__device__ __forceinline__ unsigned __int128 slot128(uint64_t key, uint64_t pay)
+{
+    return ((unsigned __int128)pay << 64) | (unsigned __int128)key;
+}
+
+template <int UNROLL>
+__global__ void __launch_bounds__(256) ht_build16_kernel(BuildArgs a)
+{
+    const longlong2* R = reinterpret_cast<const longlong2*>(a.base);
+    unsigned long long* slots = reinterpret_cast<unsigned long long*>(a.slots);
+    unsigned __int128* slots128 = reinterpret_cast<unsigned __int128*>(a.slots);
+    const unsigned __int128 empty = slot128(kEmptyKey, 0);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    unsigned long long fresh = 0;
+    bool dup = false, full = false;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; base < a.n; base += stride * UNROLL) {
+        longlong2 t[UNROLL];
+        uint64_t s[UNROLL];
+        unsigned long long prev[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            int64_t i = base + u * stride;
+            t[u] = i < a.n ? __ldcs(&R[i]) : make_longlong2((long long)kEmptyKey, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            uint64_t k = (uint64_t)t[u].x;
+            s[u] = reduce_range(mix64(k), a.cap);
+            prev[u] = k == kEmptyKey
+                          ? ~0ULL
+                          : (unsigned long long)atomicCAS(&slots128[s[u]], empty, slot128(k, (uint64_t)t[u].y));
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            int64_t i = base + u * stride;
+            if (i >= a.n) continue;
+            uint64_t k = (uint64_t)t[u].x;
+            if (k == kEmptyKey) {
+                unsigned long long e = atomicAdd(&a.flags[2], 1ULL);
+                if ((int64_t)e < a.side_cap) {
+                    a.side[2 * e] = k;
+                    a.side[2 * e + 1] = (uint64_t)t[u].y;
+                }
+                continue;
+            }
+            uint64_t ss = s[u];
+            unsigned long long pv = prev[u];  // key word of the slot before the CAS
+            uint64_t steps = 0;
+            while (pv != kEmptyKey && pv != k) {
+                if (++steps >= a.cap) {
+                    full = true;
+                    break;
+                }
+                ss = (ss + 1 == a.cap) ? 0 : ss + 1;
+                pv = (unsigned long long)atomicCAS(&slots128[ss], empty, slot128(k, (uint64_t)t[u].y));
+            }
+            if (pv == kEmptyKey) {
+                ++fresh;  // the CAS stored key and payload together
+            } else if (pv == k) {
+                dup = true;
+                atomicAdd(&slots[2 * ss + 1], (unsigned long long)t[u].y);
+            }
+        }
+    }
+    fresh = warp_sum_u64(fresh);
+    bool anydup = __any_sync(0xffffffffu, dup), anyfull = __any_sync(0xffffffffu, full);
+    if ((threadIdx.x & 31) == 0) {
+        if (fresh) atomicAdd(&a.flags[3], fresh);
+        if (anydup) a.flags[0] = 1;
+        if (anyfull) a.flags[1] = 1;
+    }
+}
+
 // Duplicate counts for an AGGREGATE table (run only when duplicates exist).
 __global__ void ht_count_kernel(BuildArgs a, unsigned long long* __restrict__ counts)
 {
@@ -151,8 +231,15 @@ __device__ __forceinline__ void block_flush(uint64_t* acc, int nacc, unsigned lo
 // match count, the build-payload sum and the probe-value sum.  FILLERS:
 // tuples whose key is the empty marker are padding (skipped) rather than
 // real keys (matched against the side list).
+#ifndef PYG_PROBE_UNROLL
+#define PYG_PROBE_UNROLL 4
+#endif
+#ifndef PYG_PROBE_MIN_BLOCKS
+#define PYG_PROBE_MIN_BLOCKS 4
+#endif
+
 template <int UNROLL, bool FILLERS>
-__global__ void __launch_bounds__(256) probe_agg16_kernel(const longlong2* __restrict__ S, int64_t n,
+__global__ void __launch_bounds__(256, PYG_PROBE_MIN_BLOCKS) probe_agg16_kernel(const longlong2* __restrict__ S, int64_t n,
                                                           const ulonglong2* __restrict__ slots, uint64_t cap,
                                                           const unsigned long long* __restrict__ counts,
                                                           const uint64_t* __restrict__ side, int64_t nside,
@@ -270,15 +357,6 @@ __global__ void __launch_bounds__(256) probe_agg_kernel(ProbeArgs a, unsigned lo
     block_flush(acc, a.nproj + 1, out);
 }
 
-__device__ __forceinline__ void store_col(uint8_t* dst, uint64_t v, int32_t type)
-{
-    if (type == PYG_INT32) {
-        uint32_t w = (uint32_t)v;
-        memcpy(dst, &w, 4);
-    } else {
-        memcpy(dst, &v, 8);
-    }
-}
 
 // Materialising probe.  Each lane first counts its matches, the warp
 // reserves one contiguous output range with a single atomic, then every lane
@@ -329,7 +407,7 @@ __global__ void __launch_bounds__(256) probe_mat_kernel(ProbeArgs a, uint8_t* __
                 uint8_t* dst = out + pos * (int64_t)a.out_tb;
                 for (int p = 0; p < a.nproj; ++p) {
                     uint64_t v = a.pside[p] ? (uint64_t)load_col(t, a.poff[p], a.ptype[p]) : e[a.pidx[p]];
-                    store_col(dst + a.outoff[p], v, a.ptype[p]);
+                    store_col(dst, a.outoff[p], a.ptype[p], v);
                 }
             }
             ++pos;
@@ -441,12 +519,13 @@ static int launch_probe16(pyg_ctx* ctx, const pyg_hashtable* ht, const longlong2
 {
     if (n <= 0) return PYG_OK;
     int threads = 256;
-    int grid = grid_for(ctx, n, threads, 4, 8);
+    constexpr int U = PYG_PROBE_UNROLL;
+    int grid = grid_for(ctx, n, threads, U, 8);
     if (fillers)
-        probe_agg16_kernel<4, true><<<grid, threads, 0, ctx->stream>>>(S, n, (const ulonglong2*)ht->slots, ht->cap,
+        probe_agg16_kernel<U, true><<<grid, threads, 0, ctx->stream>>>(S, n, (const ulonglong2*)ht->slots, ht->cap,
                                                                        ht->counts, ht->side, ht->nside, acc);
     else
-        probe_agg16_kernel<4, false><<<grid, threads, 0, ctx->stream>>>(S, n, (const ulonglong2*)ht->slots, ht->cap,
+        probe_agg16_kernel<U, false><<<grid, threads, 0, ctx->stream>>>(S, n, (const ulonglong2*)ht->slots, ht->cap,
                                                                         ht->counts, ht->side, ht->nside, acc);
     PYG_LAUNCHED(ctx);
     return PYG_OK;
@@ -499,15 +578,22 @@ static int probe16_stream_host(pyg_ctx* ctx, const pyg_hashtable* ht, const long
 // probed separately; unused capacity is filled with empty-marker padding.
 
 constexpr int TP_THREADS = 512;
-constexpr int TP_TILE = 4096;
+constexpr int TP_TILE = 2048;
 
 __global__ void sample_part_hist_kernel(const longlong2* __restrict__ S, int64_t n, int64_t stride, int pbits,
                                         unsigned long long* __restrict__ hist)
 {
+    extern __shared__ unsigned sh_hist[];
+    const int P = 1 << pbits;
+    for (int b = threadIdx.x; b < P; b += blockDim.x) sh_hist[b] = 0;
+    __syncthreads();
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j * stride < n; j += (int64_t)gridDim.x * blockDim.x) {
         uint64_t k = (uint64_t)S[j * stride].x;
-        atomicAdd(&hist[mix64(k) >> (64 - pbits)], 1ULL);
+        atomicAdd(&sh_hist[mix64(k) >> (64 - pbits)], 1u);
     }
+    __syncthreads();
+    for (int b = threadIdx.x; b < P; b += blockDim.x)
+        if (sh_hist[b]) atomicAdd(&hist[b], (unsigned long long)sh_hist[b]);
 }
 
 __global__ void __launch_bounds__(TP_THREADS) tile_partition16_kernel(
@@ -742,8 +828,16 @@ int pyg_hashjoin_build(pyg_ctx* ctx, const pyg_rel* build, const int32_t* key_co
         a.side_cap = side_cap;
         a.flags = flags;
         if (a.n > 0) {
-            grid = grid_for(ctx, a.n, threads, 1, 8);
-            ht_build_kernel<<<grid, threads, 0, ctx->stream>>>(a);
+            bool fast = a.agg && a.W == 2 && a.tb == 16 && a.ks.nkeys == 1 && a.ks.off0 == 0 &&
+                        a.ks.type0 == PYG_INT64 && a.pay.off[0] == 8 && a.pay.type[0] == PYG_INT64 &&
+                        (uintptr_t)a.base % 16 == 0;
+            if (fast) {
+                grid = grid_for(ctx, a.n, threads, 4, 8);
+                ht_build16_kernel<4><<<grid, threads, 0, ctx->stream>>>(a);
+            } else {
+                grid = grid_for(ctx, a.n, threads, 1, 8);
+                ht_build_kernel<<<grid, threads, 0, ctx->stream>>>(a);
+            }
             PYG_LAUNCHED(ctx);
         }
         unsigned long long* h = (unsigned long long*)ctx->pinned;
@@ -989,14 +1083,18 @@ int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_ke
         PYG_CUDA(cudaMemsetAsync(hist, 0, (size_t)P * 8, ctx->stream));
         PYG_CUDA(cudaMemsetAsync(cursor, 0, (size_t)(P + 1) * 8, ctx->stream));
         if (nS > 0) {
-            sample_part_hist_kernel<<<grid_for(ctx, (nS + stride - 1) / stride, 256, 4, 4), 256, 0, ctx->stream>>>(
+            sample_part_hist_kernel<<<grid_for(ctx, (nS + stride - 1) / stride, 256, 4, 4), 256, (size_t)P * 4,
+                                      ctx->stream>>>(
                 (const longlong2*)probe->base, nS, stride, pbits, hist);
             PYG_LAUNCHED(ctx);
         }
         tm.mark(ctx, 1);
         pyg_rel Rrel = *build;
         Rrel.base = Rp;
-        if ((rc = pyg_hashjoin_build(ctx, &Rrel, build_keys, 1, pay, npay, PYG_HT_AGGREGATE, lf, &ht))) break;
+        // The 16-byte probe kernel reads {key, payload sum} slots: keep the
+        // build payload column whatever the projection references.
+        const int32_t rpay[1] = {1};
+        if ((rc = pyg_hashjoin_build(ctx, &Rrel, build_keys, 1, rpay, 1, PYG_HT_AGGREGATE, lf, &ht))) break;
         tm.mark(ctx, 2);
         // pyg_hashjoin_build synchronised the stream: the sample is ready.
         PYG_CUDA(cudaMemcpyAsync(hh.data(), hist, (size_t)P * 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1017,7 +1115,8 @@ int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_ke
         size_t smem = (size_t)TP_TILE * 16 + (size_t)(2 * P + 2) * 4 + (size_t)P * 8;
         PYG_CUDA(cudaFuncSetAttribute(tile_partition16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         if (nS > 0) {
-            int grid = grid_for(ctx, (nS + TP_TILE - 1) / TP_TILE, 1, 1, smem > 100000 ? 1 : 2);  // one tile per unit
+            int per_sm = (int)std::min<size_t>(2048 / TP_THREADS, (200 * 1024) / smem);
+            int grid = grid_for(ctx, (nS + TP_TILE - 1) / TP_TILE, 1, 1, per_sm > 0 ? per_sm : 1);  // one tile per unit
             tile_partition16_kernel<<<grid, TP_THREADS, smem, ctx->stream>>>(
                 (const longlong2*)probe->base, nS, pbits, pstart, pcap, cursor, Sp, ovf, ovf_cursor, ovf_cap);
             PYG_LAUNCHED(ctx);

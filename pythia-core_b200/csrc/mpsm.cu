@@ -219,8 +219,8 @@ __global__ void __launch_bounds__(MP_JOIN_THREADS) mp_join_kernel(JoinArgs a)
                     const uint8_t* rt = a.rbase + (int64_t)a.R[r].y * a.rtb;
                     uint8_t* dst = a.out + pos * (int64_t)a.out_tb;
                     for (int p = 0; p < a.nproj; ++p) {
-                        int sz = a.ptype[p] == PYG_INT32 ? 4 : 8;
-                        memcpy(dst + a.ooff[p], (a.pside[p] ? st : rt) + a.poff[p], sz);
+                        store_col(dst, a.ooff[p], a.ptype[p],
+                                  (uint64_t)load_col(a.pside[p] ? st : rt, a.poff[p], a.ptype[p]));
                     }
                 }
             }

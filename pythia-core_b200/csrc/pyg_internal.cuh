@@ -79,24 +79,38 @@ struct ColSpec {
     int32_t type[PYG_MAX_COLS];
 };
 
+// Column access.  Every column of a packed relation is 4 or 8 bytes wide
+// and starts at a multiple of 4 bytes (columns are packed back to back and
+// buffers are at least 16-byte aligned), so a column is read with one
+// 32-bit load, or one 64-bit load when 8-byte aligned, else two 32-bit loads.
 __device__ __forceinline__ int64_t load_col(const uint8_t* t, int32_t off, int32_t type)
 {
+    const uint8_t* p = t + off;
+    if (type == PYG_INT32) return (int64_t)*reinterpret_cast<const int32_t*>(p);
+    if (((uintptr_t)p & 7) == 0) return *reinterpret_cast<const int64_t*>(p);
+    const uint32_t* q = reinterpret_cast<const uint32_t*>(p);
+    return (int64_t)(((uint64_t)q[1] << 32) | (uint64_t)q[0]);
+}
+
+__device__ __forceinline__ void store_col(uint8_t* t, int32_t off, int32_t type, uint64_t v)
+{
+    uint8_t* p = t + off;
     if (type == PYG_INT32) {
-        int32_t v;
-        memcpy(&v, t + off, 4);
-        return (int64_t)v;
+        *reinterpret_cast<uint32_t*>(p) = (uint32_t)v;
+    } else if (((uintptr_t)p & 7) == 0) {
+        *reinterpret_cast<uint64_t*>(p) = v;
+    } else {
+        uint32_t* q = reinterpret_cast<uint32_t*>(p);
+        q[0] = (uint32_t)v;
+        q[1] = (uint32_t)(v >> 32);
     }
-    int64_t v;
-    memcpy(&v, t + off, 8);
-    return v;
 }
 
 __device__ __forceinline__ uint64_t load_key(const uint8_t* t, const KeySpec& ks)
 {
     if (ks.nkeys == 1) return (uint64_t)load_col(t, ks.off0, ks.type0);
-    uint32_t a, b;
-    memcpy(&a, t + ks.off0, 4);
-    memcpy(&b, t + ks.off1, 4);
+    uint32_t a = *reinterpret_cast<const uint32_t*>(t + ks.off0);
+    uint32_t b = *reinterpret_cast<const uint32_t*>(t + ks.off1);
     return ((uint64_t)a << 32) | (uint64_t)b;
 }
 

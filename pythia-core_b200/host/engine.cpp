@@ -1,0 +1,744 @@
+// Operator shims for the join / aggregation hot path over the libpyg C ABI.
+#include "engine.h"
+
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+#include "../../include/pyg_mpsm.h"
+
+namespace pyg_host {
+
+pyg_ctx* Operator::ctx = nullptr;
+
+static void check(int rc, const char* what)
+{
+    if (rc != PYG_OK) throw EngineError(std::string(what) + ": " + pyg_last_error());
+}
+
+// ---------------------------------------------------------------- Schema
+
+void Schema::add(int32_t type)
+{
+    types.push_back(type);
+    offs.push_back(tuple_bytes);
+    tuple_bytes += type == PYG_INT32 ? 4 : 8;
+}
+
+int64_t Schema::get(const uint8_t* tup, size_t col) const
+{
+    if (types[col] == PYG_INT32) {
+        int32_t v;
+        memcpy(&v, tup + offs[col], 4);
+        return v;
+    }
+    int64_t v;
+    memcpy(&v, tup + offs[col], 8);
+    return v;
+}
+
+std::string Schema::prettyprint(const uint8_t* tup, char sep) const
+{
+    std::string s;
+    for (size_t c = 0; c < types.size(); ++c) {
+        if (c) s += sep;
+        s += std::to_string(get(tup, c));
+    }
+    return s;
+}
+
+pyg_rel Schema::rel(const void* base, int64_t n, bool on_device) const
+{
+    pyg_rel r;
+    memset(&r, 0, sizeof(r));
+    r.base = base;
+    r.ntuples = n;
+    r.tuple_bytes = tuple_bytes;
+    r.ncols = (int32_t)types.size();
+    for (size_t c = 0; c < types.size(); ++c) {
+        r.col_offset[c] = offs[c];
+        r.col_type[c] = types[c];
+    }
+    r.on_device = on_device ? 1 : 0;
+    return r;
+}
+
+int32_t Schema::type_of(const std::string& name)
+{
+    if (name == "int" || name == "integer") return PYG_INT32;
+    if (name == "long" || name == "date") return PYG_INT64;
+    throw EngineError("column type '" + name + "' is not on the GPU join/aggregation path (int, long)");
+}
+
+// ---------------------------------------------------------------- HostRel
+
+HostRel::~HostRel()
+{
+    if (data) pyg_host_free(data);
+}
+
+void HostRel::reserve(int64_t bytes)
+{
+    if (bytes <= cap_bytes) return;
+    int64_t cap = cap_bytes ? cap_bytes : (1 << 20);
+    while (cap < bytes) cap *= 2;
+    void* p = nullptr;
+    check(pyg_host_alloc((size_t)cap, &p), "pinned allocation");
+    if (data) {
+        memcpy(p, data, (size_t)ntuples * tuple_bytes);
+        pyg_host_free(data);
+    }
+    data = (uint8_t*)p;
+    cap_bytes = cap;
+}
+
+void HostRel::append(const uint8_t* src, int64_t n)
+{
+    reserve((ntuples + n) * tuple_bytes);
+    memcpy(data + ntuples * tuple_bytes, src, (size_t)n * tuple_bytes);
+    ntuples += n;
+}
+
+void drain(Operator* op, unsigned short tid, HostRel& out)
+{
+    out.tuple_bytes = op->getOutSchema().tuple_bytes;
+    out.ntuples = 0;
+    for (;;) {
+        Operator::GetNextResultT r = op->getNext(tid);
+        if (r.first == Operator::Error) throw EngineError("child '" + op->name + "' returned Error");
+        if (r.second && r.second->ntuples) out.append(r.second->data, r.second->ntuples);
+        if (r.first == Operator::Finished) break;
+    }
+}
+
+// -------------------------------------------------------------- Operator
+
+void Operator::init(const Setting& root, const Setting& node)
+{
+    buffsize = root.getInt("buffsize", 1 << 20);
+    if (buffsize < 1) throw EngineError("buffsize must be positive");
+}
+
+Operator::GetNextResultT MaterializedOp::getNext(unsigned short tid)
+{
+    int64_t per = buffsize / (schema.tuple_bytes ? schema.tuple_bytes : 1);
+    if (per < 1) per = 1;
+    int64_t left = result.ntuples - served;
+    int64_t n = left < per ? left : per;
+    page.data = result.data ? result.data + served * schema.tuple_bytes : nullptr;
+    page.ntuples = n;
+    page.tuple_bytes = schema.tuple_bytes;
+    served += n;
+    return std::make_pair(served >= result.ntuples ? Finished : Ready, &page);
+}
+
+Operator::ResultCode MaterializedOp::scanStop(unsigned short tid)
+{
+    served = 0;
+    return Ready;
+}
+
+void MaterializedOp::serve_from_device(const void* dev, int64_t n)
+{
+    result.tuple_bytes = schema.tuple_bytes;
+    result.ntuples = 0;
+    result.reserve(n * schema.tuple_bytes);
+    if (n) check(pyg_memcpy_d2h(ctx, result.data, dev, (size_t)n * schema.tuple_bytes), "copy result");
+    result.ntuples = n;
+    served = 0;
+}
+
+// ------------------------------------------------------------------ scans
+
+// `scan` / `parallelscan` / `partitionedscan` (operators/scan.cpp,
+// parallelscan.cpp:41-190): all listed files, binary (raw packed tuples,
+// operators/loaders/table.cpp:198-348) or '|'-separated text.
+class ScanOp : public MaterializedOp {
+public:
+    void init(const Setting& root, const Setting& node) override
+    {
+        Operator::init(root, node);
+        const Setting& sch = node["schema"];
+        for (size_t i = 0; i < sch.size(); ++i) schema.add(Schema::type_of(sch[i].asString()));
+        std::string path = root.getString("path", "./");
+        if (!path.empty() && path.back() != '/') path += '/';
+        const Setting& f = node["files"];
+        if (f.isAggregate())
+            for (size_t i = 0; i < f.size(); ++i) files.push_back(path + f[i].asString());
+        else
+            files.push_back(path + f.asString());
+        binary = node.getString("filetype", "text") == "binary";
+        sep = node.getString("separators", "|");
+    }
+
+    ResultCode scanStart(unsigned short tid) override
+    {
+        if (!loaded) load();
+        served = 0;
+        return Ready;
+    }
+
+private:
+    void load()
+    {
+        result.tuple_bytes = schema.tuple_bytes;
+        for (auto& fn : files) {
+            std::ifstream in(fn, std::ios::binary);
+            if (!in) throw EngineError("cannot open input file " + fn);
+            if (binary) {
+                in.seekg(0, std::ios::end);
+                int64_t bytes = (int64_t)in.tellg();
+                in.seekg(0);
+                if (bytes % schema.tuple_bytes)
+                    throw EngineError(fn + ": size is not a multiple of the tuple size");
+                result.reserve(result.ntuples * schema.tuple_bytes + bytes);
+                in.read((char*)result.data + result.ntuples * schema.tuple_bytes, bytes);
+                result.ntuples += bytes / schema.tuple_bytes;
+            } else {
+                std::string line;
+                std::vector<uint8_t> tup(schema.tuple_bytes);
+                while (std::getline(in, line)) {
+                    if (line.empty()) continue;
+                    size_t pos = 0;
+                    for (size_t c = 0; c < schema.columns(); ++c) {
+                        size_t e = line.find_first_of(sep, pos);
+                        std::string field = line.substr(pos, e == std::string::npos ? std::string::npos : e - pos);
+                        int64_t v = strtoll(field.c_str(), nullptr, 10);
+                        if (schema.types[c] == PYG_INT32) {
+                            int32_t w = (int32_t)v;
+                            memcpy(tup.data() + schema.offs[c], &w, 4);
+                        } else {
+                            memcpy(tup.data() + schema.offs[c], &v, 8);
+                        }
+                        pos = e == std::string::npos ? line.size() : e + 1;
+                    }
+                    result.append(tup.data(), 1);
+                }
+            }
+        }
+        loaded = true;
+    }
+
+    std::vector<std::string> files;
+    bool binary = false, loaded = false;
+    std::string sep;
+};
+
+// `merge` (operators/merge.cpp): the GPU replaces the worker threads; the
+// input passes through.
+class MergeOp : public SingleInputOp {
+public:
+    void init(const Setting& root, const Setting& node) override
+    {
+        Operator::init(root, node);
+        schema = nextOp->getOutSchema();
+    }
+    ResultCode scanStart(unsigned short tid) override { return nextOp->scanStart(tid); }
+    GetNextResultT getNext(unsigned short tid) override { return nextOp->getNext(tid); }
+    ResultCode scanStop(unsigned short tid) override { return nextOp->scanStop(tid); }
+};
+
+// `printer_tuplecount` (operators/printer_tuplecount.cpp): counts tuples.
+class TupleCountPrinter : public SingleInputOp {
+public:
+    void init(const Setting& root, const Setting& node) override
+    {
+        Operator::init(root, node);
+        schema = nextOp->getOutSchema();
+    }
+    ResultCode scanStart(unsigned short tid) override { return nextOp->scanStart(tid); }
+    GetNextResultT getNext(unsigned short tid) override
+    {
+        GetNextResultT r = nextOp->getNext(tid);
+        if (r.second) total += r.second->ntuples;
+        return r;
+    }
+    ResultCode scanStop(unsigned short tid) override { return nextOp->scanStop(tid); }
+    int64_t total = 0;
+};
+
+// ------------------------------------------------------------- hash join
+
+static std::vector<pyg_proj> parse_projection(const Setting& line)
+{
+    // "B$i" / "P$i" (operators/join.cpp:142-183).
+    std::vector<pyg_proj> out;
+    for (size_t i = 0; i < line.size(); ++i) {
+        const std::string& s = line[i].asString();
+        size_t d = s.find('$');
+        if (d == std::string::npos || d == 0) throw EngineError("bad projection '" + s + "'");
+        char side = s[d - 1];
+        if (side != 'B' && side != 'P') throw EngineError("bad projection '" + s + "'");
+        pyg_proj p;
+        p.side = side == 'P' ? 1 : 0;
+        p.col = (int32_t)strtol(s.c_str() + d + 1, nullptr, 10);
+        out.push_back(p);
+    }
+    return out;
+}
+
+static std::vector<int32_t> parse_attrs(const Setting& s)
+{
+    std::vector<int32_t> v;
+    if (s.isAggregate())
+        for (size_t i = 0; i < s.size(); ++i) v.push_back((int32_t)s[i].asInt());
+    else
+        v.push_back((int32_t)s.asInt());
+    return v;
+}
+
+// `hashjoin` (HashJoinOp, operators/join.cpp:367-903).
+class HashJoinOp : public DualInputOp {
+public:
+    void init(const Setting& root, const Setting& node) override
+    {
+        Operator::init(root, node);
+        proj = parse_projection(node["projection"]);
+        bkeys = parse_attrs(node["buildjattr"]);
+        pkeys = parse_attrs(node["probejattr"]);
+        if (bkeys.size() != pkeys.size()) throw EngineError("hashjoin: key arity differs");
+        for (auto& p : proj) {
+            Schema& s = p.side ? probeOp->getOutSchema() : buildOp->getOutSchema();
+            if (p.col < 0 || (size_t)p.col >= s.columns()) throw EngineError("hashjoin: projection out of range");
+            schema.add(s.types[p.col]);
+        }
+        if (node.exists("gpu") && node["gpu"].exists("loadfactor"))
+            load_factor = (float)node["gpu"]["loadfactor"].asFloat();
+    }
+
+    // An aggregate above asks for count + column sums instead of rows.
+    bool fuse = false;
+    pyg_join_result fused;
+
+    ResultCode scanStart(unsigned short tid) override
+    {
+        if (buildOp->scanStart(tid) == Error || probeOp->scanStart(tid) == Error) return Error;
+        HostRel R, S;
+        drain(buildOp, tid, R);
+        drain(probeOp, tid, S);
+        buildOp->scanStop(tid);
+        pyg_rel r = buildOp->getOutSchema().rel(R.data, R.ntuples, false);
+        pyg_rel s = probeOp->getOutSchema().rel(S.data, S.ntuples, false);
+        if (fuse) {
+            pyg_join_opts o = {PYG_JOIN_AUTO, 0, load_factor, 0};
+            check(pyg_hashjoin_agg(ctx, &r, bkeys.data(), &s, pkeys.data(), (int32_t)bkeys.size(), proj.data(),
+                                   (int32_t)proj.size(), &o, &fused, nullptr),
+                  "hashjoin (fused aggregate)");
+            result.ntuples = 0;
+            served = 0;
+            return Ready;
+        }
+        std::vector<int32_t> pay;
+        for (auto& p : proj)
+            if (!p.side) pay.push_back(p.col);
+        pyg_hashtable* ht = nullptr;
+        check(pyg_hashjoin_build(ctx, &r, bkeys.data(), (int32_t)bkeys.size(), pay.data(), (int32_t)pay.size(),
+                                 PYG_HT_MATERIALIZE, load_factor, &ht),
+              "hashjoin build");
+        int64_t n = 0;
+        int rc = pyg_hashjoin_probe_materialize(ctx, ht, &s, pkeys.data(), proj.data(), (int32_t)proj.size(), nullptr,
+                                                0, &n);
+        if (rc != PYG_OK && rc != PYG_ERR_CAPACITY) check(rc, "hashjoin probe");
+        void* out = nullptr;
+        check(pyg_alloc(ctx, (size_t)(n > 0 ? n : 1) * schema.tuple_bytes, &out), "hashjoin output");
+        rc = pyg_hashjoin_probe_materialize(ctx, ht, &s, pkeys.data(), proj.data(), (int32_t)proj.size(), out, n, &n);
+        pyg_hashtable_free(ctx, ht);
+        if (rc == PYG_OK) serve_from_device(out, n);
+        pyg_free(ctx, out);
+        check(rc, "hashjoin probe");
+        return Ready;
+    }
+
+    GetNextResultT getNext(unsigned short tid) override
+    {
+        int64_t per = buffsize / schema.tuple_bytes;
+        if (per < 1) per = 1;
+        int64_t left = result.ntuples - served;
+        int64_t n = left < per ? left : per;
+        page.data = result.data ? result.data + served * schema.tuple_bytes : nullptr;
+        page.ntuples = n;
+        page.tuple_bytes = schema.tuple_bytes;
+        served += n;
+        return std::make_pair(served >= result.ntuples ? Finished : Ready, &page);
+    }
+
+    ResultCode scanStop(unsigned short tid) override
+    {
+        served = 0;
+        return probeOp->scanStop(tid);
+    }
+
+    std::vector<pyg_proj> proj;
+    std::vector<int32_t> bkeys, pkeys;
+
+private:
+    void serve_from_device(const void* dev, int64_t n)
+    {
+        result.tuple_bytes = schema.tuple_bytes;
+        result.ntuples = 0;
+        result.reserve(n * schema.tuple_bytes);
+        if (n) check(pyg_memcpy_d2h(ctx, result.data, dev, (size_t)n * schema.tuple_bytes), "copy result");
+        result.ntuples = n;
+        served = 0;
+    }
+    float load_factor = 0.5f;
+    HostRel result;
+    int64_t served = 0;
+    Page page;
+};
+
+// ------------------------------------------------------------ aggregates
+
+// `aggregate_sum` / `aggregate_count` (GenericAggregate + AggregateSum /
+// AggregateCount, operators/genericaggregate.cpp:51-494).  Groups come out
+// ordered by key (the reference emits hash order; any order is valid).
+class AggregateOp : public MaterializedOp {
+public:
+    explicit AggregateOp(bool sum) : is_sum(sum) {}
+    Operator* nextOp = nullptr;
+    std::vector<Operator*> children() override { return {nextOp}; }
+
+    void init(const Setting& root, const Setting& node) override
+    {
+        Operator::init(root, node);
+        if (node.exists("fields")) {
+            const Setting& f = node["fields"];
+            for (size_t i = 0; i < f.size(); ++i) keys.push_back((int32_t)f[i].asInt());
+        } else {
+            keys.push_back((int32_t)node["field"].asInt());
+        }
+        Schema& in = nextOp->getOutSchema();
+        for (int32_t k : keys) {
+            if (k < 0 || (size_t)k >= in.columns()) throw EngineError(name + ": group field out of range");
+            schema.add(in.types[k]);
+        }
+        if (is_sum) {
+            sumfield = (int32_t)node["sumfield"].asInt();
+            if (sumfield < 0 || (size_t)sumfield >= in.columns()) throw EngineError(name + ": sumfield out of range");
+            schema.add(in.types[sumfield]);
+        } else {
+            schema.add(PYG_INT64);
+        }
+        if (node.exists("hash") && node["hash"].exists("buckets")) expected = node["hash"]["buckets"].asInt();
+        if (keys.size() > 2) throw EngineError(name + ": at most two group-by columns on the GPU path");
+    }
+
+    ResultCode scanStart(unsigned short tid) override
+    {
+        served = 0;
+        // No GROUP BY straight over a hash join (possibly through
+        // printer_tuplecount / merge): fuse the aggregate into the probe.
+        if (keys.empty()) {
+            std::vector<TupleCountPrinter*> counters;
+            Operator* op = nextOp;
+            while (op) {
+                if (auto* c = dynamic_cast<TupleCountPrinter*>(op)) {
+                    counters.push_back(c);
+                    op = c->nextOp;
+                } else if (auto* m = dynamic_cast<MergeOp*>(op)) {
+                    op = m->nextOp;
+                } else {
+                    break;
+                }
+            }
+            auto* hj = dynamic_cast<HashJoinOp*>(op);
+            if (hj) {
+                hj->fuse = true;
+                if (nextOp->scanStart(tid) == Error) return Error;
+                nextOp->scanStop(tid);
+                for (auto* c : counters) c->total += hj->fused.count;
+                uint64_t v = is_sum ? (uint64_t)hj->fused.sums[sumfield] : (uint64_t)hj->fused.count;
+                result.tuple_bytes = schema.tuple_bytes;
+                result.ntuples = 0;
+                if (hj->fused.count > 0) {
+                    uint8_t row[8];
+                    if (schema.types[0] == PYG_INT32) {
+                        uint32_t w = (uint32_t)v;
+                        memcpy(row, &w, 4);
+                    } else {
+                        memcpy(row, &v, 8);
+                    }
+                    result.append(row, 1);
+                }
+                return Ready;
+            }
+        }
+        if (nextOp->scanStart(tid) == Error) return Error;
+        HostRel in;
+        drain(nextOp, tid, in);
+        nextOp->scanStop(tid);
+        pyg_rel r = nextOp->getOutSchema().rel(in.data, in.ntuples, false);
+        int64_t cap = in.ntuples > 0 ? in.ntuples : 1;
+        void* out = nullptr;
+        check(pyg_alloc(ctx, (size_t)cap * schema.tuple_bytes, &out), name.c_str());
+        int64_t g = 0;
+        int rc = pyg_groupby(ctx, &r, keys.data(), (int32_t)keys.size(), is_sum ? PYG_AGG_SUM : PYG_AGG_COUNT,
+                             is_sum ? sumfield : 0, 1, expected, out, cap, &g);
+        if (rc == PYG_OK) serve_from_device(out, g);
+        pyg_free(ctx, out);
+        check(rc, name.c_str());
+        return Ready;
+    }
+
+private:
+    bool is_sum;
+    std::vector<int32_t> keys;
+    int32_t sumfield = 0;
+    int64_t expected = 0;
+};
+
+// ------------------------------------------------------ partition / sort
+
+// `partition` (PartitionOp, operators/partition.cpp:44-404): exact range
+// partition on `attr` over `range` into `buckets`; the partitions come out
+// one after another (partition b is what reference thread b serves).
+class PartitionOp : public MaterializedOp {
+public:
+    Operator* nextOp = nullptr;
+    std::vector<Operator*> children() override { return {nextOp}; }
+    void init(const Setting& root, const Setting& node) override
+    {
+        Operator::init(root, node);
+        schema = nextOp->getOutSchema();
+        attr = (int32_t)node["attr"].asInt();
+        mn = node["range"][0].asInt();
+        mx = node["range"][1].asInt();
+        buckets = (int32_t)node["buckets"].asInt();
+        sortout = node.getString("sort", "no") == "yes";
+        sortattr = (int32_t)node.getInt("sortattr", attr);
+    }
+    ResultCode scanStart(unsigned short tid) override
+    {
+        if (nextOp->scanStart(tid) == Error) return Error;
+        HostRel in;
+        drain(nextOp, tid, in);
+        nextOp->scanStop(tid);
+        pyg_rel r = schema.rel(in.data, in.ntuples, false);
+        void* out = nullptr;
+        check(pyg_alloc(ctx, (size_t)(in.ntuples > 0 ? in.ntuples : 1) * schema.tuple_bytes, &out), "partition");
+        pyg_splitter s = {PYG_SPLIT_EXACTRANGE, buckets, mn, mx, nullptr};
+        offsets.assign(buckets + 1, 0);
+        int rc = pyg_partition(ctx, &r, attr, &s, out, offsets.data());
+        if (rc == PYG_OK && sortout) {
+            // Sort each partition on sortattr (PartitionOp with sort = yes).
+            void* tmp = nullptr;
+            rc = pyg_alloc(ctx, (size_t)(in.ntuples > 0 ? in.ntuples : 1) * schema.tuple_bytes, &tmp);
+            for (int b = 0; rc == PYG_OK && b < buckets; ++b) {
+                int64_t n = offsets[b + 1] - offsets[b];
+                if (n < 2) continue;
+                pyg_rel pr = schema.rel((uint8_t*)out + offsets[b] * schema.tuple_bytes, n, true);
+                rc = pyg_sort(ctx, &pr, sortattr, (uint8_t*)tmp + offsets[b] * schema.tuple_bytes);
+                if (rc == PYG_OK)
+                    rc = pyg_memcpy_d2d(ctx, (uint8_t*)out + offsets[b] * schema.tuple_bytes,
+                                        (uint8_t*)tmp + offsets[b] * schema.tuple_bytes, (size_t)n * schema.tuple_bytes);
+            }
+            pyg_free(ctx, tmp);
+        }
+        if (rc == PYG_OK) serve_from_device(out, in.ntuples);
+        pyg_free(ctx, out);
+        check(rc, "partition");
+        return Ready;
+    }
+    std::vector<int64_t> offsets;
+
+private:
+    int32_t attr = 0, buckets = 1, sortattr = 0;
+    int64_t mn = 0, mx = 0;
+    bool sortout = false;
+};
+
+// `sort` (SortOp, operators/sort.cpp:87-311) on `attr`.
+class SortOp : public MaterializedOp {
+public:
+    Operator* nextOp = nullptr;
+    std::vector<Operator*> children() override { return {nextOp}; }
+    void init(const Setting& root, const Setting& node) override
+    {
+        Operator::init(root, node);
+        schema = nextOp->getOutSchema();
+        attr = (int32_t)node["attr"].asInt();
+    }
+    ResultCode scanStart(unsigned short tid) override
+    {
+        if (nextOp->scanStart(tid) == Error) return Error;
+        HostRel in;
+        drain(nextOp, tid, in);
+        nextOp->scanStop(tid);
+        pyg_rel r = schema.rel(in.data, in.ntuples, false);
+        void* out = nullptr;
+        check(pyg_alloc(ctx, (size_t)(in.ntuples > 0 ? in.ntuples : 1) * schema.tuple_bytes, &out), "sort");
+        int rc = pyg_sort(ctx, &r, attr, out);
+        if (rc == PYG_OK) serve_from_device(out, in.ntuples);
+        pyg_free(ctx, out);
+        check(rc, "sort");
+        return Ready;
+    }
+
+private:
+    int32_t attr = 0;
+};
+
+// `sortmergejoin` / `mpsmjoin` / `newmpsmjoin` / `preprejoin`
+// (operators/join.cpp:905-2212): MPSM join on single keys.  The
+// buildprepartitioned range (if any) gives equal-width splitters as the
+// reference; an optional gpu { splitter = "sampled" | "learned" |
+// "exactrange"; fanout = N; } group picks the splitters.
+class MpsmJoinOp : public DualInputOp {
+public:
+    void init(const Setting& root, const Setting& node) override
+    {
+        Operator::init(root, node);
+        proj = parse_projection(node["projection"]);
+        bkey = parse_attrs(node["buildjattr"]).at(0);
+        pkey = parse_attrs(node["probejattr"]).at(0);
+        for (auto& p : proj) {
+            Schema& s = p.side ? probeOp->getOutSchema() : buildOp->getOutSchema();
+            if (p.col < 0 || (size_t)p.col >= s.columns()) throw EngineError("mpsm: projection out of range");
+            schema.add(s.types[p.col]);
+        }
+        memset(&opts, 0, sizeof(opts));
+        opts.splitter_kind = PYG_MPSM_SPLIT_SAMPLED;
+        opts.fanout = 1024;
+        opts.sample_rate = 0.01;
+        opts.cdf_leaves = 1024;
+        opts.page_tuples = 256;
+        opts.seed = 1;
+        if (node.exists("buildprepartitioned")) {
+            opts.splitter_kind = PYG_MPSM_SPLIT_EXACTRANGE;
+            opts.fanout = (int32_t)node["buildprepartitioned"]["buckets"].asInt();
+        }
+        if (node.exists("gpu")) {
+            const Setting& g = node["gpu"];
+            std::string k = g.getString("splitter", "sampled");
+            opts.splitter_kind = k == "learned" ? PYG_MPSM_SPLIT_LEARNED
+                                 : k == "exactrange" ? PYG_MPSM_SPLIT_EXACTRANGE : PYG_MPSM_SPLIT_SAMPLED;
+            opts.fanout = (int32_t)g.getInt("fanout", opts.fanout);
+        }
+    }
+    ResultCode scanStart(unsigned short tid) override
+    {
+        if (buildOp->scanStart(tid) == Error || probeOp->scanStart(tid) == Error) return Error;
+        HostRel R, S;
+        drain(buildOp, tid, R);
+        drain(probeOp, tid, S);
+        buildOp->scanStop(tid);
+        probeOp->scanStop(tid);
+        pyg_rel r = buildOp->getOutSchema().rel(R.data, R.ntuples, false);
+        pyg_rel s = probeOp->getOutSchema().rel(S.data, S.ntuples, false);
+        int64_t n = 0;
+        int rc = pyg_mpsm_join_materialize(ctx, &r, bkey, &s, pkey, proj.data(), (int32_t)proj.size(), &opts, nullptr,
+                                           0, &n);
+        if (rc != PYG_OK && rc != PYG_ERR_CAPACITY) check(rc, "mpsm join");
+        void* out = nullptr;
+        check(pyg_alloc(ctx, (size_t)(n > 0 ? n : 1) * schema.tuple_bytes, &out), "mpsm output");
+        rc = pyg_mpsm_join_materialize(ctx, &r, bkey, &s, pkey, proj.data(), (int32_t)proj.size(), &opts, out, n, &n);
+        if (rc == PYG_OK) {
+            result.tuple_bytes = schema.tuple_bytes;
+            result.ntuples = 0;
+            result.reserve(n * schema.tuple_bytes);
+            if (n) rc = pyg_memcpy_d2h(ctx, result.data, out, (size_t)n * schema.tuple_bytes);
+            result.ntuples = n;
+        }
+        pyg_free(ctx, out);
+        check(rc, "mpsm join");
+        served = 0;
+        return Ready;
+    }
+    GetNextResultT getNext(unsigned short tid) override
+    {
+        int64_t per = buffsize / schema.tuple_bytes;
+        if (per < 1) per = 1;
+        int64_t left = result.ntuples - served;
+        int64_t n = left < per ? left : per;
+        page.data = result.data ? result.data + served * schema.tuple_bytes : nullptr;
+        page.ntuples = n;
+        page.tuple_bytes = schema.tuple_bytes;
+        served += n;
+        return std::make_pair(served >= result.ntuples ? Finished : Ready, &page);
+    }
+    ResultCode scanStop(unsigned short tid) override
+    {
+        served = 0;
+        return Ready;
+    }
+
+private:
+    std::vector<pyg_proj> proj;
+    int32_t bkey = 0, pkey = 0;
+    pyg_mpsm_opts opts;
+    HostRel result;
+    int64_t served = 0;
+    Page page;
+};
+
+// ------------------------------------------------------------------ Query
+
+static void set_input(Operator* op, Operator* child)
+{
+    if (auto* s = dynamic_cast<SingleInputOp*>(op)) s->nextOp = child;
+    else if (auto* a = dynamic_cast<AggregateOp*>(op)) a->nextOp = child;
+    else if (auto* p = dynamic_cast<PartitionOp*>(op)) p->nextOp = child;
+    else if (auto* so = dynamic_cast<SortOp*>(op)) so->nextOp = child;
+    else throw EngineError("operator '" + op->name + "' takes no input");
+}
+
+static Operator* construct(Query& q, const Setting& root, const Setting& node)
+{
+    const std::string& name = node["name"].asString();
+    const Setting& cfg = root[name];
+    const std::string type = cfg["type"].asString();
+    std::unique_ptr<Operator> op;
+    if (type == "scan" || type == "parallelscan" || type == "partitionedscan") op.reset(new ScanOp());
+    else if (type == "hashjoin") op.reset(new HashJoinOp());
+    else if (type == "sortmergejoin" || type == "mpsmjoin" || type == "newmpsmjoin" || type == "preprejoin")
+        op.reset(new MpsmJoinOp());
+    else if (type == "aggregate_sum") op.reset(new AggregateOp(true));
+    else if (type == "aggregate_count") op.reset(new AggregateOp(false));
+    else if (type == "merge") op.reset(new MergeOp());
+    else if (type == "printer_tuplecount") op.reset(new TupleCountPrinter());
+    else if (type == "partition") op.reset(new PartitionOp());
+    else if (type == "sort") op.reset(new SortOp());
+    else throw EngineError("plan node type '" + type + "' is not on the GPU join/aggregation path");
+    op->type = type;
+    op->name = name;
+    Operator* raw = op.get();
+    q.ops.push_back(std::move(op));
+    if (auto* d = dynamic_cast<DualInputOp*>(raw)) {
+        d->buildOp = construct(q, root, node["build"]);
+        d->probeOp = construct(q, root, node["probe"]);
+    } else if (node.exists("input")) {
+        set_input(raw, construct(q, root, node["input"]));
+    } else if (!dynamic_cast<ScanOp*>(raw)) {
+        throw EngineError("operator '" + name + "' needs an input");
+    }
+    raw->init(root, cfg);  // after the children, as Query::create does
+    return raw;
+}
+
+void Query::create(std::unique_ptr<Setting> plan_root)
+{
+    plan = std::move(plan_root);
+    root = construct(*this, *plan, (*plan)["treeroot"]);
+}
+
+void Query::threadInit()
+{
+    for (auto& op : ops) op->threadInit(0);
+}
+
+void Query::threadClose()
+{
+    for (auto& op : ops) op->threadClose(0);
+}
+
+std::vector<std::string> Query::counter_report() const
+{
+    std::vector<std::string> out;
+    for (auto& op : ops)
+        if (auto* c = dynamic_cast<TupleCountPrinter*>(op.get()))
+            out.push_back("TupleCountPrinter (total=" + std::to_string(c->total) + " tuples)");
+    return out;
+}
+
+}  // namespace pyg_host

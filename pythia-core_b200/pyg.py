@@ -162,6 +162,7 @@ SIGNATURES = [
     ("pyg_batch_run", C.c_int, [_P, _P, _PI64, _PI64, C.POINTER(C.c_double)]),
     ("pyg_batch_free", C.c_int, [_P, _P]),
     ("pyg_batch_run_plain", C.c_int, [_P, C.POINTER(pyg_fragment), _I32, _PI64, _PI64, C.POINTER(C.c_double)]),
+    ("pyg_batch_inject_stall", C.c_int, [_P, _P, _I32]),
     ("pyg_autotune", C.c_int, [_P, C.POINTER(pyg_fragment), _I32, C.c_char_p, C.POINTER(pyg_tuning)]),
     ("pyg_gen_pk", C.c_int, [_P, _P, _I64, _I64, C.c_uint64]),
     ("pyg_gen_fk", C.c_int, [_P, _P, _I64, _I64, C.c_double, C.c_uint64, _I64, C.c_uint64]),
@@ -435,6 +436,46 @@ class Ctx:
         if rc not in (PYG_OK, PYG_ERR_CAPACITY):
             check(rc)
         return rc, cnt.value
+
+    # -- batched fragments ---------------------------------------------
+    @staticmethod
+    def fragments(pairs):
+        """pairs: [(build_tensor, nbuild, probe_tensor, nprobe)] -> ctypes array."""
+        arr = (pyg_fragment * len(pairs))()
+        for i, (b, nb, p, np_) in enumerate(pairs):
+            arr[i] = pyg_fragment(_ptr(b), nb, _ptr(p), np_)
+        return arr
+
+    def batch_create(self, frags, tuning=None):
+        h = C.c_void_p()
+        check(lib().pyg_batch_create(self.h, frags, len(frags), C.byref(tuning) if tuning else None, C.byref(h)))
+        return h.value
+
+    def batch_run(self, b, n):
+        c = np.zeros(n, dtype=np.int64)
+        s = np.zeros(n, dtype=np.int64)
+        lat = np.zeros(n, dtype=np.float64)
+        rc = lib().pyg_batch_run(self.h, b, c.ctypes.data_as(_PI64), s.ctypes.data_as(_PI64),
+                                 lat.ctypes.data_as(C.POINTER(C.c_double)))
+        return rc, c, s, lat
+
+    def batch_free(self, b):
+        check(lib().pyg_batch_free(self.h, b))
+
+    def batch_run_plain(self, frags):
+        n = len(frags)
+        c = np.zeros(n, dtype=np.int64)
+        s = np.zeros(n, dtype=np.int64)
+        lat = np.zeros(n, dtype=np.float64)
+        check(lib().pyg_batch_run_plain(self.h, frags, n, c.ctypes.data_as(_PI64), s.ctypes.data_as(_PI64),
+                                        lat.ctypes.data_as(C.POINTER(C.c_double))))
+        return c, s, lat
+
+    def autotune(self, frags, cache_path=None):
+        t = pyg_tuning()
+        check(lib().pyg_autotune(self.h, frags, len(frags), cache_path.encode() if cache_path else None,
+                                 C.byref(t)))
+        return t
 
     # -- generators ---------------------------------------------------
     def gen_pk(self, out, n, mul, seed):
