@@ -284,8 +284,10 @@ def main_gpu(args):
               "gbs": round(v[1] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else None,
               "frac": round(v[1] / (v[0] / 1e3) / 1e9 / hbm, 4) if v[0] > 0 else None} for k, v in phases.items()}
     top = max((k for k in ph if ph[k]["ms"] > 0), key=lambda k: ph[k]["ms"])
-    kernel_name = {"probe": "probe_agg16_kernel", "probe_partition": "tile_partition16_kernel",
-                   "build": "ht_build_kernel", "build_partition": "pt_scatter_kernel"}[top]
+    radix = int(phase[0].algorithm) == pyg.JOIN_RADIX
+    kernel_name = {"probe": "part_join_kernel" if radix else "probe_agg16_kernel",
+                   "probe_partition": "tile_partition16_kernel", "build": "ht_build16_kernel",
+                   "build_partition": "pt_scatter_kernel"}[top]
     step_bytes = (nR + nS) * 16
     roofline = {"bound": "hbm", "kernel": kernel_name, "phase": top, "achieved": ph[top]["gbs"], "peak": hbm,
                 "unit": "GB/s", "frac": ph[top]["frac"], "peak_source": peak_kind, "traffic": None,

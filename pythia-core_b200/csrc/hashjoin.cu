@@ -688,6 +688,140 @@ __global__ void __launch_bounds__(TP_THREADS) tile_partition16_kernel(
     }
 }
 
+// ---------------------------------------------------------------------------
+// Partition-at-a-time join: one cooperative (co-resident) grid walks the
+// partitions in order.  For partition p it clears a table slice in one of
+// two reused buffers, inserts the build partition, then probes the probe
+// partition; two grid barriers separate the phases.  The two buffers are
+// sized to stay in L2, so the table never goes to HBM and every insert and
+// probe is an L2 hit; HBM traffic is one read of each partitioned
+// relation.  Slots are 32 bytes {key, payload sum, count, -}.  Barrier
+// waits are bounded: on timeout a flag is set, every CTA leaves, and the
+// host reports PYG_ERR_TIMEOUT.
+
+struct GridBarrier {
+    unsigned int count;
+    unsigned int gen;
+    unsigned int error;
+    unsigned int pad;
+};
+
+constexpr long long kBarrierSpinLimit = 1LL << 24;
+
+__device__ __forceinline__ unsigned ld_volatile_u32(const unsigned* p) { return *(volatile const unsigned*)p; }
+
+// Returns false (for every thread of the CTA) if the barrier timed out or an
+// earlier barrier did.
+__device__ bool grid_barrier(GridBarrier* b, unsigned nblocks)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned g = ld_volatile_u32(&b->gen);
+        int good = ld_volatile_u32(&b->error) == 0;
+        if (good) {
+            unsigned arrived = atomicAdd(&b->count, 1u) + 1;
+            if (arrived == nblocks) {
+                b->count = 0;
+                __threadfence();
+                atomicAdd(&b->gen, 1u);
+            } else {
+                good = 0;
+                for (long long i = 0; i < kBarrierSpinLimit; ++i) {
+                    if (ld_volatile_u32(&b->gen) != g) {
+                        good = 1;
+                        break;
+                    }
+                    if (ld_volatile_u32(&b->error)) break;
+                    __nanosleep(64);
+                }
+                if (!good) atomicOr(&b->error, 1u);
+            }
+        }
+        __threadfence();
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+struct PartJoinArgs {
+    const longlong2* R;                 // build relation partitioned by the top pbits hash bits
+    const unsigned long long* roff;     // P + 1 offsets
+    const longlong2* S;                 // probe partitions (tile-partitioned, with capacity gaps)
+    const unsigned long long* pstart;   // P partition starts in S
+    const unsigned long long* pcap;     // P capacities
+    const unsigned long long* pcount;   // P tuples written (may exceed capacity: overflow)
+    ulonglong4* slices;                 // two slice buffers of slice_cap slots
+    uint64_t slice_cap;
+    int pbits;
+    GridBarrier* bar;
+    unsigned long long* acc;            // count, build sum, probe sum
+};
+
+__device__ __forceinline__ uint64_t slice_slot(uint64_t h, int pbits, uint64_t cap)
+{
+    return __umul64hi(h << pbits, cap);
+}
+
+__global__ void __launch_bounds__(512) part_join_kernel(PartJoinArgs a)
+{
+    const int P = 1 << a.pbits;
+    const unsigned nblocks = gridDim.x;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+    uint64_t cnt = 0, bsum = 0, psum = 0;
+    for (int p = 0; p < P; ++p) {
+        ulonglong4* T = a.slices + (p & 1) * a.slice_cap;
+        for (int64_t i = tid; i < (int64_t)a.slice_cap; i += nthreads) T[i] = make_ulonglong4(kEmptyKey, 0, 0, 0);
+        if (!grid_barrier(a.bar, nblocks)) break;
+        for (int64_t i = (int64_t)a.roff[p] + tid; i < (int64_t)a.roff[p + 1]; i += nthreads) {
+            longlong2 t = a.R[i];
+            uint64_t k = (uint64_t)t.x;
+            if (k == kEmptyKey) continue;  // joined by the overflow path (probe keys equal to the marker go there)
+            uint64_t s = slice_slot(mix64(k), a.pbits, a.slice_cap);
+            for (uint64_t steps = 0; steps < a.slice_cap; ++steps) {
+                unsigned long long* slot = (unsigned long long*)&T[s];
+                unsigned long long prev = atomicCAS(slot, kEmptyKey, k);
+                if (prev == kEmptyKey || prev == k) {
+                    atomicAdd(slot + 1, (unsigned long long)t.y);
+                    atomicAdd(slot + 2, 1ULL);
+                    break;
+                }
+                s = (s + 1 == a.slice_cap) ? 0 : s + 1;
+            }
+        }
+        if (!grid_barrier(a.bar, nblocks)) break;
+        const int64_t s0 = (int64_t)a.pstart[p];
+        const int64_t s1 = s0 + (int64_t)(a.pcount[p] < a.pcap[p] ? a.pcount[p] : a.pcap[p]);
+        for (int64_t i = s0 + tid; i < s1; i += nthreads) {
+            longlong2 t = __ldcs(&a.S[i]);
+            uint64_t k = (uint64_t)t.x;
+            uint64_t s = slice_slot(mix64(k), a.pbits, a.slice_cap);
+            for (uint64_t steps = 0; steps < a.slice_cap; ++steps) {
+                ulonglong4 e = T[s];
+                if (e.x == k) {
+                    cnt += e.z;
+                    bsum += e.y;
+                    psum += e.z * (uint64_t)t.y;
+                    break;
+                }
+                if (e.x == kEmptyKey) break;
+                s = (s + 1 == a.slice_cap) ? 0 : s + 1;
+            }
+        }
+    }
+    cnt = warp_sum_u64(cnt);
+    bsum = warp_sum_u64(bsum);
+    psum = warp_sum_u64(psum);
+    if ((threadIdx.x & 31) == 0 && (cnt | bsum | psum)) {
+        atomicAdd(&a.acc[0], (unsigned long long)cnt);
+        atomicAdd(&a.acc[1], (unsigned long long)bsum);
+        atomicAdd(&a.acc[2], (unsigned long long)psum);
+    }
+}
+
 // Pads [start + min(cursor, cap), start + cap) of every partition with
 // empty-marker tuples.
 __global__ void fill_gaps_kernel(longlong2* __restrict__ out, int P, const unsigned long long* __restrict__ pstart,
@@ -1054,10 +1188,11 @@ int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_ke
     const int64_t nR = build->ntuples, nS = probe->ntuples;
     int pbits = opts ? opts->radix_bits : 0;
     if (pbits <= 0) {
-        // About 8 MiB of table per partition.
-        double table = (double)nR / lf * 16.0;
+        // Two table slices of 32-byte slots at twice the partition size
+        // within about 40 MiB of L2.
+        double slices = 2.0 * 2.0 * (double)nR * 32.0;
         pbits = 4;
-        while (pbits < 12 && table / (double)(1 << pbits) > 8.0 * (1 << 20)) ++pbits;
+        while (pbits < 12 && slices / (double)(1 << pbits) > 40.0 * (1 << 20)) ++pbits;
     }
     if (pbits < 1 || pbits > 12) {
         set_error("pyg_hashjoin_agg: radix bits must be in [1, 12]");
@@ -1068,36 +1203,34 @@ int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_ke
     void* Rp = nullptr;
     unsigned long long* meta = nullptr;  // roffs[P+1] | hist[P] | pstart[P] | pcap[P] | cursor[P] | ovf
     longlong2 *Sp = nullptr, *ovf = nullptr;
+    ulonglong4* slices = nullptr;
     pyg_hashtable* ht = nullptr;
     unsigned long long* acc = ctx->dcounters + 8;
+    GridBarrier* bar = (GridBarrier*)(ctx->dcounters + 128);
     std::vector<unsigned long long> hh(3 * P);
+    std::vector<unsigned long long> ro(P + 1);
     do {
         if ((rc = dalloc(ctx, &Rp, (size_t)(nR > 0 ? nR : 1) * 16))) break;
         if ((rc = dalloc(ctx, (void**)&meta, (size_t)(6 * P + 2) * 8))) break;
         unsigned long long *roffs = meta, *hist = meta + P + 1, *pstart = hist + P, *pcap = pstart + P,
                            *cursor = pcap + P, *ovf_cursor = cursor + P;
+        PYG_CUDA(cudaMemsetAsync(roffs, 0, (size_t)(P + 1) * 8, ctx->stream));
         if (nR > 0 && (rc = partition_by_hash(ctx, build, pbits, Rp, roffs))) break;
-        // Sample histogram of the probe side (about 2^20 samples).
+        tm.mark(ctx, 1);
+        tm.mark(ctx, 2);
+        // Probe side: sample histogram (about 2^20 samples) -> capacities
+        // -> one-pass tile partition.
         int64_t stride = nS >> 20;
         if (stride < 1) stride = 1;
         PYG_CUDA(cudaMemsetAsync(hist, 0, (size_t)P * 8, ctx->stream));
         PYG_CUDA(cudaMemsetAsync(cursor, 0, (size_t)(P + 1) * 8, ctx->stream));
         if (nS > 0) {
             sample_part_hist_kernel<<<grid_for(ctx, (nS + stride - 1) / stride, 256, 4, 4), 256, (size_t)P * 4,
-                                      ctx->stream>>>(
-                (const longlong2*)probe->base, nS, stride, pbits, hist);
+                                      ctx->stream>>>((const longlong2*)probe->base, nS, stride, pbits, hist);
             PYG_LAUNCHED(ctx);
         }
-        tm.mark(ctx, 1);
-        pyg_rel Rrel = *build;
-        Rrel.base = Rp;
-        // The 16-byte probe kernel reads {key, payload sum} slots: keep the
-        // build payload column whatever the projection references.
-        const int32_t rpay[1] = {1};
-        if ((rc = pyg_hashjoin_build(ctx, &Rrel, build_keys, 1, rpay, 1, PYG_HT_AGGREGATE, lf, &ht))) break;
-        tm.mark(ctx, 2);
-        // pyg_hashjoin_build synchronised the stream: the sample is ready.
         PYG_CUDA(cudaMemcpyAsync(hh.data(), hist, (size_t)P * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(ro.data(), roffs, (size_t)(P + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
         PYG_CUDA(cudaStreamSynchronize(ctx->stream));
         unsigned long long total = 0;
         for (int b = 0; b < P; ++b) {
@@ -1120,30 +1253,61 @@ int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_ke
             tile_partition16_kernel<<<grid, TP_THREADS, smem, ctx->stream>>>(
                 (const longlong2*)probe->base, nS, pbits, pstart, pcap, cursor, Sp, ovf, ovf_cursor, ovf_cap);
             PYG_LAUNCHED(ctx);
-            fill_gaps_kernel<<<P < 4 * ctx->sm_count ? P : 4 * ctx->sm_count, 256, 0, ctx->stream>>>(Sp, P, pstart, pcap,
-                                                                                                    cursor);
-            PYG_LAUNCHED(ctx);
-        }
-        tm.mark(ctx, 3);
-        if (nS > 0) {
-            if ((rc = launch_probe16(ctx, ht, Sp, (int64_t)total, true, acc))) break;
         }
         unsigned long long* h = (unsigned long long*)ctx->pinned;
         PYG_CUDA(cudaMemcpyAsync(h + 16, ovf_cursor, 8, cudaMemcpyDeviceToHost, ctx->stream));
         PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-        int64_t novf = (int64_t)h[16];
-        if (novf > ovf_cap) {
-            // The sample badly under-estimated some partitions: probe the
-            // original relation instead (same table, exact result).
+        tm.mark(ctx, 3);
+        const int64_t novf = (int64_t)h[16];
+        if (novf > 0) {
+            // Probe tuples that did not fit their partition's sampled
+            // capacity, or whose key is the table's empty marker: join the
+            // whole input through one table instead (exact, rarely taken).
+            pyg_rel Rrel = *build;
+            Rrel.base = Rp;
+            const int32_t rpay[1] = {1};
+            if ((rc = pyg_hashjoin_build(ctx, &Rrel, build_keys, 1, rpay, 1, PYG_HT_AGGREGATE, lf, &ht))) break;
             PYG_CUDA(cudaMemsetAsync(acc, 0, (PYG_MAX_COLS + 1) * 8, ctx->stream));
-            rc = launch_probe16(ctx, ht, (const longlong2*)probe->base, nS, false, acc);
-        } else if (novf > 0) {
-            rc = launch_probe16(ctx, ht, ovf, novf, false, acc);
+            if ((rc = launch_probe16(ctx, ht, (const longlong2*)probe->base, nS, false, acc))) break;
+        } else if (nS > 0 && nR > 0) {
+            uint64_t maxr = 0;
+            for (int b = 0; b < P; ++b) maxr = std::max<uint64_t>(maxr, ro[b + 1] - ro[b]);
+            uint64_t slice_cap = (uint64_t)((double)maxr / lf) + 64;
+            if ((rc = dalloc(ctx, (void**)&slices, (size_t)2 * slice_cap * sizeof(ulonglong4)))) break;
+            PYG_CUDA(cudaMemsetAsync(bar, 0, sizeof(GridBarrier), ctx->stream));
+            PartJoinArgs ja;
+            ja.R = (const longlong2*)Rp;
+            ja.roff = roffs;
+            ja.S = Sp;
+            ja.pstart = pstart;
+            ja.pcap = pcap;
+            ja.pcount = cursor;
+            ja.slices = slices;
+            ja.slice_cap = slice_cap;
+            ja.pbits = pbits;
+            ja.bar = bar;
+            ja.acc = acc;
+            int per_sm = 0;
+            PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, part_join_kernel, 512, 0));
+            if (per_sm < 1) {
+                set_error("pyg_hashjoin_agg: partition join kernel cannot be resident");
+                rc = PYG_ERR_CUDA;
+                break;
+            }
+            void* kargs[] = {&ja};
+            PYG_CUDA(cudaLaunchCooperativeKernel((void*)part_join_kernel, dim3(ctx->sm_count * per_sm), dim3(512), kargs,
+                                                 0, ctx->stream));
+            PYG_LAUNCHED(ctx);
         }
-        if (rc) break;
         tm.mark(ctx, 4);
         PYG_CUDA(cudaMemcpyAsync(h, acc, 3 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(h + 20, bar, sizeof(GridBarrier), cudaMemcpyDeviceToHost, ctx->stream));
         PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (novf == 0 && ((GridBarrier*)(h + 20))->error) {
+            set_error("pyg_hashjoin_agg: a grid barrier of the partition join timed out");
+            rc = PYG_ERR_TIMEOUT;
+            break;
+        }
         memset(out, 0, sizeof(*out));
         out->count = (int64_t)h[0];
         for (int p = 0; p < nproj; ++p) out->sums[p] = (int64_t)(proj[p].side ? h[2] : h[1]);
@@ -1156,6 +1320,7 @@ int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_ke
         }
         rc = PYG_OK;
     } while (0);
+    dfree(ctx, slices);
     if (ht) pyg_hashtable_free(ctx, ht);
     dfree(ctx, Rp);
     dfree(ctx, meta);
