@@ -141,6 +141,7 @@ SIGNATURES = [
     ("pyg_hashjoin_agg", C.c_int, [_P, C.POINTER(pyg_rel), _PI32, C.POINTER(pyg_rel), _PI32, _I32, C.POINTER(pyg_proj),
                                    _I32, C.POINTER(pyg_join_opts), C.POINTER(pyg_join_result),
                                    C.POINTER(pyg_join_stats)]),
+    ("pyg_hashjoin_agg_noalloc", C.c_int, [_P, _I64, _P, _I64, _P, _P]),
     ("pyg_groupby", C.c_int, [_P, C.POINTER(pyg_rel), _PI32, _I32, _I32, _I32, _I32, _I64, _P, _I64, _PI64]),
     ("pyg_partition", C.c_int, [_P, C.POINTER(pyg_rel), _I32, C.POINTER(pyg_splitter), _P, _PI64]),
     ("pyg_sort", C.c_int, [_P, C.POINTER(pyg_rel), _I32, _P]),
