@@ -43,7 +43,7 @@ CPU_SAMPLE_SHIFT = 4
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--theta", type=float, default=0.0)
     ap.add_argument("--impl", default="pyg", choices=["pyg", "reference"])
@@ -59,27 +59,52 @@ def parse():
 # ---------------------------------------------------------------- helpers
 
 class Clocks:
-    """Samples nvidia-smi clocks / throttle reasons during the timed region."""
+    """Samples SM clocks and clock-event (throttle) reasons every 20 ms during
+    the timed region through NVML (read-only queries), else nvidia-smi."""
 
     Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    BITS = [0x8, 0x40, 0x20, 0x4]  # NVML clocks-event reason masks, in NAMES order
 
     def __init__(self, index):
         self.index = index
-        self.samples = []
+        self.samples = []  # (sm_mhz, max_mhz, [active reason names])
         self._stop = threading.Event()
         self._t = None
 
+    def _handle(self):
+        try:
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return None
+
     def _run(self):
+        nv = self._handle()
         while not self._stop.is_set():
             try:
-                r = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                    "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                if r.returncode == 0 and r.stdout.strip():
-                    self.samples.append([x.strip() for x in r.stdout.strip().split(",")])
+                if nv:
+                    m, h = nv
+                    sm = m.nvmlDeviceGetClockInfo(h, m.NVML_CLOCK_SM)
+                    mx = m.nvmlDeviceGetMaxClockInfo(h, m.NVML_CLOCK_SM)
+                    bits = m.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((float(sm), float(mx), [n for n, b in zip(self.NAMES, self.BITS) if bits & b]))
+                else:
+                    r = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                        "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                    f = [x.strip() for x in r.stdout.strip().split(",")]
+                    if r.returncode == 0 and len(f) == 6:
+                        self.samples.append((float(f[0]), float(f[1]),
+                                             [n for n, v in zip(self.NAMES, f[2:]) if v == "Active"]))
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(0.02 if nv else 0.2)
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -92,13 +117,10 @@ class Clocks:
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(x[0] for x in self.samples),
+                "sm_max_mhz": max(x[1] for x in self.samples),
+                "reasons": sorted({n for x in self.samples for n in x[2]}), "samples": len(self.samples)}
 
 
 def peaks():
@@ -166,6 +188,17 @@ def run_reference_cpu(theta, steps, shift=CPU_SAMPLE_SHIFT):
         times.append(time.perf_counter() - t0)
     return {"kind": "port", "cores": 1, "sample": sample + ", C oracle single thread", "times": times,
             "tuples": n_tuples}
+
+
+def max_over_ranks(ms, dist, device):
+    """The job's time: the slowest rank's device-timed milliseconds."""
+    if dist is None:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def dist_env():
@@ -247,51 +280,55 @@ def main_gpu(args):
 
     for _ in range(args.warmup):
         step(Rr, Sr)
-    # Phase timings (CUDA events inside the library, on the same stream)
-    # from separate untimed steps, so the timed steps carry no extra events.
-    phase = [step(Rr, Sr, stats=True)[2] for _ in range(3)]
     launches0 = ctx.launches()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
+    # Each timed step also reports its phase times: CUDA events the library
+    # records on the stream its kernels run on (the step synchronises on its
+    # result anyway, so they add no wait).
+    phase = []
     with Clocks(local) as clk:
         t_start.record(stream)
         for k in range(args.steps):
-            step(Rr, Sr)
+            phase.append(step(Rr, Sr, stats=True)[2])
         t_end.record(stream)
         torch.cuda.synchronize()
     launches = ctx.launches() - launches0
-    ms = t_start.elapsed_time(t_end)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(t_start.elapsed_time(t_end), dist, "cuda")
     value = (nR + nS) * args.steps * world / (ms / 1000.0)
 
     hbm, peak_kind = peaks()
-    med = lambda f: statistics.median(getattr(p, f) for p in phase)  # noqa: E731
-    # Algorithmic bytes per phase: every tuple read once (and written once
-    # by a partition pass).
-    phases = {
-        "build_partition": (med("build_partition_ms"), nR * 16 * 2),
-        "build": (med("build_ms"), nR * 16),
-        "probe_partition": (med("probe_partition_ms"), nS * 16 * 2),
-        "probe": (med("probe_ms"), nS * 16),
-    }
-    ph = {k: {"ms": round(v[0], 3), "bytes": v[1],
+    mean = lambda f: statistics.fmean(getattr(p, f) for p in phase)  # noqa: E731
+    radix = int(phase[0].algorithm) == pyg.JOIN_RADIX
+    two_pass = radix and int(phase[0].radix_bits) > 9
+    # Algorithmic bytes per phase: every tuple read once, and written once
+    # more by each partition pass.
+    if radix:
+        npass = 2 if two_pass else 1
+        phases = {
+            "histogram": (mean("histogram_ms"), (nR + nS) * 16, "rj_hist_kernel"),
+            "build_partition": (mean("build_partition_ms"), nR * 32 * npass, "rj_partition_kernel"),
+            "probe_partition": (mean("probe_partition_ms"), nS * 32 * npass, "rj_partition_kernel"),
+            "join": (mean("probe_ms"), (nR + nS) * 16, "rj_join_kernel"),
+        }
+    else:
+        phases = {
+            "build": (mean("build_ms"), nR * 16, "ht_build16_kernel"),
+            "probe": (mean("probe_ms"), nS * 16, "probe_agg16_kernel"),
+        }
+    ph = {k: {"ms": round(v[0], 3), "bytes": v[1], "kernel": v[2],
               "gbs": round(v[1] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else None,
               "frac": round(v[1] / (v[0] / 1e3) / 1e9 / hbm, 4) if v[0] > 0 else None} for k, v in phases.items()}
     top = max((k for k in ph if ph[k]["ms"] > 0), key=lambda k: ph[k]["ms"])
-    radix = int(phase[0].algorithm) == pyg.JOIN_RADIX
-    kernel_name = {"probe": "part_join_kernel" if radix else "probe_agg16_kernel",
-                   "probe_partition": "tile_partition16_kernel", "build": "ht_build16_kernel",
-                   "build_partition": "pt_scatter_kernel"}[top]
+    kernel_name = ph[top]["kernel"]
     step_bytes = (nR + nS) * 16
     roofline = {"bound": "hbm", "kernel": kernel_name, "phase": top, "achieved": ph[top]["gbs"], "peak": hbm,
                 "unit": "GB/s", "frac": ph[top]["frac"], "peak_source": peak_kind, "traffic": None,
                 "phases": ph, "algorithm": int(phase[0].algorithm), "radix_bits": int(phase[0].radix_bits),
+                "passes": (2 if two_pass else 1) if radix else 0,
                 "step_achieved_gbs": round(step_bytes / (ms / args.steps / 1000.0) / 1e9, 1),
                 "step_frac": round(step_bytes / (ms / args.steps / 1000.0) / 1e9 / hbm, 4)}
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
@@ -369,11 +406,7 @@ def run_e2e(args, torch, pyg, ctx, R, S, nR, nS, world, dist):
         t1.record(stream)
         torch.cuda.synchronize()
         assert c == nS
-        ms = t0.elapsed_time(t1)
-        if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(t0.elapsed_time(t1), dist, "cuda")
         return {"value": (nR + nS) * steps * world / (ms / 1000.0), "unit": UNIT,
                 "h2d_bytes_per_step": (nR + nS) * 16, "d2h_bytes_per_step": 2 * 8 * 4 + 9 * 8,
                 "ms_per_step": ms / steps, "host_buffers": "pinned"}

@@ -164,6 +164,7 @@ typedef struct pyg_join_stats {
     double probe_ms;            /* probes + fused aggregation           */
     int64_t overflow_tuples;
     int64_t padded_tuples;
+    double histogram_ms;        /* exact partition histograms (RADIX)   */
 } pyg_join_stats;
 
 int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_keys,

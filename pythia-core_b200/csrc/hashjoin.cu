@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "pyg_internal.cuh"
+#include "radixjoin.cuh"
 #include "hashtable.cuh"
 #include "partition.cuh"
 
@@ -565,288 +566,6 @@ static int probe16_stream_host(pyg_ctx* ctx, const pyg_hashtable* ht, const long
     return rc;
 }
 
-// ---------------------------------------------------------------------------
-// Hash-ordered radix join.  Build and probe relations are partitioned by
-// the top bits of mix64(key); the table's slot function (multiply-high of
-// the same hash) maps partition p to the p-th slice of the table, so a
-// partition's inserts and probes touch one L2-sized slice at a time.
-// The probe relation is partitioned in one pass (no histogram pass):
-// partition capacities come from a sample, each CTA stages a 4096-tuple
-// tile in shared memory grouped by partition and reserves space with one
-// atomic per (tile, partition), so runs are written contiguously.  Tuples
-// that do not fit (or carry the empty-marker key) go to an overflow area
-// probed separately; unused capacity is filled with empty-marker padding.
-
-constexpr int TP_THREADS = 512;
-constexpr int TP_TILE = 2048;
-
-__global__ void sample_part_hist_kernel(const longlong2* __restrict__ S, int64_t n, int64_t stride, int pbits,
-                                        unsigned long long* __restrict__ hist)
-{
-    extern __shared__ unsigned sh_hist[];
-    const int P = 1 << pbits;
-    for (int b = threadIdx.x; b < P; b += blockDim.x) sh_hist[b] = 0;
-    __syncthreads();
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j * stride < n; j += (int64_t)gridDim.x * blockDim.x) {
-        uint64_t k = (uint64_t)S[j * stride].x;
-        atomicAdd(&sh_hist[mix64(k) >> (64 - pbits)], 1u);
-    }
-    __syncthreads();
-    for (int b = threadIdx.x; b < P; b += blockDim.x)
-        if (sh_hist[b]) atomicAdd(&hist[b], (unsigned long long)sh_hist[b]);
-}
-
-__global__ void __launch_bounds__(TP_THREADS) tile_partition16_kernel(
-    const longlong2* __restrict__ S, int64_t n, int pbits, const unsigned long long* __restrict__ pstart,
-    const unsigned long long* __restrict__ pcap, unsigned long long* __restrict__ cursor, longlong2* __restrict__ out,
-    longlong2* __restrict__ ovf, unsigned long long* __restrict__ ovf_cursor, int64_t ovf_cap)
-{
-    extern __shared__ __align__(16) unsigned char tp_smem[];
-    const int P = 1 << pbits;
-    longlong2* stage = (longlong2*)tp_smem;
-    unsigned* hist = (unsigned*)(stage + TP_TILE);
-    unsigned* loff = hist + P;
-    unsigned long long* gbase = (unsigned long long*)(loff + P + (P & 1));
-    __shared__ unsigned warp_tot[TP_THREADS / 32];
-    __shared__ unsigned tile_n;
-    const int64_t ntiles = (n + TP_TILE - 1) / TP_TILE;
-    constexpr int PER = TP_TILE / TP_THREADS;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        for (int b = threadIdx.x; b < P; b += TP_THREADS) hist[b] = 0;
-        __syncthreads();
-        const int64_t base = tile * TP_TILE;
-        longlong2 t[PER];
-        unsigned bin[PER], rank[PER];
-#pragma unroll
-        for (int j = 0; j < PER; ++j) {
-            int64_t i = base + j * TP_THREADS + threadIdx.x;
-            bin[j] = 0xFFFFFFFFu;
-            if (i < n) {
-                t[j] = __ldcs(&S[i]);
-                uint64_t k = (uint64_t)t[j].x;
-                if (k == kEmptyKey) {
-                    unsigned long long o = atomicAdd(ovf_cursor, 1ULL);
-                    if ((int64_t)o < ovf_cap) ovf[o] = t[j];
-                } else {
-                    bin[j] = (unsigned)(mix64(k) >> (64 - pbits));
-                    rank[j] = atomicAdd(&hist[bin[j]], 1u);
-                }
-            }
-        }
-        __syncthreads();
-        // Exclusive scan of the tile histogram; each thread owns a run of
-        // consecutive bins.  Reserve global space per non-empty bin.
-        const int per = (P + TP_THREADS - 1) / TP_THREADS;
-        const int b0 = threadIdx.x * per;
-        unsigned local = 0;
-        for (int b = b0; b < b0 + per && b < P; ++b) local += hist[b];
-        unsigned incl = local;
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
-        }
-        if (lane == 31) warp_tot[w] = incl;
-        __syncthreads();
-        if (w == 0) {
-            unsigned x = lane < TP_THREADS / 32 ? warp_tot[lane] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                unsigned v = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += v;
-            }
-            if (lane < TP_THREADS / 32) warp_tot[lane] = x;
-            if (lane == TP_THREADS / 32 - 1) tile_n = x;
-        }
-        __syncthreads();
-        unsigned run = incl - local + (w > 0 ? warp_tot[w - 1] : 0);
-        for (int b = b0; b < b0 + per && b < P; ++b) {
-            unsigned c = hist[b];
-            loff[b] = run;
-            run += c;
-            if (c) gbase[b] = atomicAdd(&cursor[b], (unsigned long long)c);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int j = 0; j < PER; ++j)
-            if (bin[j] != 0xFFFFFFFFu) stage[loff[bin[j]] + rank[j]] = t[j];
-        __syncthreads();
-        const unsigned cnt = tile_n;
-        for (unsigned i = threadIdx.x; i < cnt; i += TP_THREADS) {
-            longlong2 v = stage[i];
-            unsigned b = (unsigned)(mix64((uint64_t)v.x) >> (64 - pbits));
-            unsigned long long g = gbase[b] + (i - loff[b]);
-            if (g < pcap[b]) {
-                __stcs(&out[pstart[b] + g], v);
-            } else {
-                unsigned long long o = atomicAdd(ovf_cursor, 1ULL);
-                if ((int64_t)o < ovf_cap) ovf[o] = v;
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Partition-at-a-time join: one cooperative (co-resident) grid walks the
-// partitions in order.  For partition p it clears a table slice in one of
-// two reused buffers, inserts the build partition, then probes the probe
-// partition; two grid barriers separate the phases.  The two buffers are
-// sized to stay in L2, so the table never goes to HBM and every insert and
-// probe is an L2 hit; HBM traffic is one read of each partitioned
-// relation.  Slots are 32 bytes {key, payload sum, count, -}.  Barrier
-// waits are bounded: on timeout a flag is set, every CTA leaves, and the
-// host reports PYG_ERR_TIMEOUT.
-
-struct GridBarrier {
-    unsigned int count;
-    unsigned int gen;
-    unsigned int error;
-    unsigned int pad;
-};
-
-constexpr long long kBarrierSpinLimit = 1LL << 24;
-
-__device__ __forceinline__ unsigned ld_volatile_u32(const unsigned* p) { return *(volatile const unsigned*)p; }
-
-// Returns false (for every thread of the CTA) if the barrier timed out or an
-// earlier barrier did.
-__device__ bool grid_barrier(GridBarrier* b, unsigned nblocks)
-{
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        unsigned g = ld_volatile_u32(&b->gen);
-        int good = ld_volatile_u32(&b->error) == 0;
-        if (good) {
-            unsigned arrived = atomicAdd(&b->count, 1u) + 1;
-            if (arrived == nblocks) {
-                b->count = 0;
-                __threadfence();
-                atomicAdd(&b->gen, 1u);
-            } else {
-                good = 0;
-                for (long long i = 0; i < kBarrierSpinLimit; ++i) {
-                    if (ld_volatile_u32(&b->gen) != g) {
-                        good = 1;
-                        break;
-                    }
-                    if (ld_volatile_u32(&b->error)) break;
-                    __nanosleep(64);
-                }
-                if (!good) atomicOr(&b->error, 1u);
-            }
-        }
-        __threadfence();
-        ok = good;
-    }
-    __syncthreads();
-    return ok != 0;
-}
-
-struct PartJoinArgs {
-    const longlong2* R;                 // build relation partitioned by the top pbits hash bits
-    const unsigned long long* roff;     // P + 1 offsets
-    const longlong2* S;                 // probe partitions (tile-partitioned, with capacity gaps)
-    const unsigned long long* pstart;   // P partition starts in S
-    const unsigned long long* pcap;     // P capacities
-    const unsigned long long* pcount;   // P tuples written (may exceed capacity: overflow)
-    ulonglong4* slices;                 // two slice buffers of slice_cap slots
-    uint64_t slice_cap;
-    int pbits;
-    GridBarrier* bar;
-    unsigned long long* acc;            // count, build sum, probe sum
-};
-
-__device__ __forceinline__ uint64_t slice_slot(uint64_t h, int pbits, uint64_t cap)
-{
-    return __umul64hi(h << pbits, cap);
-}
-
-__global__ void __launch_bounds__(512) part_join_kernel(PartJoinArgs a)
-{
-    const int P = 1 << a.pbits;
-    const unsigned nblocks = gridDim.x;
-    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
-    uint64_t cnt = 0, bsum = 0, psum = 0;
-    for (int p = 0; p < P; ++p) {
-        ulonglong4* T = a.slices + (p & 1) * a.slice_cap;
-        for (int64_t i = tid; i < (int64_t)a.slice_cap; i += nthreads) T[i] = make_ulonglong4(kEmptyKey, 0, 0, 0);
-        if (!grid_barrier(a.bar, nblocks)) break;
-        for (int64_t i = (int64_t)a.roff[p] + tid; i < (int64_t)a.roff[p + 1]; i += nthreads) {
-            longlong2 t = a.R[i];
-            uint64_t k = (uint64_t)t.x;
-            if (k == kEmptyKey) continue;  // joined by the overflow path (probe keys equal to the marker go there)
-            uint64_t s = slice_slot(mix64(k), a.pbits, a.slice_cap);
-            for (uint64_t steps = 0; steps < a.slice_cap; ++steps) {
-                unsigned long long* slot = (unsigned long long*)&T[s];
-                unsigned long long prev = atomicCAS(slot, kEmptyKey, k);
-                if (prev == kEmptyKey || prev == k) {
-                    atomicAdd(slot + 1, (unsigned long long)t.y);
-                    atomicAdd(slot + 2, 1ULL);
-                    break;
-                }
-                s = (s + 1 == a.slice_cap) ? 0 : s + 1;
-            }
-        }
-        if (!grid_barrier(a.bar, nblocks)) break;
-        const int64_t s0 = (int64_t)a.pstart[p];
-        const int64_t s1 = s0 + (int64_t)(a.pcount[p] < a.pcap[p] ? a.pcount[p] : a.pcap[p]);
-        for (int64_t i = s0 + tid; i < s1; i += nthreads) {
-            longlong2 t = __ldcs(&a.S[i]);
-            uint64_t k = (uint64_t)t.x;
-            uint64_t s = slice_slot(mix64(k), a.pbits, a.slice_cap);
-            for (uint64_t steps = 0; steps < a.slice_cap; ++steps) {
-                ulonglong4 e = T[s];
-                if (e.x == k) {
-                    cnt += e.z;
-                    bsum += e.y;
-                    psum += e.z * (uint64_t)t.y;
-                    break;
-                }
-                if (e.x == kEmptyKey) break;
-                s = (s + 1 == a.slice_cap) ? 0 : s + 1;
-            }
-        }
-    }
-    cnt = warp_sum_u64(cnt);
-    bsum = warp_sum_u64(bsum);
-    psum = warp_sum_u64(psum);
-    if ((threadIdx.x & 31) == 0 && (cnt | bsum | psum)) {
-        atomicAdd(&a.acc[0], (unsigned long long)cnt);
-        atomicAdd(&a.acc[1], (unsigned long long)bsum);
-        atomicAdd(&a.acc[2], (unsigned long long)psum);
-    }
-}
-
-// Pads [start + min(cursor, cap), start + cap) of every partition with
-// empty-marker tuples.
-__global__ void fill_gaps_kernel(longlong2* __restrict__ out, int P, const unsigned long long* __restrict__ pstart,
-                                 const unsigned long long* __restrict__ pcap,
-                                 const unsigned long long* __restrict__ cursor)
-{
-    for (int b = blockIdx.x; b < P; b += gridDim.x) {
-        unsigned long long used = cursor[b] < pcap[b] ? cursor[b] : pcap[b];
-        for (unsigned long long i = used + threadIdx.x; i < pcap[b]; i += blockDim.x)
-            out[pstart[b] + i] = make_longlong2((long long)kEmptyKey, 0);
-    }
-}
-
-// Exact partitioning of the build relation by the same hash bits (the
-// histogram / scan / scatter partitioner).
-static int partition_by_hash(pyg_ctx* ctx, const pyg_rel* r, int pbits, void* out, unsigned long long* offs)
-{
-    BucketFn f;
-    memset(&f, 0, sizeof(f));
-    f.kind = PYG_SPLIT_HASH;
-    f.fanout = 1u << pbits;
-    f.log2f = pbits;
-    return partition_device(ctx, r, 0, f, out, offs);
-}
-
 struct PhaseTimer {
     static constexpr int N = 5;
     cudaEvent_t ev[N] = {};
@@ -1185,148 +904,16 @@ int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_ke
         }
         return rc;
     }
-    const int64_t nR = build->ntuples, nS = probe->ntuples;
-    int pbits = opts ? opts->radix_bits : 0;
-    if (pbits <= 0) {
-        // Two table slices of 32-byte slots at twice the partition size
-        // within about 40 MiB of L2.
-        double slices = 2.0 * 2.0 * (double)nR * 32.0;
-        pbits = 4;
-        while (pbits < 12 && slices / (double)(1 << pbits) > 40.0 * (1 << 20)) ++pbits;
-    }
-    if (pbits < 1 || pbits > 12) {
-        set_error("pyg_hashjoin_agg: radix bits must be in [1, 12]");
-        return PYG_ERR_ARG;
-    }
-    const int P = 1 << pbits;
-    tm.start(ctx, stats != nullptr);
-    void* Rp = nullptr;
-    unsigned long long* meta = nullptr;  // roffs[P+1] | hist[P] | pstart[P] | pcap[P] | cursor[P] | ovf
-    longlong2 *Sp = nullptr, *ovf = nullptr;
-    ulonglong4* slices = nullptr;
-    pyg_hashtable* ht = nullptr;
-    unsigned long long* acc = ctx->dcounters + 8;
-    GridBarrier* bar = (GridBarrier*)(ctx->dcounters + 128);
-    std::vector<unsigned long long> hh(3 * P);
-    std::vector<unsigned long long> ro(P + 1);
-    do {
-        if ((rc = dalloc(ctx, &Rp, (size_t)(nR > 0 ? nR : 1) * 16))) break;
-        if ((rc = dalloc(ctx, (void**)&meta, (size_t)(6 * P + 2) * 8))) break;
-        unsigned long long *roffs = meta, *hist = meta + P + 1, *pstart = hist + P, *pcap = pstart + P,
-                           *cursor = pcap + P, *ovf_cursor = cursor + P;
-        PYG_CUDA(cudaMemsetAsync(roffs, 0, (size_t)(P + 1) * 8, ctx->stream));
-        if (nR > 0 && (rc = partition_by_hash(ctx, build, pbits, Rp, roffs))) break;
-        tm.mark(ctx, 1);
-        tm.mark(ctx, 2);
-        // Probe side: sample histogram (about 2^20 samples) -> capacities
-        // -> one-pass tile partition.
-        int64_t stride = nS >> 20;
-        if (stride < 1) stride = 1;
-        PYG_CUDA(cudaMemsetAsync(hist, 0, (size_t)P * 8, ctx->stream));
-        PYG_CUDA(cudaMemsetAsync(cursor, 0, (size_t)(P + 1) * 8, ctx->stream));
-        if (nS > 0) {
-            sample_part_hist_kernel<<<grid_for(ctx, (nS + stride - 1) / stride, 256, 4, 4), 256, (size_t)P * 4,
-                                      ctx->stream>>>((const longlong2*)probe->base, nS, stride, pbits, hist);
-            PYG_LAUNCHED(ctx);
-        }
-        PYG_CUDA(cudaMemcpyAsync(hh.data(), hist, (size_t)P * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        PYG_CUDA(cudaMemcpyAsync(ro.data(), roffs, (size_t)(P + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-        unsigned long long total = 0;
-        for (int b = 0; b < P; ++b) {
-            double est = (double)hh[b] * (double)stride;
-            unsigned long long cap = (unsigned long long)(est * 1.06) + 2048;
-            hh[P + b] = total;
-            hh[2 * P + b] = cap;
-            total += cap;
-        }
-        int64_t ovf_cap = nS / 64 + (1 << 20);
-        if ((rc = dalloc(ctx, (void**)&Sp, (size_t)total * 16))) break;
-        if ((rc = dalloc(ctx, (void**)&ovf, (size_t)ovf_cap * 16))) break;
-        PYG_CUDA(cudaMemcpyAsync(pstart, hh.data() + P, (size_t)2 * P * 8, cudaMemcpyHostToDevice, ctx->stream));
-        PYG_CUDA(cudaMemsetAsync(acc, 0, (PYG_MAX_COLS + 1) * 8, ctx->stream));
-        size_t smem = (size_t)TP_TILE * 16 + (size_t)(2 * P + 2) * 4 + (size_t)P * 8;
-        PYG_CUDA(cudaFuncSetAttribute(tile_partition16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        if (nS > 0) {
-            int per_sm = (int)std::min<size_t>(2048 / TP_THREADS, (200 * 1024) / smem);
-            int grid = grid_for(ctx, (nS + TP_TILE - 1) / TP_TILE, 1, 1, per_sm > 0 ? per_sm : 1);  // one tile per unit
-            tile_partition16_kernel<<<grid, TP_THREADS, smem, ctx->stream>>>(
-                (const longlong2*)probe->base, nS, pbits, pstart, pcap, cursor, Sp, ovf, ovf_cursor, ovf_cap);
-            PYG_LAUNCHED(ctx);
-        }
-        unsigned long long* h = (unsigned long long*)ctx->pinned;
-        PYG_CUDA(cudaMemcpyAsync(h + 16, ovf_cursor, 8, cudaMemcpyDeviceToHost, ctx->stream));
-        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-        tm.mark(ctx, 3);
-        const int64_t novf = (int64_t)h[16];
-        if (novf > 0) {
-            // Probe tuples that did not fit their partition's sampled
-            // capacity, or whose key is the table's empty marker: join the
-            // whole input through one table instead (exact, rarely taken).
-            pyg_rel Rrel = *build;
-            Rrel.base = Rp;
-            const int32_t rpay[1] = {1};
-            if ((rc = pyg_hashjoin_build(ctx, &Rrel, build_keys, 1, rpay, 1, PYG_HT_AGGREGATE, lf, &ht))) break;
-            PYG_CUDA(cudaMemsetAsync(acc, 0, (PYG_MAX_COLS + 1) * 8, ctx->stream));
-            if ((rc = launch_probe16(ctx, ht, (const longlong2*)probe->base, nS, false, acc))) break;
-        } else if (nS > 0 && nR > 0) {
-            uint64_t maxr = 0;
-            for (int b = 0; b < P; ++b) maxr = std::max<uint64_t>(maxr, ro[b + 1] - ro[b]);
-            uint64_t slice_cap = (uint64_t)((double)maxr / lf) + 64;
-            if ((rc = dalloc(ctx, (void**)&slices, (size_t)2 * slice_cap * sizeof(ulonglong4)))) break;
-            PYG_CUDA(cudaMemsetAsync(bar, 0, sizeof(GridBarrier), ctx->stream));
-            PartJoinArgs ja;
-            ja.R = (const longlong2*)Rp;
-            ja.roff = roffs;
-            ja.S = Sp;
-            ja.pstart = pstart;
-            ja.pcap = pcap;
-            ja.pcount = cursor;
-            ja.slices = slices;
-            ja.slice_cap = slice_cap;
-            ja.pbits = pbits;
-            ja.bar = bar;
-            ja.acc = acc;
-            int per_sm = 0;
-            PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, part_join_kernel, 512, 0));
-            if (per_sm < 1) {
-                set_error("pyg_hashjoin_agg: partition join kernel cannot be resident");
-                rc = PYG_ERR_CUDA;
-                break;
-            }
-            void* kargs[] = {&ja};
-            PYG_CUDA(cudaLaunchCooperativeKernel((void*)part_join_kernel, dim3(ctx->sm_count * per_sm), dim3(512), kargs,
-                                                 0, ctx->stream));
-            PYG_LAUNCHED(ctx);
-        }
-        tm.mark(ctx, 4);
-        PYG_CUDA(cudaMemcpyAsync(h, acc, 3 * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        PYG_CUDA(cudaMemcpyAsync(h + 20, bar, sizeof(GridBarrier), cudaMemcpyDeviceToHost, ctx->stream));
-        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-        if (novf == 0 && ((GridBarrier*)(h + 20))->error) {
-            set_error("pyg_hashjoin_agg: a grid barrier of the partition join timed out");
-            rc = PYG_ERR_TIMEOUT;
-            break;
-        }
-        memset(out, 0, sizeof(*out));
-        out->count = (int64_t)h[0];
-        for (int p = 0; p < nproj; ++p) out->sums[p] = (int64_t)(proj[p].side ? h[2] : h[1]);
-        if (stats) {
-            tm.finish(stats);
-            stats->algorithm = PYG_JOIN_RADIX;
-            stats->radix_bits = pbits;
-            stats->overflow_tuples = novf;
-            stats->padded_tuples = (int64_t)total;
-        }
-        rc = PYG_OK;
-    } while (0);
-    dfree(ctx, slices);
-    if (ht) pyg_hashtable_free(ctx, ht);
-    dfree(ctx, Rp);
-    dfree(ctx, meta);
-    dfree(ctx, Sp);
-    dfree(ctx, ovf);
-    return rc;
+    // Radix path: exact two-level hash partitioning, then a join with one
+    // shared-memory table per CTA (radixjoin.cu).
+    unsigned long long r3[3];
+    if ((rc = radix_join16(ctx, build->base, build->ntuples, probe->base, probe->ntuples, opts ? opts->radix_bits : 0,
+                           r3, stats)))
+        return rc;
+    memset(out, 0, sizeof(*out));
+    out->count = (int64_t)r3[0];
+    for (int p = 0; p < nproj; ++p) out->sums[p] = (int64_t)(proj[p].side ? r3[2] : r3[1]);
+    return PYG_OK;
 }
 
 }  // extern "C"

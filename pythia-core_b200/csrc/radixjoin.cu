@@ -1,0 +1,647 @@
+// Radix hash join + aggregation with shared-memory tables.
+//
+// Restates the reference's partitioned hash join (the `hashjoin` node over
+// `partition` outputs, operators/hashjoin.cpp and operators/partition.cpp)
+// for the 16-byte (int64 key, int64 payload) case, B200-first:
+//
+//   1. histogram  one read of each relation counts the top `fine_bits`
+//                 bits of mix64(key) in a shared-memory histogram per CTA;
+//                 the host turns the counts into exact partition offsets.
+//   2. partition  one or two tile passes (coarse bits, then the remaining
+//                 bits inside each coarse partition).  A CTA groups a
+//                 2048-tuple tile by partition in shared memory and writes
+//                 each group as one contiguous run; exact offsets mean no
+//                 capacity slack and no overflow path.
+//   3. join       a persistent kernel takes work items (a build partition,
+//                 or a chunk of it, and a chunk of the matching probe
+//                 partition) from a queue.  The CTA builds the partition's
+//                 table in 192 KB of shared memory, then streams the probe
+//                 chunk from HBM against it.  No grid-wide barrier: CTAs
+//                 never wait for one another, and table lookups never leave
+//                 the SM.
+//
+// Build keys equal to the table's empty marker (INT64_MIN) are counted on
+// the side per work item: they all hash to one fine partition, as do the
+// probe keys they match.
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "pyg_internal.cuh"
+#include "radixjoin.cuh"
+
+namespace pyg {
+
+constexpr int RJ_TILE = 2048;        // tuples per partition tile
+constexpr int RJ_PT_THREADS = 512;   // partition CTA
+constexpr int RJ_JOIN_THREADS = 1024;
+constexpr int RJ_PROBE_UNROLL = 8;   // probe tuples in flight per thread
+constexpr int RJ_TABLE_BYTES = 192 * 1024;
+constexpr int RJ_SLOTS_UNIQUE = RJ_TABLE_BYTES / 16;   // {key, payload}
+constexpr int RJ_SLOTS_COUNTED = RJ_TABLE_BYTES / 32;  // {key, payload sum, count, -}
+constexpr int64_t RJ_SCHUNK = 1 << 16;                 // probe tuples per work item (at most)
+constexpr int RJ_MAX_LOCAL_BITS = 9;                   // bins of one partition pass
+
+__device__ __forceinline__ unsigned rj_bin(uint64_t h, int shift, unsigned mask)
+{
+    return shift >= 64 ? 0u : (unsigned)(h >> shift) & mask;
+}
+
+// ---------------------------------------------------------------------------
+// 1. Histogram of the top `bits` hash bits (bits <= 15: 128 KB of shared
+// counters per CTA).
+
+__global__ void __launch_bounds__(1024) rj_hist_kernel(const longlong2* __restrict__ in, int64_t n, int bits,
+                                                       unsigned long long* __restrict__ hist)
+{
+    extern __shared__ unsigned rj_sh_hist[];
+    const int P = 1 << bits;
+    const int shift = 64 - bits;
+    for (int b = threadIdx.x; b < P; b += blockDim.x) rj_sh_hist[b] = 0;
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    constexpr int U = 8;
+    for (; i + (U - 1) * stride < n; i += U * stride) {
+        longlong2 t[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) t[u] = __ldcs(&in[i + u * stride]);
+#pragma unroll
+        for (int u = 0; u < U; ++u) atomicAdd(&rj_sh_hist[rj_bin(mix64((uint64_t)t[u].x), shift, P - 1)], 1u);
+    }
+    for (; i < n; i += stride) atomicAdd(&rj_sh_hist[rj_bin(mix64((uint64_t)__ldcs(&in[i]).x), shift, P - 1)], 1u);
+    __syncthreads();
+    for (int b = threadIdx.x; b < P; b += blockDim.x)
+        if (rj_sh_hist[b]) atomicAdd(&hist[b], (unsigned long long)rj_sh_hist[b]);
+}
+
+// ---------------------------------------------------------------------------
+// 2. Tile partition pass with exact offsets.  The input is a sequence of
+// segments (one for the first pass; the coarse partitions for the second);
+// tiles never straddle a segment.  Output bin of a tuple = (segment <<
+// lbits) | ((mix64(key) >> shift) & mask).
+
+struct RJPass {
+    const longlong2* in;
+    longlong2* out;
+    const unsigned long long* seg_start;  // nseg + 1 exact segment bounds in `in`
+    const unsigned long long* seg_tile0;  // nseg + 1 prefix of tiles per segment
+    int nseg;
+    int shift;
+    unsigned mask;
+    int lbits;
+    const unsigned long long* bin_start;  // exact output start per output bin
+    unsigned long long* cursor;           // per output bin, zeroed before the pass
+};
+
+struct RJTileRange {
+    long long begin, end;
+    int seg;
+};
+
+__device__ RJTileRange rj_tile_range(const RJPass& a, long long tile)
+{
+    int lo = 0, hi = a.nseg;  // seg_tile0[lo] <= tile < seg_tile0[hi]
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if ((long long)a.seg_tile0[mid] <= tile) lo = mid;
+        else hi = mid;
+    }
+    RJTileRange r;
+    r.seg = lo;
+    r.begin = (long long)a.seg_start[lo] + (tile - (long long)a.seg_tile0[lo]) * RJ_TILE;
+    r.end = min(r.begin + RJ_TILE, (long long)a.seg_start[lo + 1]);
+    return r;
+}
+
+__global__ void __launch_bounds__(RJ_PT_THREADS, 2) rj_partition_kernel(RJPass a, long long ntiles)
+{
+    constexpr int PER = RJ_TILE / RJ_PT_THREADS;
+    constexpr int LMAX = 1 << RJ_MAX_LOCAL_BITS;
+    __shared__ __align__(16) longlong2 stage[RJ_TILE];
+    __shared__ unsigned short stage_bin[RJ_TILE];
+    __shared__ unsigned hist[LMAX], loff[LMAX];
+    __shared__ unsigned long long gbase[LMAX];
+    __shared__ unsigned warp_tot[RJ_PT_THREADS / 32];
+    __shared__ unsigned tile_n;
+    __shared__ RJTileRange next_range;
+    const int L = 1 << a.lbits;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+
+    // Software pipeline: the next tile's loads are issued before the
+    // current tile is grouped and written out.
+    if (threadIdx.x == 0 && blockIdx.x < ntiles) next_range = rj_tile_range(a, blockIdx.x);
+    __syncthreads();
+    RJTileRange nr = next_range;
+    longlong2 nxt[PER];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        long long i = nr.begin + j * RJ_PT_THREADS + threadIdx.x;
+        if (blockIdx.x < ntiles && i < nr.end) nxt[j] = __ldcs(&a.in[i]);
+    }
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const RJTileRange cur = nr;
+        __syncthreads();  // previous tile finished with shared memory
+        for (int b = threadIdx.x; b < L; b += RJ_PT_THREADS) hist[b] = 0;
+        if (threadIdx.x == 0 && tile + gridDim.x < ntiles) next_range = rj_tile_range(a, tile + gridDim.x);
+        __syncthreads();
+        longlong2 t[PER];
+#pragma unroll
+        for (int j = 0; j < PER; ++j) t[j] = nxt[j];
+        if (tile + gridDim.x < ntiles) {
+            nr = next_range;
+#pragma unroll
+            for (int j = 0; j < PER; ++j) {
+                long long i = nr.begin + j * RJ_PT_THREADS + threadIdx.x;
+                if (i < nr.end) nxt[j] = __ldcs(&a.in[i]);
+            }
+        }
+        unsigned bin[PER], rank[PER];
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            long long i = cur.begin + j * RJ_PT_THREADS + threadIdx.x;
+            bin[j] = 0xFFFFFFFFu;
+            if (i < cur.end) {
+                bin[j] = rj_bin(mix64((uint64_t)t[j].x), a.shift, a.mask);
+                rank[j] = atomicAdd(&hist[bin[j]], 1u);
+            }
+        }
+        __syncthreads();
+        // Exclusive scan of the tile histogram (each thread owns a run of
+        // consecutive bins), then one global reservation per non-empty bin.
+        const int per = (L + RJ_PT_THREADS - 1) / RJ_PT_THREADS;
+        const int b0 = threadIdx.x * per;
+        unsigned local = 0;
+        for (int b = b0; b < b0 + per && b < L; ++b) local += hist[b];
+        unsigned incl = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) warp_tot[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            unsigned x = lane < RJ_PT_THREADS / 32 ? warp_tot[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                unsigned v = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += v;
+            }
+            if (lane < RJ_PT_THREADS / 32) warp_tot[lane] = x;
+            if (lane == RJ_PT_THREADS / 32 - 1) tile_n = x;
+        }
+        __syncthreads();
+        unsigned run = incl - local + (w > 0 ? warp_tot[w - 1] : 0);
+        const unsigned obase = (unsigned)cur.seg << a.lbits;
+        for (int b = b0; b < b0 + per && b < L; ++b) {
+            unsigned c = hist[b];
+            loff[b] = run;
+            run += c;
+            if (c) gbase[b] = a.bin_start[obase | b] + atomicAdd(&a.cursor[obase | b], (unsigned long long)c);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < PER; ++j)
+            if (bin[j] != 0xFFFFFFFFu) {
+                const unsigned s = loff[bin[j]] + rank[j];
+                stage[s] = t[j];
+                stage_bin[s] = (unsigned short)bin[j];
+            }
+        __syncthreads();
+        const unsigned cnt = tile_n;
+        for (unsigned i = threadIdx.x; i < cnt; i += RJ_PT_THREADS) {
+            const unsigned b = stage_bin[i];
+            __stcs(&a.out[gbase[b] + (i - loff[b])], stage[i]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3. Join: persistent CTAs, one shared-memory table each.
+
+struct RJItem {
+    unsigned long long r0, s0;  // first build / probe tuple of the item
+    unsigned rn, sn;            // build tuples (<= table capacity / 2), probe tuples
+};
+
+struct RJJoinArgs {
+    const longlong2* R;
+    const longlong2* S;
+    const RJItem* items;
+    long long nitems;
+    unsigned* next;             // work queue head, zeroed
+    int fine_bits;              // the table's slot uses the hash bits below these
+    unsigned long long* acc;    // count, build sum, probe sum
+    unsigned* dup;              // set when a build key repeats (UNIQUE)
+};
+
+template <bool UNIQUE>
+__global__ void __launch_bounds__(RJ_JOIN_THREADS, 1) rj_join_kernel(RJJoinArgs a)
+{
+    extern __shared__ __align__(16) unsigned char rj_table[];
+    constexpr int TS = UNIQUE ? RJ_SLOTS_UNIQUE : RJ_SLOTS_COUNTED;
+    constexpr int U = RJ_PROBE_UNROLL;
+    __shared__ long long item_idx;
+    __shared__ unsigned long long side_cnt, side_sum;
+    ulonglong2* T2 = reinterpret_cast<ulonglong2*>(rj_table);  // UNIQUE slots
+    ulonglong4* T4 = reinterpret_cast<ulonglong4*>(rj_table);  // counted slots
+    uint64_t cnt = 0, bsum = 0, psum = 0;
+    bool dup = false;
+    const int fb = a.fine_bits;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            item_idx = (long long)atomicAdd(a.next, 1u);
+            side_cnt = side_sum = 0;
+        }
+        for (int i = threadIdx.x; i < TS; i += RJ_JOIN_THREADS) {
+            if constexpr (UNIQUE) T2[i] = make_ulonglong2(kEmptyKey, 0);
+            else T4[i] = make_ulonglong4(kEmptyKey, 0, 0, 0);
+        }
+        __syncthreads();
+        const long long it = item_idx;
+        if (it >= a.nitems) break;
+        const RJItem item = a.items[it];
+        // Build: linear probing with 64-bit shared-memory CAS.  At most
+        // TS / 2 tuples per item, so a free slot always exists.
+        for (unsigned i = threadIdx.x; i < item.rn; i += RJ_JOIN_THREADS) {
+            const longlong2 t = a.R[item.r0 + i];
+            const uint64_t k = (uint64_t)t.x;
+            if (k == kEmptyKey) {
+                atomicAdd(&side_cnt, 1ULL);
+                atomicAdd(&side_sum, (unsigned long long)t.y);
+                continue;
+            }
+            unsigned pos = (unsigned)__umul64hi(mix64(k) << fb, (uint64_t)TS);
+            for (int steps = 0; steps < TS; ++steps) {
+                unsigned long long* key = UNIQUE ? &T2[pos].x : &T4[pos].x;
+                const unsigned long long prev = atomicCAS(key, kEmptyKey, k);
+                if (prev == kEmptyKey || prev == k) {
+                    if constexpr (UNIQUE) {
+                        if (prev == k) dup = true;
+                        else T2[pos].y = (unsigned long long)t.y;  // the CAS owns the slot
+                    } else {
+                        atomicAdd(&T4[pos].y, (unsigned long long)t.y);
+                        atomicAdd(&T4[pos].z, 1ULL);
+                    }
+                    break;
+                }
+                pos = pos + 1 == TS ? 0 : pos + 1;
+            }
+        }
+        __syncthreads();
+        const uint64_t scnt = side_cnt, ssum = side_sum;
+        if (UNIQUE && scnt > 1) dup = true;
+        // Probe: U independent streaming loads per thread, lookups in
+        // shared memory.
+        const longlong2* S = a.S + item.s0;
+        for (unsigned i = threadIdx.x; i < item.sn; i += U * RJ_JOIN_THREADS) {
+            longlong2 t[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const unsigned j = i + u * RJ_JOIN_THREADS;
+                if (j < item.sn) t[u] = __ldcs(&S[j]);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const unsigned j = i + u * RJ_JOIN_THREADS;
+                if (j >= item.sn) continue;
+                const uint64_t k = (uint64_t)t[u].x;
+                if (k == kEmptyKey) {
+                    cnt += scnt;
+                    bsum += ssum;
+                    psum += scnt * (uint64_t)t[u].y;
+                    continue;
+                }
+                unsigned pos = (unsigned)__umul64hi(mix64(k) << fb, (uint64_t)TS);
+                for (int steps = 0; steps < TS; ++steps) {
+                    if constexpr (UNIQUE) {
+                        const ulonglong2 e = T2[pos];
+                        if (e.x == k) {
+                            cnt += 1;
+                            bsum += e.y;
+                            psum += (uint64_t)t[u].y;
+                            break;
+                        }
+                        if (e.x == kEmptyKey) break;
+                    } else {
+                        const ulonglong4 e = T4[pos];
+                        if (e.x == k) {
+                            cnt += e.z;
+                            bsum += e.y;
+                            psum += e.z * (uint64_t)t[u].y;
+                            break;
+                        }
+                        if (e.x == kEmptyKey) break;
+                    }
+                    pos = pos + 1 == TS ? 0 : pos + 1;
+                }
+            }
+        }
+        __syncthreads();  // table and item slots are reused by the next item
+    }
+    cnt = warp_sum_u64(cnt);
+    bsum = warp_sum_u64(bsum);
+    psum = warp_sum_u64(psum);
+    if ((threadIdx.x & 31) == 0 && (cnt | bsum | psum)) {
+        atomicAdd(&a.acc[0], (unsigned long long)cnt);
+        atomicAdd(&a.acc[1], (unsigned long long)bsum);
+        atomicAdd(&a.acc[2], (unsigned long long)psum);
+    }
+    if (__any_sync(0xffffffffu, dup) && (threadIdx.x & 31) == 0) atomicOr(a.dup, 1u);
+}
+
+// ---------------------------------------------------------------------------
+// Host driver.
+
+namespace {
+
+struct RJEvents {
+    static constexpr int N = 5;
+    cudaEvent_t ev[N] = {};
+    bool on = false;
+    void start(pyg_ctx* ctx, bool enable)
+    {
+        on = enable;
+        if (!on) return;
+        for (auto& e : ev) cudaEventCreate(&e);
+        cudaEventRecord(ev[0], ctx->stream);
+    }
+    void mark(pyg_ctx* ctx, int i)
+    {
+        if (on) cudaEventRecord(ev[i], ctx->stream);
+    }
+    float ms(int a, int b)
+    {
+        float m = 0.f;
+        cudaEventElapsedTime(&m, ev[a], ev[b]);
+        return m;
+    }
+    ~RJEvents()
+    {
+        if (on)
+            for (auto& e : ev) cudaEventDestroy(e);
+    }
+};
+
+// Work items: every (build chunk, probe chunk) pair of every fine partition
+// with both sides non-empty.
+void make_items(const std::vector<unsigned long long>& hr, const std::vector<unsigned long long>& hs,
+                const std::vector<unsigned long long>& rs, const std::vector<unsigned long long>& ss, unsigned rcap,
+                std::vector<RJItem>& items)
+{
+    items.clear();
+    const size_t F = hr.size();
+    for (size_t f = 0; f < F; ++f) {
+        const unsigned long long rn = hr[f], sn = hs[f];
+        if (!rn || !sn) continue;
+        for (unsigned long long r = 0; r < rn; r += rcap)
+            for (unsigned long long s = 0; s < sn; s += RJ_SCHUNK) {
+                RJItem it;
+                it.r0 = rs[f] + r;
+                it.s0 = ss[f] + s;
+                it.rn = (unsigned)std::min<unsigned long long>(rcap, rn - r);
+                it.sn = (unsigned)std::min<unsigned long long>(RJ_SCHUNK, sn - s);
+                items.push_back(it);
+            }
+    }
+}
+
+int launch_pass(pyg_ctx* ctx, const RJPass& p, long long ntiles)
+{
+    if (ntiles <= 0) return PYG_OK;
+    int per_sm = 0;
+    PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rj_partition_kernel, RJ_PT_THREADS, 0));
+    if (per_sm < 1) per_sm = 1;
+    long long grid = std::min<long long>(ntiles, (long long)ctx->sm_count * per_sm);
+    rj_partition_kernel<<<(unsigned)grid, RJ_PT_THREADS, 0, ctx->stream>>>(p, ntiles);
+    PYG_LAUNCHED(ctx);
+    return PYG_OK;
+}
+
+}  // namespace
+
+int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t nS, int fine_bits,
+                 unsigned long long out[3], pyg_join_stats* stats)
+{
+    const longlong2* R = (const longlong2*)Rv;
+    const longlong2* S = (const longlong2*)Sv;
+    out[0] = out[1] = out[2] = 0;
+    if (fine_bits <= 0) {
+        // Fine partitions of about 0.7 x the table's build capacity.
+        fine_bits = 1;
+        while (fine_bits < RJ_MAX_FINE_BITS &&
+               (double)nR / (double)(1 << fine_bits) > 0.7 * (RJ_SLOTS_UNIQUE / 2))
+            ++fine_bits;
+    }
+    if (fine_bits < 1 || fine_bits > RJ_MAX_FINE_BITS) {
+        set_error("pyg_hashjoin_agg: radix bits must be in [1, %d]", RJ_MAX_FINE_BITS);
+        return PYG_ERR_ARG;
+    }
+    const int FB = fine_bits;
+    const bool two = FB > RJ_MAX_LOCAL_BITS;
+    const int CB = two ? (FB + 1) / 2 : FB;
+    const int F = 1 << FB, C = 1 << CB;
+    if (stats) {
+        stats->algorithm = PYG_JOIN_RADIX;
+        stats->radix_bits = FB;
+    }
+    if (nR == 0 || nS == 0) return PYG_OK;
+
+    RJEvents tm;
+    tm.start(ctx, stats != nullptr);
+    // Device metadata (u64 words):
+    //   histR[F] histS[F] | fineR[F+1] fineS[F+1] | coarseR[C+1] coarseS[C+1]
+    //   | tilesR[C+1] tilesS[C+1] | curR1[C] curS1[C] curR2[F] curS2[F]
+    //   | whole[4] = {0, nR, 0, nS} | wtiles[4] = {0, tiles(R), 0, tiles(S)}
+    const size_t nmeta = 2 * (size_t)F + 2 * (size_t)(F + 1) + 4 * (size_t)(C + 1) + 2 * (size_t)C + 2 * (size_t)F + 8;
+    unsigned long long* meta = nullptr;
+    void *R1 = nullptr, *R2 = nullptr, *S1 = nullptr, *S2 = nullptr;
+    RJItem* ditems = nullptr;
+    int rc = PYG_OK;
+    do {
+        if ((rc = dalloc(ctx, (void**)&meta, nmeta * 8))) break;
+        unsigned long long* histR = meta;
+        unsigned long long* histS = histR + F;
+        unsigned long long* fineR = histS + F;
+        unsigned long long* fineS = fineR + F + 1;
+        unsigned long long* coarseR = fineS + F + 1;
+        unsigned long long* coarseS = coarseR + C + 1;
+        unsigned long long* tilesR = coarseS + C + 1;
+        unsigned long long* tilesS = tilesR + C + 1;
+        unsigned long long* curR1 = tilesS + C + 1;
+        unsigned long long* curS1 = curR1 + C;
+        unsigned long long* curR2 = curS1 + C;
+        unsigned long long* curS2 = curR2 + F;
+        unsigned long long* whole = curS2 + F;  // single-segment bounds of the unpartitioned inputs
+        unsigned long long* wtiles = whole + 4;
+        PYG_CUDA(cudaMemsetAsync(meta, 0, nmeta * 8, ctx->stream));
+
+        // 1. Histograms.
+        const size_t hsm = (size_t)F * 4;
+        PYG_CUDA(cudaFuncSetAttribute(rj_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
+        int hper = 0;
+        PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&hper, rj_hist_kernel, 1024, hsm));
+        if (hper < 1) hper = 1;
+        rj_hist_kernel<<<ctx->sm_count * hper, 1024, hsm, ctx->stream>>>(R, nR, FB, histR);
+        PYG_LAUNCHED(ctx);
+        rj_hist_kernel<<<ctx->sm_count * hper, 1024, hsm, ctx->stream>>>(S, nS, FB, histS);
+        PYG_LAUNCHED(ctx);
+        std::vector<unsigned long long> hr(F), hs(F);
+        PYG_CUDA(cudaMemcpyAsync(hr.data(), histR, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(hs.data(), histS, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+
+        // Host: exact offsets, tile prefixes, work items.
+        const int sub = FB - CB;
+        std::vector<unsigned long long> up((size_t)2 * (F + 1) + 4 * (size_t)(C + 1));
+        unsigned long long* fR = up.data();
+        unsigned long long* fS = fR + F + 1;
+        unsigned long long* cR = fS + F + 1;
+        unsigned long long* cS = cR + C + 1;
+        unsigned long long* tR = cS + C + 1;
+        unsigned long long* tS = tR + C + 1;
+        fR[0] = fS[0] = 0;
+        for (int f = 0; f < F; ++f) {
+            fR[f + 1] = fR[f] + hr[f];
+            fS[f + 1] = fS[f] + hs[f];
+        }
+        if (fR[F] != (unsigned long long)nR || fS[F] != (unsigned long long)nS) {
+            set_error("pyg_hashjoin_agg: partition histogram does not add up");
+            rc = PYG_ERR_CUDA;
+            break;
+        }
+        tR[0] = tS[0] = 0;
+        for (int c = 0; c <= C; ++c) {
+            cR[c] = fR[(size_t)c << sub];
+            cS[c] = fS[(size_t)c << sub];
+        }
+        for (int c = 0; c < C; ++c) {
+            tR[c + 1] = tR[c] + (cR[c + 1] - cR[c] + RJ_TILE - 1) / RJ_TILE;
+            tS[c + 1] = tS[c] + (cS[c + 1] - cS[c] + RJ_TILE - 1) / RJ_TILE;
+        }
+        const long long ntR = (nR + RJ_TILE - 1) / RJ_TILE, ntS = (nS + RJ_TILE - 1) / RJ_TILE;
+        const unsigned long long wh[8] = {0, (unsigned long long)nR, 0, (unsigned long long)nS,
+                                          0, (unsigned long long)ntR, 0, (unsigned long long)ntS};
+        std::vector<RJItem> items;
+        std::vector<unsigned long long> rstart(fR, fR + F), sstart(fS, fS + F);
+        make_items(hr, hs, rstart, sstart, RJ_SLOTS_UNIQUE / 2, items);
+        PYG_CUDA(cudaMemcpyAsync(fineR, up.data(), up.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(whole, wh, sizeof(wh), cudaMemcpyHostToDevice, ctx->stream));
+        if (!items.empty()) {
+            if ((rc = dalloc(ctx, (void**)&ditems, items.size() * sizeof(RJItem)))) break;
+            PYG_CUDA(cudaMemcpyAsync(ditems, items.data(), items.size() * sizeof(RJItem), cudaMemcpyHostToDevice,
+                                     ctx->stream));
+        }
+        tm.mark(ctx, 1);
+
+        // 2. Partition passes.
+        if ((rc = dalloc(ctx, &R1, (size_t)nR * 16)) || (rc = dalloc(ctx, &S1, (size_t)nS * 16))) break;
+        if (two && ((rc = dalloc(ctx, &R2, (size_t)nR * 16)) || (rc = dalloc(ctx, &S2, (size_t)nS * 16)))) break;
+        auto run_side = [&](const longlong2* in, const unsigned long long* seg, const unsigned long long* segt,
+                            long long ntiles, unsigned long long* coarse, unsigned long long* cur1,
+                            unsigned long long* fine, unsigned long long* cur2, unsigned long long* tiles, void* o1,
+                            void* o2, long long ntiles2) -> int {
+            RJPass p;
+            p.in = in;
+            p.out = (longlong2*)o1;
+            p.seg_start = seg;
+            p.seg_tile0 = segt;
+            p.nseg = 1;
+            p.shift = 64 - CB;
+            p.mask = (unsigned)(C - 1);
+            p.lbits = CB;
+            p.bin_start = two ? coarse : fine;
+            p.cursor = two ? cur1 : cur2;
+            int r = launch_pass(ctx, p, ntiles);
+            if (r || !two) return r;
+            p.in = (const longlong2*)o1;
+            p.out = (longlong2*)o2;
+            p.seg_start = coarse;
+            p.seg_tile0 = tiles;
+            p.nseg = C;
+            p.shift = 64 - FB;
+            p.mask = (unsigned)((1 << sub) - 1);
+            p.lbits = sub;
+            p.bin_start = fine;
+            p.cursor = cur2;
+            return launch_pass(ctx, p, ntiles2);
+        };
+        if ((rc = run_side(R, whole, wtiles, ntR, coarseR, curR1, fineR, curR2, tilesR, R1, R2, (long long)tR[C])))
+            break;
+        tm.mark(ctx, 2);
+        if ((rc = run_side(S, whole + 2, wtiles + 2, ntS, coarseS, curS1, fineS, curS2, tilesS, S1, S2,
+                           (long long)tS[C])))
+            break;
+        tm.mark(ctx, 3);
+
+        // 3. Join: distinct build keys first (16-byte slots); on a repeated
+        // key, again with counted 32-byte slots and smaller build chunks.
+        const longlong2* Rf = (const longlong2*)(two ? R2 : R1);
+        const longlong2* Sf = (const longlong2*)(two ? S2 : S1);
+        unsigned long long* acc = ctx->dcounters + 8;
+        unsigned* next = (unsigned*)(ctx->dcounters + 200);  // word 200: queue head, word 201: dup flag
+        unsigned* dupf = (unsigned*)(ctx->dcounters + 201);
+        unsigned long long* h = (unsigned long long*)ctx->pinned;
+        for (int pass = 0; pass < 2 && !items.empty(); ++pass) {
+            const bool unique = pass == 0;
+            if (!unique) {
+                make_items(hr, hs, rstart, sstart, RJ_SLOTS_COUNTED / 2, items);
+                dfree(ctx, ditems);
+                ditems = nullptr;
+                if ((rc = dalloc(ctx, (void**)&ditems, items.size() * sizeof(RJItem)))) break;
+                PYG_CUDA(cudaMemcpyAsync(ditems, items.data(), items.size() * sizeof(RJItem), cudaMemcpyHostToDevice,
+                                         ctx->stream));
+            }
+            void* fn = unique ? (void*)rj_join_kernel<true> : (void*)rj_join_kernel<false>;
+            PYG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, RJ_TABLE_BYTES));
+            PYG_CUDA(cudaMemsetAsync(acc, 0, 3 * 8, ctx->stream));
+            PYG_CUDA(cudaMemsetAsync(next, 0, 16, ctx->stream));
+            RJJoinArgs ja;
+            ja.R = Rf;
+            ja.S = Sf;
+            ja.items = ditems;
+            ja.nitems = (long long)items.size();
+            ja.next = next;
+            ja.fine_bits = FB;
+            ja.acc = acc;
+            ja.dup = dupf;
+            const unsigned grid = (unsigned)std::min<long long>((long long)ctx->sm_count, ja.nitems);
+            if (unique) rj_join_kernel<true><<<grid, RJ_JOIN_THREADS, RJ_TABLE_BYTES, ctx->stream>>>(ja);
+            else rj_join_kernel<false><<<grid, RJ_JOIN_THREADS, RJ_TABLE_BYTES, ctx->stream>>>(ja);
+            PYG_LAUNCHED(ctx);
+            PYG_CUDA(cudaMemcpyAsync(h, acc, 3 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaMemcpyAsync(h + 3, next, 16, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+            if (!unique || (unsigned)h[4] == 0) break;
+        }
+        if (rc) break;
+        tm.mark(ctx, 4);
+        if (!items.empty()) {
+            out[0] = h[0];
+            out[1] = h[1];
+            out[2] = h[2];
+        }
+        if (stats) {
+            cudaEventSynchronize(tm.ev[4]);
+            stats->histogram_ms = tm.ms(0, 1);
+            stats->build_partition_ms = tm.ms(1, 2);
+            stats->build_ms = 0;
+            stats->probe_partition_ms = tm.ms(2, 3);
+            stats->probe_ms = tm.ms(3, 4);
+        }
+    } while (0);
+    dfree(ctx, ditems);
+    dfree(ctx, R1);
+    dfree(ctx, R2);
+    dfree(ctx, S1);
+    dfree(ctx, S2);
+    dfree(ctx, meta);
+    return rc;
+}
+
+}  // namespace pyg

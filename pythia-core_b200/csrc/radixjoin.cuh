@@ -1,0 +1,22 @@
+// Radix hash join + aggregation with shared-memory tables (radixjoin.cu).
+#pragma once
+#include <stdint.h>
+
+#include "pyg.h"
+
+struct pyg_ctx;
+
+namespace pyg {
+
+// Largest fine partition count (log2): the histogram kernel keeps 2^bits
+// 32-bit counters in shared memory.
+constexpr int RJ_MAX_FINE_BITS = 15;
+
+// Joins 16-byte (int64 key, int64 payload) device relations R and S on the
+// key and returns out = {match count, wrapped sum of R payloads, wrapped sum
+// of S payloads} over the joined pairs.  fine_bits <= 0 picks the partition
+// count from |R|.  Fills the timing fields of stats when it is not null.
+int radix_join16(pyg_ctx* ctx, const void* R, int64_t nR, const void* S, int64_t nS, int fine_bits,
+                 unsigned long long out[3], pyg_join_stats* stats);
+
+}  // namespace pyg

@@ -56,6 +56,40 @@ def test_radix_sentinel_keys_and_duplicates(ctx, torch_cuda):
     assert ctx.hashjoin_agg(Rd, [0], Sd, [0], PROJ, pyg.JOIN_RADIX) == want
 
 
+@pytest.mark.parametrize("bits", [4, 9, 11])
+def test_radix_duplicate_build_keys(ctx, torch_cuda, bits):
+    """Repeated build keys switch the join to its counted slot layout (and
+    smaller build chunks); the result must not change."""
+    rng = np.random.default_rng(bits)
+    n, m = 1 << 18, 1 << 21
+    k = rng.integers(0, 1 << 16, n)  # ~4 copies per key
+    R = struct([k, rng.integers(-(1 << 50), 1 << 50, n)], [I64, I64])
+    S = struct([rng.integers(0, (1 << 16) + 500, m), rng.integers(-(1 << 50), 1 << 50, m)], [I64, I64])
+    want = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ)
+    got, st = ctx.hashjoin_agg(dev_rel(torch_cuda, R, [I64, I64]), [0], dev_rel(torch_cuda, S, [I64, I64]), [0], PROJ,
+                               pyg.JOIN_RADIX, bits, stats=True)
+    assert st.radix_bits == bits and got == want
+
+
+@pytest.mark.parametrize("bits", [2, 10, 15])
+def test_radix_partition_shapes(ctx, torch_cuda, bits):
+    """Build partitions larger than one shared-memory table (bits 2: chunked
+    build side), two partition passes (bits 10, 15), and one hot probe key
+    that spreads over many probe chunks."""
+    rng = np.random.default_rng(100 + bits)
+    n, m = 1 << 16, 1 << 22
+    k = rng.permutation(n).astype(np.int64) - (n // 2)
+    R = struct([k, rng.integers(-(1 << 62), 1 << 62, n)], [I64, I64])
+    fk = k[rng.integers(0, n, m)]
+    fk[: m // 3] = k[7]  # a third of the probe side is one key
+    fk[::97] = n + 5     # misses
+    S = struct([fk, rng.integers(-(1 << 62), 1 << 62, m)], [I64, I64])
+    want = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ)
+    got = ctx.hashjoin_agg(dev_rel(torch_cuda, R, [I64, I64]), [0], dev_rel(torch_cuda, S, [I64, I64]), [0], PROJ,
+                           pyg.JOIN_RADIX, bits)
+    assert got == want
+
+
 def test_empty_sides(ctx, torch_cuda):
     R = struct([np.arange(100, dtype=np.int64)] * 2, [I64, I64])
     E = R[:0]
