@@ -33,6 +33,7 @@
 
 #include "pyg_internal.cuh"
 #include "radixjoin.cuh"
+#include "bulk.cuh"
 
 namespace pyg {
 
@@ -45,6 +46,12 @@ constexpr int RJ_SLOTS_UNIQUE = RJ_TABLE_BYTES / 16;   // {key, payload}
 constexpr int RJ_SLOTS_COUNTED = RJ_TABLE_BYTES / 32;  // {key, payload sum, count, -}
 constexpr int64_t RJ_SCHUNK = 1 << 16;                 // probe tuples per work item (at most)
 constexpr int RJ_MAX_LOCAL_BITS = 9;                   // bins of one partition pass
+constexpr int RJ_LMAX = 1 << RJ_MAX_LOCAL_BITS;
+#ifndef PYG_RJ_WARP_RANK
+#define PYG_RJ_WARP_RANK 0
+#endif
+constexpr int RJ_STAGES = 2;                           // input tiles in flight per partition CTA
+constexpr unsigned long long kBulkWaitNs = 2000000000ULL;  // 2 s
 
 __device__ __forceinline__ unsigned rj_bin(uint64_t h, int shift, unsigned mask)
 {
@@ -96,6 +103,7 @@ struct RJPass {
     int lbits;
     const unsigned long long* bin_start;  // exact output start per output bin
     unsigned long long* cursor;           // per output bin, zeroed before the pass
+    unsigned* err;                        // set if a tile's bulk copy never completed
 };
 
 struct RJTileRange {
@@ -118,107 +126,134 @@ __device__ RJTileRange rj_tile_range(const RJPass& a, long long tile)
     return r;
 }
 
+// Shared memory of one partition CTA: a ring of RJ_STAGES input tiles that
+// bulk copies fill ahead of use, the grouped (staged) tile, and per-bin
+// counters.
+struct RJPartSmem {
+    longlong2 in[RJ_STAGES][RJ_TILE];
+    longlong2 stage[RJ_TILE];
+    unsigned short stage_bin[RJ_TILE];
+    unsigned hist[RJ_LMAX];
+    unsigned loff[RJ_LMAX];
+    unsigned long long gbase[RJ_LMAX];
+    uint64_t bar[RJ_STAGES];
+    RJTileRange info[RJ_STAGES];
+    unsigned warp_tot[RJ_PT_THREADS / 32];
+    int ok;
+};
+
+// Thread 0: starts the bulk copy of tile `tile` into ring slot `slot`.
+__device__ __forceinline__ void rj_issue_tile(const RJPass& a, RJPartSmem& sm, int slot, long long tile)
+{
+    const RJTileRange r = rj_tile_range(a, tile);
+    sm.info[slot] = r;
+    const unsigned bytes = (unsigned)(r.end - r.begin) * 16u;
+    mbar_arrive_expect_tx(&sm.bar[slot], bytes);
+    bulk_load(sm.in[slot], a.in + r.begin, bytes, &sm.bar[slot]);
+}
+
 __global__ void __launch_bounds__(RJ_PT_THREADS, 2) rj_partition_kernel(RJPass a, long long ntiles)
 {
+    extern __shared__ __align__(128) unsigned char rj_pt_raw[];
+    RJPartSmem& sm = *reinterpret_cast<RJPartSmem*>(rj_pt_raw);
     constexpr int PER = RJ_TILE / RJ_PT_THREADS;
-    constexpr int LMAX = 1 << RJ_MAX_LOCAL_BITS;
-    __shared__ __align__(16) longlong2 stage[RJ_TILE];
-    __shared__ unsigned short stage_bin[RJ_TILE];
-    __shared__ unsigned hist[LMAX], loff[LMAX];
-    __shared__ unsigned long long gbase[LMAX];
-    __shared__ unsigned warp_tot[RJ_PT_THREADS / 32];
-    __shared__ unsigned tile_n;
-    __shared__ RJTileRange next_range;
     const int L = 1 << a.lbits;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-
-    // Software pipeline: the next tile's loads are issued before the
-    // current tile is grouped and written out.
-    if (threadIdx.x == 0 && blockIdx.x < ntiles) next_range = rj_tile_range(a, blockIdx.x);
-    __syncthreads();
-    RJTileRange nr = next_range;
-    longlong2 nxt[PER];
-#pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        long long i = nr.begin + j * RJ_PT_THREADS + threadIdx.x;
-        if (blockIdx.x < ntiles && i < nr.end) nxt[j] = __ldcs(&a.in[i]);
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    for (int b = tid; b < RJ_LMAX; b += RJ_PT_THREADS) sm.hist[b] = 0;
+    if (tid == 0) {
+        for (int s = 0; s < RJ_STAGES; ++s) mbar_init(&sm.bar[s], 1);
+        mbar_fence_init();
+        for (int s = 0; s < RJ_STAGES; ++s)
+            if (blockIdx.x + (long long)s * gridDim.x < ntiles) rj_issue_tile(a, sm, s, blockIdx.x + (long long)s * gridDim.x);
+        sm.ok = 1;
     }
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const RJTileRange cur = nr;
-        __syncthreads();  // previous tile finished with shared memory
-        for (int b = threadIdx.x; b < L; b += RJ_PT_THREADS) hist[b] = 0;
-        if (threadIdx.x == 0 && tile + gridDim.x < ntiles) next_range = rj_tile_range(a, tile + gridDim.x);
-        __syncthreads();
+    __syncthreads();
+    const unsigned lt_mask = (1u << lane) - 1u;
+    long long k = 0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k) {
+        const int slot = (int)(k % RJ_STAGES);
+        const unsigned parity = (unsigned)((k / RJ_STAGES) & 1);
+        // Every thread waits for the tile; a wait that runs out marks the
+        // CTA failed and that thread's tuples are left out, so nothing is
+        // written from memory the copy did not fill.
+        const bool landed = mbar_wait(&sm.bar[slot], parity, kBulkWaitNs);
+        if (!landed) sm.ok = 0;
+        const RJTileRange cur = sm.info[slot];
+        const unsigned n = (unsigned)(cur.end - cur.begin);
+        // (1) Bin and rank every tuple; one shared atomic per (warp, bin).
         longlong2 t[PER];
-#pragma unroll
-        for (int j = 0; j < PER; ++j) t[j] = nxt[j];
-        if (tile + gridDim.x < ntiles) {
-            nr = next_range;
-#pragma unroll
-            for (int j = 0; j < PER; ++j) {
-                long long i = nr.begin + j * RJ_PT_THREADS + threadIdx.x;
-                if (i < nr.end) nxt[j] = __ldcs(&a.in[i]);
-            }
-        }
         unsigned bin[PER], rank[PER];
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
-            long long i = cur.begin + j * RJ_PT_THREADS + threadIdx.x;
+            const unsigned i = j * RJ_PT_THREADS + tid;
+            const bool valid = landed && i < n;
             bin[j] = 0xFFFFFFFFu;
-            if (i < cur.end) {
+            if (valid) {
+                t[j] = sm.in[slot][i];
                 bin[j] = rj_bin(mix64((uint64_t)t[j].x), a.shift, a.mask);
-                rank[j] = atomicAdd(&hist[bin[j]], 1u);
             }
+#if PYG_RJ_WARP_RANK
+            const unsigned peers = __match_any_sync(0xffffffffu, bin[j]);
+            const int leader = __ffs(peers) - 1;
+            unsigned base = 0;
+            if (valid && lane == leader) base = atomicAdd(&sm.hist[bin[j]], (unsigned)__popc(peers));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            rank[j] = base + __popc(peers & lt_mask);
+#else
+            if (valid) rank[j] = atomicAdd(&sm.hist[bin[j]], 1u);
+#endif
         }
-        __syncthreads();
-        // Exclusive scan of the tile histogram (each thread owns a run of
-        // consecutive bins), then one global reservation per non-empty bin.
-        const int per = (L + RJ_PT_THREADS - 1) / RJ_PT_THREADS;
-        const int b0 = threadIdx.x * per;
-        unsigned local = 0;
-        for (int b = b0; b < b0 + per && b < L; ++b) local += hist[b];
-        unsigned incl = local;
+        __syncthreads();  // A: histogram complete
+        if (!sm.ok) break;
+        // (2) Exclusive scan over bins (thread b owns bin b), reservation
+        // of each non-empty bin's run, and reset of the counter.
+        unsigned c = tid < L ? sm.hist[tid] : 0u;
+        unsigned incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += v;
         }
-        if (lane == 31) warp_tot[w] = incl;
-        __syncthreads();
-        if (w == 0) {
-            unsigned x = lane < RJ_PT_THREADS / 32 ? warp_tot[lane] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                unsigned v = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += v;
+        if (lane == 31) sm.warp_tot[w] = incl;
+        __syncthreads();  // B
+        unsigned excl = incl - c, total = 0;
+        for (int v = 0; v < RJ_PT_THREADS / 32; ++v) {
+            if (v == w) excl += total;
+            total += sm.warp_tot[v];
+        }
+        if (tid < L) {
+            sm.loff[tid] = excl;
+            if (c) {
+                const unsigned ob = ((unsigned)cur.seg << a.lbits) | (unsigned)tid;
+                sm.gbase[tid] = a.bin_start[ob] + atomicAdd(&a.cursor[ob], (unsigned long long)c);
             }
-            if (lane < RJ_PT_THREADS / 32) warp_tot[lane] = x;
-            if (lane == RJ_PT_THREADS / 32 - 1) tile_n = x;
+            sm.hist[tid] = 0;
         }
-        __syncthreads();
-        unsigned run = incl - local + (w > 0 ? warp_tot[w - 1] : 0);
-        const unsigned obase = (unsigned)cur.seg << a.lbits;
-        for (int b = b0; b < b0 + per && b < L; ++b) {
-            unsigned c = hist[b];
-            loff[b] = run;
-            run += c;
-            if (c) gbase[b] = a.bin_start[obase | b] + atomicAdd(&a.cursor[obase | b], (unsigned long long)c);
-        }
-        __syncthreads();
+        __syncthreads();  // C: offsets ready
+        // (3) Group the tile by bin in shared memory.
 #pragma unroll
         for (int j = 0; j < PER; ++j)
             if (bin[j] != 0xFFFFFFFFu) {
-                const unsigned s = loff[bin[j]] + rank[j];
-                stage[s] = t[j];
-                stage_bin[s] = (unsigned short)bin[j];
+                const unsigned s = sm.loff[bin[j]] + rank[j];
+                sm.stage[s] = t[j];
+                sm.stage_bin[s] = (unsigned short)bin[j];
             }
-        __syncthreads();
-        const unsigned cnt = tile_n;
-        for (unsigned i = threadIdx.x; i < cnt; i += RJ_PT_THREADS) {
-            const unsigned b = stage_bin[i];
-            __stcs(&a.out[gbase[b] + (i - loff[b])], stage[i]);
+        __syncthreads();  // D: ring slot consumed, stage complete
+        if (tid == 0) {
+            const long long nt = tile + (long long)RJ_STAGES * gridDim.x;
+            if (nt < ntiles) {
+                fence_proxy_async_smem();
+                rj_issue_tile(a, sm, slot, nt);
+            }
+        }
+        // (4) Write each bin's run contiguously.
+        for (unsigned i = tid; i < total; i += RJ_PT_THREADS) {
+            const unsigned b = sm.stage_bin[i];
+            __stcs(&a.out[sm.gbase[b] + (i - sm.loff[b])], sm.stage[i]);
         }
     }
+    __syncthreads();
+    if (tid == 0 && !sm.ok) atomicOr(a.err, 1u);
 }
 
 // ---------------------------------------------------------------------------
@@ -414,11 +449,13 @@ void make_items(const std::vector<unsigned long long>& hr, const std::vector<uns
 int launch_pass(pyg_ctx* ctx, const RJPass& p, long long ntiles)
 {
     if (ntiles <= 0) return PYG_OK;
+    const size_t smem = sizeof(RJPartSmem);
+    PYG_CUDA(cudaFuncSetAttribute(rj_partition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rj_partition_kernel, RJ_PT_THREADS, 0));
+    PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rj_partition_kernel, RJ_PT_THREADS, smem));
     if (per_sm < 1) per_sm = 1;
     long long grid = std::min<long long>(ntiles, (long long)ctx->sm_count * per_sm);
-    rj_partition_kernel<<<(unsigned)grid, RJ_PT_THREADS, 0, ctx->stream>>>(p, ntiles);
+    rj_partition_kernel<<<(unsigned)grid, RJ_PT_THREADS, smem, ctx->stream>>>(p, ntiles);
     PYG_LAUNCHED(ctx);
     return PYG_OK;
 }
@@ -480,6 +517,8 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
         unsigned long long* whole = curS2 + F;  // single-segment bounds of the unpartitioned inputs
         unsigned long long* wtiles = whole + 4;
         PYG_CUDA(cudaMemsetAsync(meta, 0, nmeta * 8, ctx->stream));
+        unsigned* perr = (unsigned*)(ctx->dcounters + 202);  // partition passes: a bulk copy never landed
+        PYG_CUDA(cudaMemsetAsync(perr, 0, 8, ctx->stream));
 
         // 1. Histograms.
         const size_t hsm = (size_t)F * 4;
@@ -557,6 +596,7 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
             p.lbits = CB;
             p.bin_start = two ? coarse : fine;
             p.cursor = two ? cur1 : cur2;
+            p.err = perr;
             int r = launch_pass(ctx, p, ntiles);
             if (r || !two) return r;
             p.in = (const longlong2*)o1;
@@ -615,8 +655,13 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
             else rj_join_kernel<false><<<grid, RJ_JOIN_THREADS, RJ_TABLE_BYTES, ctx->stream>>>(ja);
             PYG_LAUNCHED(ctx);
             PYG_CUDA(cudaMemcpyAsync(h, acc, 3 * 8, cudaMemcpyDeviceToHost, ctx->stream));
-            PYG_CUDA(cudaMemcpyAsync(h + 3, next, 16, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaMemcpyAsync(h + 3, next, 24, cudaMemcpyDeviceToHost, ctx->stream));
             PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+            if ((unsigned)h[5]) {
+                set_error("pyg_hashjoin_agg: a partition tile copy did not complete in time");
+                rc = PYG_ERR_TIMEOUT;
+                break;
+            }
             if (!unique || (unsigned)h[4] == 0) break;
         }
         if (rc) break;
