@@ -39,11 +39,30 @@ namespace pyg {
 
 constexpr int RJ_TILE = 2048;        // tuples per partition tile
 constexpr int RJ_PT_THREADS = 512;   // partition CTA
-constexpr int RJ_JOIN_THREADS = 1024;
-constexpr int RJ_PROBE_UNROLL = 8;   // probe tuples in flight per thread
-constexpr int RJ_TABLE_BYTES = 192 * 1024;
+#ifndef PYG_RJ_JOIN_THREADS
+#define PYG_RJ_JOIN_THREADS 1024
+#endif
+#ifndef PYG_RJ_JOIN_BLOCKS
+#define PYG_RJ_JOIN_BLOCKS 1
+#endif
+#ifndef PYG_RJ_TABLE_KB
+#define PYG_RJ_TABLE_KB 192
+#endif
+#ifndef PYG_RJ_RCAP_PCT
+#define PYG_RJ_RCAP_PCT 50
+#endif
+constexpr int RJ_JOIN_THREADS = PYG_RJ_JOIN_THREADS;
+constexpr int RJ_JOIN_BLOCKS = PYG_RJ_JOIN_BLOCKS;  // join CTAs per SM
+#ifndef PYG_RJ_PROBE_UNROLL
+#define PYG_RJ_PROBE_UNROLL 4
+#endif
+constexpr int RJ_PROBE_UNROLL = PYG_RJ_PROBE_UNROLL;  // probe tuples in flight per thread
+constexpr int RJ_TABLE_BYTES = PYG_RJ_TABLE_KB * 1024;
 constexpr int RJ_SLOTS_UNIQUE = RJ_TABLE_BYTES / 16;   // {key, payload}
 constexpr int RJ_SLOTS_COUNTED = RJ_TABLE_BYTES / 32;  // {key, payload sum, count, -}
+// Build tuples per work item: at most this share of the table's slots.
+constexpr unsigned RJ_RCAP_UNIQUE = RJ_SLOTS_UNIQUE * PYG_RJ_RCAP_PCT / 100;
+constexpr unsigned RJ_RCAP_COUNTED = RJ_SLOTS_COUNTED * PYG_RJ_RCAP_PCT / 100;
 constexpr int64_t RJ_SCHUNK = 1 << 16;                 // probe tuples per work item (at most)
 constexpr int RJ_MAX_LOCAL_BITS = 9;                   // bins of one partition pass
 constexpr int RJ_LMAX = 1 << RJ_MAX_LOCAL_BITS;
@@ -168,7 +187,9 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, 2) rj_partition_kernel(RJPass a
         sm.ok = 1;
     }
     __syncthreads();
+#if PYG_RJ_WARP_RANK
     const unsigned lt_mask = (1u << lane) - 1u;
+#endif
     long long k = 0;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k) {
         const int slot = (int)(k % RJ_STAGES);
@@ -275,30 +296,62 @@ struct RJJoinArgs {
     unsigned* dup;              // set when a build key repeats (UNIQUE)
 };
 
+// Slot of a key in a table of TS slots: multiply-high of the 32 hash bits
+// below the fine partition bits (all keys of one partition share the top
+// fine_bits bits).
+__device__ __forceinline__ unsigned rj_slot(uint64_t h, int fb, unsigned TS)
+{
+    return __umulhi((unsigned)(h >> (32 - fb)), TS);
+}
+
+// Warms L2 with [p, p + bytes) (16-byte aligned start; bytes rounded down
+// to a multiple of 16); no registers are held for it.
+__device__ __forceinline__ void rj_prefetch_l2(const void* p, unsigned long long bytes)
+{
+    bytes &= ~15ULL;
+    if (bytes == 0) return;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((unsigned long long)__cvta_generic_to_global(p)),
+                 "r"((unsigned)bytes)
+                 : "memory");
+}
+
 template <bool UNIQUE>
-__global__ void __launch_bounds__(RJ_JOIN_THREADS, 1) rj_join_kernel(RJJoinArgs a)
+__global__ void __launch_bounds__(RJ_JOIN_THREADS, RJ_JOIN_BLOCKS) rj_join_kernel(RJJoinArgs a)
 {
     extern __shared__ __align__(16) unsigned char rj_table[];
-    constexpr int TS = UNIQUE ? RJ_SLOTS_UNIQUE : RJ_SLOTS_COUNTED;
+    constexpr unsigned TS = UNIQUE ? RJ_SLOTS_UNIQUE : RJ_SLOTS_COUNTED;
     constexpr int U = RJ_PROBE_UNROLL;
-    __shared__ long long item_idx;
+    __shared__ long long item_cur, item_next;
     __shared__ unsigned long long side_cnt, side_sum;
     ulonglong2* T2 = reinterpret_cast<ulonglong2*>(rj_table);  // UNIQUE slots
     ulonglong4* T4 = reinterpret_cast<ulonglong4*>(rj_table);  // counted slots
     uint64_t cnt = 0, bsum = 0, psum = 0;
     bool dup = false;
     const int fb = a.fine_bits;
+    // One item of look-ahead: while this CTA works on an item, the next
+    // one is already claimed and its build partition (and the head of its
+    // probe chunk) is being pulled into L2.
+    if (threadIdx.x == 0) item_next = (long long)atomicAdd(a.next, 1u);
     for (;;) {
+        __syncthreads();  // previous item done with the table and item slots
         if (threadIdx.x == 0) {
-            item_idx = (long long)atomicAdd(a.next, 1u);
+            item_cur = item_next;
             side_cnt = side_sum = 0;
+            if (item_cur < a.nitems) {
+                item_next = (long long)atomicAdd(a.next, 1u);
+                if (item_next < a.nitems) {
+                    const RJItem nx = a.items[item_next];
+                    rj_prefetch_l2(a.R + nx.r0, (unsigned long long)nx.rn * 16);
+                    rj_prefetch_l2(a.S + nx.s0, (unsigned long long)min(nx.sn, 4096u) * 16);
+                }
+            }
         }
-        for (int i = threadIdx.x; i < TS; i += RJ_JOIN_THREADS) {
+        for (unsigned i = threadIdx.x; i < TS; i += RJ_JOIN_THREADS) {
             if constexpr (UNIQUE) T2[i] = make_ulonglong2(kEmptyKey, 0);
             else T4[i] = make_ulonglong4(kEmptyKey, 0, 0, 0);
         }
         __syncthreads();
-        const long long it = item_idx;
+        const long long it = item_cur;
         if (it >= a.nitems) break;
         const RJItem item = a.items[it];
         // Build: linear probing with 64-bit shared-memory CAS.  At most
@@ -311,8 +364,8 @@ __global__ void __launch_bounds__(RJ_JOIN_THREADS, 1) rj_join_kernel(RJJoinArgs 
                 atomicAdd(&side_sum, (unsigned long long)t.y);
                 continue;
             }
-            unsigned pos = (unsigned)__umul64hi(mix64(k) << fb, (uint64_t)TS);
-            for (int steps = 0; steps < TS; ++steps) {
+            unsigned pos = rj_slot(mix64(k), fb, TS);
+            for (unsigned steps = 0; steps < TS; ++steps) {
                 unsigned long long* key = UNIQUE ? &T2[pos].x : &T4[pos].x;
                 const unsigned long long prev = atomicCAS(key, kEmptyKey, k);
                 if (prev == kEmptyKey || prev == k) {
@@ -333,51 +386,49 @@ __global__ void __launch_bounds__(RJ_JOIN_THREADS, 1) rj_join_kernel(RJJoinArgs 
         if (UNIQUE && scnt > 1) dup = true;
         // Probe: U independent streaming loads per thread, lookups in
         // shared memory.
+        auto probe = [&](const longlong2 t) {
+            const uint64_t k = (uint64_t)t.x;
+            if (k == kEmptyKey) {
+                cnt += scnt;
+                bsum += ssum;
+                psum += scnt * (uint64_t)t.y;
+                return;
+            }
+            unsigned pos = rj_slot(mix64(k), fb, TS);
+            for (unsigned steps = 0; steps < TS; ++steps) {
+                if constexpr (UNIQUE) {
+                    const ulonglong2 e = T2[pos];
+                    if (e.x == k) {
+                        cnt += 1;
+                        bsum += e.y;
+                        psum += (uint64_t)t.y;
+                        return;
+                    }
+                    if (e.x == kEmptyKey) return;
+                } else {
+                    const ulonglong4 e = T4[pos];
+                    if (e.x == k) {
+                        cnt += e.z;
+                        bsum += e.y;
+                        psum += e.z * (uint64_t)t.y;
+                        return;
+                    }
+                    if (e.x == kEmptyKey) return;
+                }
+                pos = pos + 1 == TS ? 0 : pos + 1;
+            }
+        };
         const longlong2* S = a.S + item.s0;
-        for (unsigned i = threadIdx.x; i < item.sn; i += U * RJ_JOIN_THREADS) {
+        const unsigned sn = item.sn;
+        unsigned i = threadIdx.x;
+        for (; i + (U - 1) * RJ_JOIN_THREADS < sn; i += U * RJ_JOIN_THREADS) {
             longlong2 t[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const unsigned j = i + u * RJ_JOIN_THREADS;
-                if (j < item.sn) t[u] = __ldcs(&S[j]);
-            }
+            for (int u = 0; u < U; ++u) t[u] = __ldcs(&S[i + u * RJ_JOIN_THREADS]);
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const unsigned j = i + u * RJ_JOIN_THREADS;
-                if (j >= item.sn) continue;
-                const uint64_t k = (uint64_t)t[u].x;
-                if (k == kEmptyKey) {
-                    cnt += scnt;
-                    bsum += ssum;
-                    psum += scnt * (uint64_t)t[u].y;
-                    continue;
-                }
-                unsigned pos = (unsigned)__umul64hi(mix64(k) << fb, (uint64_t)TS);
-                for (int steps = 0; steps < TS; ++steps) {
-                    if constexpr (UNIQUE) {
-                        const ulonglong2 e = T2[pos];
-                        if (e.x == k) {
-                            cnt += 1;
-                            bsum += e.y;
-                            psum += (uint64_t)t[u].y;
-                            break;
-                        }
-                        if (e.x == kEmptyKey) break;
-                    } else {
-                        const ulonglong4 e = T4[pos];
-                        if (e.x == k) {
-                            cnt += e.z;
-                            bsum += e.y;
-                            psum += e.z * (uint64_t)t[u].y;
-                            break;
-                        }
-                        if (e.x == kEmptyKey) break;
-                    }
-                    pos = pos + 1 == TS ? 0 : pos + 1;
-                }
-            }
+            for (int u = 0; u < U; ++u) probe(t[u]);
         }
-        __syncthreads();  // table and item slots are reused by the next item
+        for (; i < sn; i += RJ_JOIN_THREADS) probe(__ldcs(&S[i]));
     }
     cnt = warp_sum_u64(cnt);
     bsum = warp_sum_u64(bsum);
@@ -472,7 +523,7 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
         // Fine partitions of about 0.7 x the table's build capacity.
         fine_bits = 1;
         while (fine_bits < RJ_MAX_FINE_BITS &&
-               (double)nR / (double)(1 << fine_bits) > 0.7 * (RJ_SLOTS_UNIQUE / 2))
+               (double)nR / (double)(1 << fine_bits) > 0.7 * RJ_RCAP_UNIQUE)
             ++fine_bits;
     }
     if (fine_bits < 1 || fine_bits > RJ_MAX_FINE_BITS) {
@@ -568,7 +619,7 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
                                           0, (unsigned long long)ntR, 0, (unsigned long long)ntS};
         std::vector<RJItem> items;
         std::vector<unsigned long long> rstart(fR, fR + F), sstart(fS, fS + F);
-        make_items(hr, hs, rstart, sstart, RJ_SLOTS_UNIQUE / 2, items);
+        make_items(hr, hs, rstart, sstart, RJ_RCAP_UNIQUE, items);
         PYG_CUDA(cudaMemcpyAsync(fineR, up.data(), up.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
         PYG_CUDA(cudaMemcpyAsync(whole, wh, sizeof(wh), cudaMemcpyHostToDevice, ctx->stream));
         if (!items.empty()) {
@@ -630,7 +681,7 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
         for (int pass = 0; pass < 2 && !items.empty(); ++pass) {
             const bool unique = pass == 0;
             if (!unique) {
-                make_items(hr, hs, rstart, sstart, RJ_SLOTS_COUNTED / 2, items);
+                make_items(hr, hs, rstart, sstart, RJ_RCAP_COUNTED, items);
                 dfree(ctx, ditems);
                 ditems = nullptr;
                 if ((rc = dalloc(ctx, (void**)&ditems, items.size() * sizeof(RJItem)))) break;
@@ -650,7 +701,7 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
             ja.fine_bits = FB;
             ja.acc = acc;
             ja.dup = dupf;
-            const unsigned grid = (unsigned)std::min<long long>((long long)ctx->sm_count, ja.nitems);
+            const unsigned grid = (unsigned)std::min<long long>((long long)ctx->sm_count * RJ_JOIN_BLOCKS, ja.nitems);
             if (unique) rj_join_kernel<true><<<grid, RJ_JOIN_THREADS, RJ_TABLE_BYTES, ctx->stream>>>(ja);
             else rj_join_kernel<false><<<grid, RJ_JOIN_THREADS, RJ_TABLE_BYTES, ctx->stream>>>(ja);
             PYG_LAUNCHED(ctx);
