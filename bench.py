@@ -309,23 +309,27 @@ def main_gpu(args):
     if radix:
         npass = 2 if two_pass else 1
         phases = {
-            "histogram": (mean("histogram_ms"), (nR + nS) * 16, "rj_hist_kernel"),
-            "build_partition": (mean("build_partition_ms"), nR * 32 * npass, "rj_partition_kernel"),
-            "probe_partition": (mean("probe_partition_ms"), nS * 32 * npass, "rj_partition_kernel"),
-            "join": (mean("probe_ms"), (nR + nS) * 16, "rj_join_kernel"),
+            "histogram": (mean("histogram_ms"), (nR + nS) * 16, "rj_hist_kernel", 2),
+            "build_partition": (mean("build_partition_ms"), nR * 32 * npass, "rj_partition_kernel", npass),
+            "probe_partition": (mean("probe_partition_ms"), nS * 32 * npass, "rj_partition_kernel", npass),
+            "join": (mean("probe_ms"), (nR + nS) * 16, "rj_join_kernel", 1),
         }
     else:
         phases = {
-            "build": (mean("build_ms"), nR * 16, "ht_build16_kernel"),
-            "probe": (mean("probe_ms"), nS * 16, "probe_agg16_kernel"),
+            "build": (mean("build_ms"), nR * 16, "ht_build16_kernel", 1),
+            "probe": (mean("probe_ms"), nS * 16, "probe_agg16_kernel", 1),
         }
-    ph = {k: {"ms": round(v[0], 3), "bytes": v[1], "kernel": v[2],
+    ph = {k: {"ms": round(v[0], 3), "bytes": v[1], "kernel": v[2], "launches": v[3],
               "gbs": round(v[1] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else None,
               "frac": round(v[1] / (v[0] / 1e3) / 1e9 / hbm, 4) if v[0] > 0 else None} for k, v in phases.items()}
     top = max((k for k in ph if ph[k]["ms"] > 0), key=lambda k: ph[k]["ms"])
     kernel_name = ph[top]["kernel"]
     step_bytes = (nR + nS) * 16
+    # achieved = algorithmic bytes per launch / average launch time of the
+    # phase's kernel (equal to the phase's bytes / phase time).
     roofline = {"bound": "hbm", "kernel": kernel_name, "phase": top, "achieved": ph[top]["gbs"], "peak": hbm,
+                "bytes_per_launch": ph[top]["bytes"] // ph[top]["launches"],
+                "ms_per_launch": round(ph[top]["ms"] / ph[top]["launches"], 4),
                 "unit": "GB/s", "frac": ph[top]["frac"], "peak_source": peak_kind, "traffic": None,
                 "phases": ph, "algorithm": int(phase[0].algorithm), "radix_bits": int(phase[0].radix_bits),
                 "passes": (2 if two_pass else 1) if radix else 0,
