@@ -309,7 +309,8 @@ def main_gpu(args):
     if radix:
         npass = 2 if two_pass else 1
         phases = {
-            "histogram": (mean("histogram_ms"), (nR + nS) * 16, "rj_hist_kernel", 2),
+            # The probe side's histogram may be a strided sample.
+            "histogram": (mean("histogram_ms"), int(phase[0].histogram_tuples) * 16, "rj_hist_kernel", 2),
             "build_partition": (mean("build_partition_ms"), nR * 32 * npass, "rj_partition_kernel", npass),
             "probe_partition": (mean("probe_partition_ms"), nS * 32 * npass, "rj_partition_kernel", npass),
             "join": (mean("probe_ms"), (nR + nS) * 16, "rj_join_kernel", 1),

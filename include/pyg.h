@@ -164,7 +164,8 @@ typedef struct pyg_join_stats {
     double probe_ms;            /* probes + fused aggregation           */
     int64_t overflow_tuples;
     int64_t padded_tuples;
-    double histogram_ms;        /* exact partition histograms (RADIX)   */
+    double histogram_ms;        /* partition histograms (RADIX)         */
+    int64_t histogram_tuples;   /* tuples the histograms read (RADIX)   */
 } pyg_join_stats;
 
 int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_keys,

@@ -29,6 +29,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "pyg_internal.cuh"
@@ -81,28 +82,49 @@ __device__ __forceinline__ unsigned rj_bin(uint64_t h, int shift, unsigned mask)
 // 1. Histogram of the top `bits` hash bits (bits <= 15: 128 KB of shared
 // counters per CTA).
 
-__global__ void __launch_bounds__(1024) rj_hist_kernel(const longlong2* __restrict__ in, int64_t n, int bits,
-                                                       unsigned long long* __restrict__ hist)
+__global__ void __launch_bounds__(1024) rj_hist_kernel(const longlong2* __restrict__ in, int64_t n, int64_t step,
+                                                       int bits, unsigned long long* __restrict__ hist)
 {
+    // Counts in[0], in[step], in[2 step], ... (step 1: every tuple).
     extern __shared__ unsigned rj_sh_hist[];
     const int P = 1 << bits;
     const int shift = 64 - bits;
+    const int64_t m = (n + step - 1) / step;
     for (int b = threadIdx.x; b < P; b += blockDim.x) rj_sh_hist[b] = 0;
     __syncthreads();
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     constexpr int U = 8;
-    for (; i + (U - 1) * stride < n; i += U * stride) {
+    for (; i + (U - 1) * stride < m; i += U * stride) {
         longlong2 t[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) t[u] = __ldcs(&in[i + u * stride]);
+        for (int u = 0; u < U; ++u) t[u] = __ldcs(&in[(i + u * stride) * step]);
 #pragma unroll
         for (int u = 0; u < U; ++u) atomicAdd(&rj_sh_hist[rj_bin(mix64((uint64_t)t[u].x), shift, P - 1)], 1u);
     }
-    for (; i < n; i += stride) atomicAdd(&rj_sh_hist[rj_bin(mix64((uint64_t)__ldcs(&in[i]).x), shift, P - 1)], 1u);
+    for (; i < m; i += stride)
+        atomicAdd(&rj_sh_hist[rj_bin(mix64((uint64_t)__ldcs(&in[i * step]).x), shift, P - 1)], 1u);
     __syncthreads();
     for (int b = threadIdx.x; b < P; b += blockDim.x)
         if (rj_sh_hist[b]) atomicAdd(&hist[b], (unsigned long long)rj_sh_hist[b]);
+}
+
+// Tiles per segment, as an exclusive prefix (one thread; at most 2^8
+// segments): tiles[C] is the pass's tile count.  Counts are first clamped
+// to their region's capacity, so a region that overflowed (its result is
+// discarded and redone) is never read past its end.
+__global__ void rj_tile_prefix_kernel(unsigned long long* __restrict__ count, const unsigned long long* __restrict__ cap,
+                                      int C, unsigned long long* __restrict__ tiles)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long t = 0;
+    tiles[0] = 0;
+    for (int c = 0; c < C; ++c) {
+        const unsigned long long n = count[c] < cap[c] ? count[c] : cap[c];
+        count[c] = n;
+        t += (n + RJ_TILE - 1) / RJ_TILE;
+        tiles[c + 1] = t;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -120,9 +142,14 @@ struct RJPass {
     int shift;
     unsigned mask;
     int lbits;
-    const unsigned long long* bin_start;  // exact output start per output bin
+    const unsigned long long* bin_start;  // output region start per output bin
     unsigned long long* cursor;           // per output bin, zeroed before the pass
     unsigned* err;                        // set if a tile's bulk copy never completed
+    // Optional (null when offsets are exact):
+    const unsigned long long* seg_count;  // tuples in each segment (segment end = start + count)
+    const unsigned long long* bin_cap;    // region capacity per output bin
+    unsigned* ovf;                        // set when a bin outgrows its region (the run is not written)
+    const unsigned long long* ntiles_dev; // tile count read on the device
 };
 
 struct RJTileRange {
@@ -141,7 +168,9 @@ __device__ RJTileRange rj_tile_range(const RJPass& a, long long tile)
     RJTileRange r;
     r.seg = lo;
     r.begin = (long long)a.seg_start[lo] + (tile - (long long)a.seg_tile0[lo]) * RJ_TILE;
-    r.end = min(r.begin + RJ_TILE, (long long)a.seg_start[lo + 1]);
+    const long long seg_end =
+        a.seg_count ? (long long)a.seg_start[lo] + (long long)a.seg_count[lo] : (long long)a.seg_start[lo + 1];
+    r.end = min(r.begin + RJ_TILE, seg_end);
     return r;
 }
 
@@ -173,6 +202,7 @@ __device__ __forceinline__ void rj_issue_tile(const RJPass& a, RJPartSmem& sm, i
 
 __global__ void __launch_bounds__(RJ_PT_THREADS, 2) rj_partition_kernel(RJPass a, long long ntiles)
 {
+    if (a.ntiles_dev) ntiles = (long long)*a.ntiles_dev;
     extern __shared__ __align__(128) unsigned char rj_pt_raw[];
     RJPartSmem& sm = *reinterpret_cast<RJPartSmem*>(rj_pt_raw);
     constexpr int PER = RJ_TILE / RJ_PT_THREADS;
@@ -242,15 +272,20 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, 2) rj_partition_kernel(RJPass a
             if (v == w) excl += total;
             total += sm.warp_tot[v];
         }
+        // The reservation's result (a global atomic, about a microsecond
+        // away) is first needed after the tile is staged.
+        unsigned long long resv = 0, bstart = 0, bcap = ~0ULL;
         if (tid < L) {
             sm.loff[tid] = excl;
             if (c) {
                 const unsigned ob = ((unsigned)cur.seg << a.lbits) | (unsigned)tid;
-                sm.gbase[tid] = a.bin_start[ob] + atomicAdd(&a.cursor[ob], (unsigned long long)c);
+                bstart = a.bin_start[ob];
+                if (a.bin_cap) bcap = a.bin_cap[ob];
+                resv = atomicAdd(&a.cursor[ob], (unsigned long long)c);
             }
             sm.hist[tid] = 0;
         }
-        __syncthreads();  // C: offsets ready
+        __syncthreads();  // C: in-tile offsets ready
         // (3) Group the tile by bin in shared memory.
 #pragma unroll
         for (int j = 0; j < PER; ++j)
@@ -259,7 +294,15 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, 2) rj_partition_kernel(RJPass a
                 sm.stage[s] = t[j];
                 sm.stage_bin[s] = (unsigned short)bin[j];
             }
-        __syncthreads();  // D: ring slot consumed, stage complete
+        if (tid < L && c) {
+            unsigned long long gb = bstart + resv;
+            if (resv + c > bcap) {  // outgrew its region: not written; the host redoes the pass exactly
+                atomicOr(a.ovf, 1u);
+                gb = ~0ULL;
+            }
+            sm.gbase[tid] = gb;
+        }
+        __syncthreads();  // D: ring slot consumed, stage and global offsets complete
         if (tid == 0) {
             const long long nt = tile + (long long)RJ_STAGES * gridDim.x;
             if (nt < ntiles) {
@@ -270,7 +313,8 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, 2) rj_partition_kernel(RJPass a
         // (4) Write each bin's run contiguously.
         for (unsigned i = tid; i < total; i += RJ_PT_THREADS) {
             const unsigned b = sm.stage_bin[i];
-            __stcs(&a.out[sm.gbase[b] + (i - sm.loff[b])], sm.stage[i]);
+            const unsigned long long gb = sm.gbase[b];
+            if (gb != ~0ULL) __stcs(&a.out[gb + (i - sm.loff[b])], sm.stage[i]);
         }
     }
     __syncthreads();
@@ -511,6 +555,169 @@ int launch_pass(pyg_ctx* ctx, const RJPass& p, long long ntiles)
     return PYG_OK;
 }
 
+// Host-side layout of one relation's partitions.  Exact layouts come from a
+// full histogram (dense, contiguous partitions); sampled layouts size each
+// partition's region from a strided sample with six standard deviations of
+// slack, and the partition pass reports any region that overflows.
+struct RJLayout {
+    bool sampled = false;
+    std::vector<unsigned long long> fstart;  // F + 1 fine region starts
+    std::vector<unsigned long long> fcap;    // F fine region capacities (sampled)
+    std::vector<unsigned long long> cstart;  // C + 1 coarse region starts
+    std::vector<unsigned long long> ccap;    // C coarse region capacities (sampled)
+    std::vector<unsigned long long> tiles2;  // C + 1 tile prefix of the second pass (exact)
+    std::vector<unsigned long long> count;   // F tuples per fine partition, once known
+    unsigned long long p1 = 0, p2 = 0;       // tuples in the pass-1 / pass-2 buffers
+    unsigned long long tiles2_max = 0;       // upper bound of the second pass's tiles (sampled)
+};
+
+void layout_exact(const std::vector<unsigned long long>& h, int C, int sub, RJLayout& L)
+{
+    const size_t F = h.size();
+    L.sampled = false;
+    L.fstart.assign(F + 1, 0);
+    for (size_t f = 0; f < F; ++f) L.fstart[f + 1] = L.fstart[f] + h[f];
+    L.cstart.assign(C + 1, 0);
+    for (int c = 0; c <= C; ++c) L.cstart[c] = L.fstart[(size_t)c << sub];
+    L.tiles2.assign(C + 1, 0);
+    for (int c = 0; c < C; ++c) L.tiles2[c + 1] = L.tiles2[c] + (L.cstart[c + 1] - L.cstart[c] + RJ_TILE - 1) / RJ_TILE;
+    L.fcap.clear();
+    L.ccap.clear();
+    L.count = h;
+    L.p1 = L.p2 = L.fstart[F];
+    L.tiles2_max = L.tiles2[C];
+}
+
+unsigned long long sampled_cap(unsigned long long c, long long step, unsigned long long extra)
+{
+    const double x = (double)c;
+    return (unsigned long long)std::ceil((x + 6.0 * std::sqrt(x) + 8.0) * (double)step) + extra;
+}
+
+void layout_sampled(const std::vector<unsigned long long>& sc, long long step, int C, int sub, RJLayout& L)
+{
+    const size_t F = sc.size();
+    L.sampled = true;
+    L.fcap.assign(F, 0);
+    L.fstart.assign(F + 1, 0);
+    for (size_t f = 0; f < F; ++f) {
+        L.fcap[f] = sampled_cap(sc[f], step, 64);
+        L.fstart[f + 1] = L.fstart[f] + L.fcap[f];
+    }
+    L.ccap.assign(C, 0);
+    L.cstart.assign(C + 1, 0);
+    L.tiles2_max = 0;
+    for (int c = 0; c < C; ++c) {
+        unsigned long long cc = 0;
+        for (size_t f = (size_t)c << sub; f < (size_t)(c + 1) << sub; ++f) cc += sc[f];
+        L.ccap[c] = sampled_cap(cc, step, 1024);
+        L.cstart[c + 1] = L.cstart[c] + L.ccap[c];
+        L.tiles2_max += (L.ccap[c] + RJ_TILE - 1) / RJ_TILE;
+    }
+    L.tiles2.clear();
+    L.count.clear();
+    L.p1 = L.cstart[C];
+    L.p2 = L.fstart[F];
+}
+
+// Device copy of one relation's partition metadata (u64 words).
+struct RJSideDev {
+    unsigned long long *fstart, *fcap, *cstart, *ccap, *cur1, *cur2, *tiles2, *whole, *wtiles;
+    static size_t words(int F, int C) { return (size_t)(F + 1) + F + (C + 1) + C + C + F + (C + 1) + 4; }
+    void carve(unsigned long long* m, int F, int C)
+    {
+        fstart = m;
+        fcap = fstart + F + 1;
+        cstart = fcap + F;
+        ccap = cstart + C + 1;
+        cur1 = ccap + C;
+        cur2 = cur1 + C;
+        tiles2 = cur2 + F;
+        whole = tiles2 + C + 1;
+        wtiles = whole + 2;
+    }
+};
+
+int upload_layout(pyg_ctx* ctx, const RJLayout& L, const RJSideDev& d, int F, int C, int64_t n)
+{
+    PYG_CUDA(cudaMemcpyAsync(d.fstart, L.fstart.data(), (size_t)(F + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    PYG_CUDA(cudaMemcpyAsync(d.cstart, L.cstart.data(), (size_t)(C + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    if (L.sampled) {
+        PYG_CUDA(cudaMemcpyAsync(d.fcap, L.fcap.data(), (size_t)F * 8, cudaMemcpyHostToDevice, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(d.ccap, L.ccap.data(), (size_t)C * 8, cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+        PYG_CUDA(cudaMemcpyAsync(d.tiles2, L.tiles2.data(), (size_t)(C + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    PYG_CUDA(cudaMemsetAsync(d.cur1, 0, (size_t)(C + F) * 8, ctx->stream));  // cur1 and cur2 are adjacent
+    const unsigned long long w[4] = {0, (unsigned long long)n, 0, (unsigned long long)((n + RJ_TILE - 1) / RJ_TILE)};
+    PYG_CUDA(cudaMemcpyAsync(d.whole, w, sizeof(w), cudaMemcpyHostToDevice, ctx->stream));
+    return PYG_OK;
+}
+
+// Runs the partition pass(es) of one relation into P1 (and P2).
+int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, const RJSideDev& d, bool two, int FB,
+               int CB, void* P1, void* P2, unsigned* err, unsigned* ovf)
+{
+    const int C = 1 << CB, sub = FB - CB;
+    RJPass p;
+    memset(&p, 0, sizeof(p));
+    p.in = in;
+    p.out = (longlong2*)P1;
+    p.seg_start = d.whole;
+    p.seg_tile0 = d.wtiles;
+    p.nseg = 1;
+    p.shift = 64 - CB;
+    p.mask = (unsigned)(C - 1);
+    p.lbits = CB;
+    p.bin_start = two ? d.cstart : d.fstart;
+    p.bin_cap = L.sampled ? (two ? d.ccap : d.fcap) : nullptr;
+    p.cursor = two ? d.cur1 : d.cur2;
+    p.err = err;
+    p.ovf = ovf;
+    int rc = launch_pass(ctx, p, (n + RJ_TILE - 1) / RJ_TILE);
+    if (rc || !two) return rc;
+    long long ntiles2;
+    if (L.sampled) {
+        // Second-pass segments are the first pass's regions, filled to the
+        // counts its cursors reached; the tile prefix is formed on the device.
+        rj_tile_prefix_kernel<<<1, 32, 0, ctx->stream>>>(d.cur1, d.ccap, C, d.tiles2);
+        PYG_LAUNCHED(ctx);
+        p.seg_count = d.cur1;
+        p.ntiles_dev = d.tiles2 + C;
+        ntiles2 = (long long)L.tiles2_max;
+    } else {
+        ntiles2 = (long long)L.tiles2[C];
+    }
+    p.in = (const longlong2*)P1;
+    p.out = (longlong2*)P2;
+    p.seg_start = d.cstart;
+    p.seg_tile0 = d.tiles2;
+    p.nseg = C;
+    p.shift = 64 - FB;
+    p.mask = (unsigned)((1 << sub) - 1);
+    p.lbits = sub;
+    p.bin_start = d.fstart;
+    p.bin_cap = L.sampled ? d.fcap : nullptr;
+    p.cursor = d.cur2;
+    return launch_pass(ctx, p, ntiles2);
+}
+
+int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int FB, unsigned long long* hist)
+{
+    const size_t hsm = (size_t)4 << FB;
+    PYG_CUDA(cudaFuncSetAttribute(rj_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
+    int per = 0;
+    PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rj_hist_kernel, 1024, hsm));
+    if (per < 1) per = 1;
+    const int64_t m = (n + step - 1) / step;
+    const int64_t want = (m + 1024 * 8 - 1) / (1024 * 8);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->sm_count * per));
+    PYG_CUDA(cudaMemsetAsync(hist, 0, (size_t)8 << FB, ctx->stream));
+    rj_hist_kernel<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, FB, hist);
+    PYG_LAUNCHED(ctx);
+    return PYG_OK;
+}
+
 }  // namespace
 
 int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t nS, int fine_bits,
@@ -522,8 +729,7 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
     if (fine_bits <= 0) {
         // Fine partitions of about 0.7 x the table's build capacity.
         fine_bits = 1;
-        while (fine_bits < RJ_MAX_FINE_BITS &&
-               (double)nR / (double)(1 << fine_bits) > 0.7 * RJ_RCAP_UNIQUE)
+        while (fine_bits < RJ_MAX_FINE_BITS && (double)nR / (double)(1 << fine_bits) > 0.7 * RJ_RCAP_UNIQUE)
             ++fine_bits;
     }
     if (fine_bits < 1 || fine_bits > RJ_MAX_FINE_BITS) {
@@ -533,141 +739,86 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
     const int FB = fine_bits;
     const bool two = FB > RJ_MAX_LOCAL_BITS;
     const int CB = two ? (FB + 1) / 2 : FB;
-    const int F = 1 << FB, C = 1 << CB;
+    const int F = 1 << FB, C = 1 << CB, sub = FB - CB;
     if (stats) {
         stats->algorithm = PYG_JOIN_RADIX;
         stats->radix_bits = FB;
     }
     if (nR == 0 || nS == 0) return PYG_OK;
+    // The probe side of a two-pass join is laid out from a sample of about
+    // 2^24 tuples instead of a full histogram read.
+    const bool sample_s = two && nS >= ((int64_t)1 << 25);
+    const int64_t sstep = sample_s ? std::max<int64_t>(1, nS >> 24) : 1;
 
     RJEvents tm;
     tm.start(ctx, stats != nullptr);
-    // Device metadata (u64 words):
-    //   histR[F] histS[F] | fineR[F+1] fineS[F+1] | coarseR[C+1] coarseS[C+1]
-    //   | tilesR[C+1] tilesS[C+1] | curR1[C] curS1[C] curR2[F] curS2[F]
-    //   | whole[4] = {0, nR, 0, nS} | wtiles[4] = {0, tiles(R), 0, tiles(S)}
-    const size_t nmeta = 2 * (size_t)F + 2 * (size_t)(F + 1) + 4 * (size_t)(C + 1) + 2 * (size_t)C + 2 * (size_t)F + 8;
+    const size_t side_words = RJSideDev::words(F, C);
     unsigned long long* meta = nullptr;
     void *R1 = nullptr, *R2 = nullptr, *S1 = nullptr, *S2 = nullptr;
     RJItem* ditems = nullptr;
     int rc = PYG_OK;
     do {
-        if ((rc = dalloc(ctx, (void**)&meta, nmeta * 8))) break;
-        unsigned long long* histR = meta;
+        if ((rc = dalloc(ctx, (void**)&meta, (2 * side_words + 2 * (size_t)F) * 8))) break;
+        RJSideDev dR, dS;
+        dR.carve(meta, F, C);
+        dS.carve(meta + side_words, F, C);
+        unsigned long long* histR = meta + 2 * side_words;
         unsigned long long* histS = histR + F;
-        unsigned long long* fineR = histS + F;
-        unsigned long long* fineS = fineR + F + 1;
-        unsigned long long* coarseR = fineS + F + 1;
-        unsigned long long* coarseS = coarseR + C + 1;
-        unsigned long long* tilesR = coarseS + C + 1;
-        unsigned long long* tilesS = tilesR + C + 1;
-        unsigned long long* curR1 = tilesS + C + 1;
-        unsigned long long* curS1 = curR1 + C;
-        unsigned long long* curR2 = curS1 + C;
-        unsigned long long* curS2 = curR2 + F;
-        unsigned long long* whole = curS2 + F;  // single-segment bounds of the unpartitioned inputs
-        unsigned long long* wtiles = whole + 4;
-        PYG_CUDA(cudaMemsetAsync(meta, 0, nmeta * 8, ctx->stream));
-        unsigned* perr = (unsigned*)(ctx->dcounters + 202);  // partition passes: a bulk copy never landed
-        PYG_CUDA(cudaMemsetAsync(perr, 0, 8, ctx->stream));
+        unsigned* flags = (unsigned*)(ctx->dcounters + 202);  // [0] a bulk copy never landed, [1] region overflow
+        PYG_CUDA(cudaMemsetAsync(flags, 0, 8, ctx->stream));
+        unsigned long long* h = (unsigned long long*)ctx->pinned;
 
-        // 1. Histograms.
-        const size_t hsm = (size_t)F * 4;
-        PYG_CUDA(cudaFuncSetAttribute(rj_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
-        int hper = 0;
-        PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&hper, rj_hist_kernel, 1024, hsm));
-        if (hper < 1) hper = 1;
-        rj_hist_kernel<<<ctx->sm_count * hper, 1024, hsm, ctx->stream>>>(R, nR, FB, histR);
-        PYG_LAUNCHED(ctx);
-        rj_hist_kernel<<<ctx->sm_count * hper, 1024, hsm, ctx->stream>>>(S, nS, FB, histS);
-        PYG_LAUNCHED(ctx);
+        // 1. Histograms: exact for the build side, sampled or exact for the
+        // probe side.
+        if ((rc = hist_launch(ctx, R, nR, 1, FB, histR))) break;
+        if ((rc = hist_launch(ctx, S, nS, sstep, FB, histS))) break;
         std::vector<unsigned long long> hr(F), hs(F);
         PYG_CUDA(cudaMemcpyAsync(hr.data(), histR, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
         PYG_CUDA(cudaMemcpyAsync(hs.data(), histS, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
         PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-
-        // Host: exact offsets, tile prefixes, work items.
-        const int sub = FB - CB;
-        std::vector<unsigned long long> up((size_t)2 * (F + 1) + 4 * (size_t)(C + 1));
-        unsigned long long* fR = up.data();
-        unsigned long long* fS = fR + F + 1;
-        unsigned long long* cR = fS + F + 1;
-        unsigned long long* cS = cR + C + 1;
-        unsigned long long* tR = cS + C + 1;
-        unsigned long long* tS = tR + C + 1;
-        fR[0] = fS[0] = 0;
-        for (int f = 0; f < F; ++f) {
-            fR[f + 1] = fR[f] + hr[f];
-            fS[f + 1] = fS[f] + hs[f];
-        }
-        if (fR[F] != (unsigned long long)nR || fS[F] != (unsigned long long)nS) {
+        RJLayout LR, LS;
+        layout_exact(hr, C, sub, LR);
+        if (sample_s) layout_sampled(hs, sstep, C, sub, LS);
+        else layout_exact(hs, C, sub, LS);
+        if (LR.fstart[F] != (unsigned long long)nR || (!sample_s && LS.fstart[F] != (unsigned long long)nS)) {
             set_error("pyg_hashjoin_agg: partition histogram does not add up");
             rc = PYG_ERR_CUDA;
             break;
         }
-        tR[0] = tS[0] = 0;
-        for (int c = 0; c <= C; ++c) {
-            cR[c] = fR[(size_t)c << sub];
-            cS[c] = fS[(size_t)c << sub];
-        }
-        for (int c = 0; c < C; ++c) {
-            tR[c + 1] = tR[c] + (cR[c + 1] - cR[c] + RJ_TILE - 1) / RJ_TILE;
-            tS[c + 1] = tS[c] + (cS[c + 1] - cS[c] + RJ_TILE - 1) / RJ_TILE;
-        }
-        const long long ntR = (nR + RJ_TILE - 1) / RJ_TILE, ntS = (nS + RJ_TILE - 1) / RJ_TILE;
-        const unsigned long long wh[8] = {0, (unsigned long long)nR, 0, (unsigned long long)nS,
-                                          0, (unsigned long long)ntR, 0, (unsigned long long)ntS};
-        std::vector<RJItem> items;
-        std::vector<unsigned long long> rstart(fR, fR + F), sstart(fS, fS + F);
-        make_items(hr, hs, rstart, sstart, RJ_RCAP_UNIQUE, items);
-        PYG_CUDA(cudaMemcpyAsync(fineR, up.data(), up.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
-        PYG_CUDA(cudaMemcpyAsync(whole, wh, sizeof(wh), cudaMemcpyHostToDevice, ctx->stream));
-        if (!items.empty()) {
-            if ((rc = dalloc(ctx, (void**)&ditems, items.size() * sizeof(RJItem)))) break;
-            PYG_CUDA(cudaMemcpyAsync(ditems, items.data(), items.size() * sizeof(RJItem), cudaMemcpyHostToDevice,
-                                     ctx->stream));
-        }
+        if ((rc = upload_layout(ctx, LR, dR, F, C, nR)) || (rc = upload_layout(ctx, LS, dS, F, C, nS))) break;
         tm.mark(ctx, 1);
 
         // 2. Partition passes.
-        if ((rc = dalloc(ctx, &R1, (size_t)nR * 16)) || (rc = dalloc(ctx, &S1, (size_t)nS * 16))) break;
-        if (two && ((rc = dalloc(ctx, &R2, (size_t)nR * 16)) || (rc = dalloc(ctx, &S2, (size_t)nS * 16)))) break;
-        auto run_side = [&](const longlong2* in, const unsigned long long* seg, const unsigned long long* segt,
-                            long long ntiles, unsigned long long* coarse, unsigned long long* cur1,
-                            unsigned long long* fine, unsigned long long* cur2, unsigned long long* tiles, void* o1,
-                            void* o2, long long ntiles2) -> int {
-            RJPass p;
-            p.in = in;
-            p.out = (longlong2*)o1;
-            p.seg_start = seg;
-            p.seg_tile0 = segt;
-            p.nseg = 1;
-            p.shift = 64 - CB;
-            p.mask = (unsigned)(C - 1);
-            p.lbits = CB;
-            p.bin_start = two ? coarse : fine;
-            p.cursor = two ? cur1 : cur2;
-            p.err = perr;
-            int r = launch_pass(ctx, p, ntiles);
-            if (r || !two) return r;
-            p.in = (const longlong2*)o1;
-            p.out = (longlong2*)o2;
-            p.seg_start = coarse;
-            p.seg_tile0 = tiles;
-            p.nseg = C;
-            p.shift = 64 - FB;
-            p.mask = (unsigned)((1 << sub) - 1);
-            p.lbits = sub;
-            p.bin_start = fine;
-            p.cursor = cur2;
-            return launch_pass(ctx, p, ntiles2);
-        };
-        if ((rc = run_side(R, whole, wtiles, ntR, coarseR, curR1, fineR, curR2, tilesR, R1, R2, (long long)tR[C])))
-            break;
+        if ((rc = dalloc(ctx, &R1, (size_t)LR.p1 * 16))) break;
+        if (two && (rc = dalloc(ctx, &R2, (size_t)LR.p2 * 16))) break;
+        if ((rc = run_passes(ctx, R, nR, LR, dR, two, FB, CB, R1, R2, flags, flags + 1))) break;
         tm.mark(ctx, 2);
-        if ((rc = run_side(S, whole + 2, wtiles + 2, ntS, coarseS, curS1, fineS, curS2, tilesS, S1, S2,
-                           (long long)tS[C])))
-            break;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            dfree(ctx, S1);
+            dfree(ctx, S2);
+            S1 = S2 = nullptr;
+            if ((rc = dalloc(ctx, &S1, (size_t)LS.p1 * 16))) break;
+            if (two && (rc = dalloc(ctx, &S2, (size_t)LS.p2 * 16))) break;
+            if ((rc = run_passes(ctx, S, nS, LS, dS, two, FB, CB, S1, S2, flags, flags + 1))) break;
+            if (!LS.sampled) break;
+            // Exact per-partition counts of the sampled layout (and whether
+            // any region overflowed).
+            LS.count.resize(F);
+            PYG_CUDA(cudaMemcpyAsync(LS.count.data(), dS.cur2, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaMemcpyAsync(h + 6, flags, 8, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+            if (((unsigned*)(h + 6))[1] == 0) break;
+            // A region overflowed (the sample misjudged a partition): redo the
+            // probe side from an exact histogram.
+            if ((rc = hist_launch(ctx, S, nS, 1, FB, histS))) break;
+            PYG_CUDA(cudaMemcpyAsync(hs.data(), histS, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+            layout_exact(hs, C, sub, LS);
+            if ((rc = upload_layout(ctx, LS, dS, F, C, nS))) break;
+            PYG_CUDA(cudaMemsetAsync(flags + 1, 0, 4, ctx->stream));
+        }
+        if (rc) break;
+        if (stats) stats->overflow_tuples = LS.sampled ? 0 : (sample_s ? 1 : 0);
         tm.mark(ctx, 3);
 
         // 3. Join: distinct build keys first (16-byte slots); on a repeated
@@ -677,17 +828,18 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
         unsigned long long* acc = ctx->dcounters + 8;
         unsigned* next = (unsigned*)(ctx->dcounters + 200);  // word 200: queue head, word 201: dup flag
         unsigned* dupf = (unsigned*)(ctx->dcounters + 201);
-        unsigned long long* h = (unsigned long long*)ctx->pinned;
-        for (int pass = 0; pass < 2 && !items.empty(); ++pass) {
+        std::vector<unsigned long long> rstart(LR.fstart.begin(), LR.fstart.end() - 1);
+        std::vector<unsigned long long> sstart(LS.fstart.begin(), LS.fstart.end() - 1);
+        std::vector<RJItem> items;
+        for (int pass = 0; pass < 2; ++pass) {
             const bool unique = pass == 0;
-            if (!unique) {
-                make_items(hr, hs, rstart, sstart, RJ_RCAP_COUNTED, items);
-                dfree(ctx, ditems);
-                ditems = nullptr;
-                if ((rc = dalloc(ctx, (void**)&ditems, items.size() * sizeof(RJItem)))) break;
-                PYG_CUDA(cudaMemcpyAsync(ditems, items.data(), items.size() * sizeof(RJItem), cudaMemcpyHostToDevice,
-                                         ctx->stream));
-            }
+            make_items(LR.count, LS.count, rstart, sstart, unique ? RJ_RCAP_UNIQUE : RJ_RCAP_COUNTED, items);
+            if (items.empty()) break;
+            dfree(ctx, ditems);
+            ditems = nullptr;
+            if ((rc = dalloc(ctx, (void**)&ditems, items.size() * sizeof(RJItem)))) break;
+            PYG_CUDA(cudaMemcpyAsync(ditems, items.data(), items.size() * sizeof(RJItem), cudaMemcpyHostToDevice,
+                                     ctx->stream));
             void* fn = unique ? (void*)rj_join_kernel<true> : (void*)rj_join_kernel<false>;
             PYG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, RJ_TABLE_BYTES));
             PYG_CUDA(cudaMemsetAsync(acc, 0, 3 * 8, ctx->stream));
@@ -706,22 +858,26 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
             else rj_join_kernel<false><<<grid, RJ_JOIN_THREADS, RJ_TABLE_BYTES, ctx->stream>>>(ja);
             PYG_LAUNCHED(ctx);
             PYG_CUDA(cudaMemcpyAsync(h, acc, 3 * 8, cudaMemcpyDeviceToHost, ctx->stream));
-            PYG_CUDA(cudaMemcpyAsync(h + 3, next, 24, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaMemcpyAsync(h + 3, next, 16, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaMemcpyAsync(h + 6, flags, 8, cudaMemcpyDeviceToHost, ctx->stream));
             PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-            if ((unsigned)h[5]) {
+            if (((unsigned*)(h + 6))[0]) {
                 set_error("pyg_hashjoin_agg: a partition tile copy did not complete in time");
                 rc = PYG_ERR_TIMEOUT;
                 break;
             }
+            if (((unsigned*)(h + 6))[1]) {
+                set_error("pyg_hashjoin_agg: a partition outgrew its exact region");
+                rc = PYG_ERR_CUDA;
+                break;
+            }
+            out[0] = h[0];
+            out[1] = h[1];
+            out[2] = h[2];
             if (!unique || (unsigned)h[4] == 0) break;
         }
         if (rc) break;
         tm.mark(ctx, 4);
-        if (!items.empty()) {
-            out[0] = h[0];
-            out[1] = h[1];
-            out[2] = h[2];
-        }
         if (stats) {
             cudaEventSynchronize(tm.ev[4]);
             stats->histogram_ms = tm.ms(0, 1);
@@ -729,6 +885,8 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
             stats->build_ms = 0;
             stats->probe_partition_ms = tm.ms(2, 3);
             stats->probe_ms = tm.ms(3, 4);
+            stats->padded_tuples = (int64_t)(LS.p2 - (unsigned long long)nS);
+            stats->histogram_tuples = nR + (nS + sstep - 1) / sstep;
         }
     } while (0);
     dfree(ctx, ditems);

@@ -76,7 +76,7 @@ class pyg_join_opts(C.Structure):
 class pyg_join_stats(C.Structure):
     _fields_ = [("algorithm", C.c_int32), ("radix_bits", C.c_int32), ("build_partition_ms", C.c_double),
                 ("build_ms", C.c_double), ("probe_partition_ms", C.c_double), ("probe_ms", C.c_double), ("overflow_tuples", C.c_int64),
-                ("padded_tuples", C.c_int64), ("histogram_ms", C.c_double)]
+                ("padded_tuples", C.c_int64), ("histogram_ms", C.c_double), ("histogram_tuples", C.c_int64)]
 
 
 class pyg_splitter(C.Structure):

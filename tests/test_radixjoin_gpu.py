@@ -90,6 +90,38 @@ def test_radix_partition_shapes(ctx, torch_cuda, bits):
     assert got == want
 
 
+def test_radix_sampled_probe_layout(ctx, torch_cuda):
+    """A probe side of at least 2^25 tuples with two partition passes is laid
+    out from a sample; the per-partition counts the passes reach are exact."""
+    rng = np.random.default_rng(21)
+    n, m = 1 << 17, (1 << 25) + 12345
+    k = rng.permutation(n).astype(np.int64) * 3 + 1
+    R = struct([k, rng.integers(-(1 << 62), 1 << 62, n)], [I64, I64])
+    S = struct([zipf_keys(rng, m, k, 0.9), rng.integers(-(1 << 62), 1 << 62, m)], [I64, I64])
+    want = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ)
+    got, st = ctx.hashjoin_agg(dev_rel(torch_cuda, R, [I64, I64]), [0], dev_rel(torch_cuda, S, [I64, I64]), [0], PROJ,
+                               pyg.JOIN_RADIX, 11, stats=True)
+    assert got == want and st.overflow_tuples == 0 and st.padded_tuples > 0
+
+
+def test_radix_sample_misjudged_redoes_exactly(ctx, torch_cuda):
+    """Every sampled probe tuple (every second one) carries the same key, so
+    the sample sizes all other partitions' regions near zero; the passes
+    report the overflow and the probe side is redone from an exact
+    histogram."""
+    rng = np.random.default_rng(22)
+    n, m = 1 << 16, 1 << 25
+    k = rng.permutation(n).astype(np.int64) + 1000
+    R = struct([k, rng.integers(0, 1 << 40, n)], [I64, I64])
+    fk = k[rng.integers(0, n, m)]
+    fk[0::2] = k[5]
+    S = struct([fk, rng.integers(0, 1 << 40, m)], [I64, I64])
+    want = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ)
+    got, st = ctx.hashjoin_agg(dev_rel(torch_cuda, R, [I64, I64]), [0], dev_rel(torch_cuda, S, [I64, I64]), [0], PROJ,
+                               pyg.JOIN_RADIX, 10, stats=True)
+    assert got == want and st.overflow_tuples == 1
+
+
 def test_empty_sides(ctx, torch_cuda):
     R = struct([np.arange(100, dtype=np.int64)] * 2, [I64, I64])
     E = R[:0]
