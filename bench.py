@@ -53,6 +53,14 @@ def parse():
     ap.add_argument("--scale-shift", type=int, default=0, help="shrink both relations by 2^s (debug only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="join", choices=["join", "join-small", "groupby", "mpsm", "batch"],
+                    help="join: the headline configuration (default); the others measure the small join, "
+                         "group-by, MPSM sort-merge join and batched-fragment configurations")
+    ap.add_argument("--groups", type=int, default=1 << 16, help="groupby: group cardinality G")
+    ap.add_argument("--zipf", action="store_true", help="groupby: Zipf(1.0) group ids instead of uniform")
+    ap.add_argument("--splitter", default="learned", choices=["learned", "sampled", "exactrange"],
+                    help="mpsm: range splitter")
+    ap.add_argument("--fanout", type=int, default=4096, help="mpsm: range partitions")
     return ap.parse_args()
 
 
@@ -420,10 +428,225 @@ def run_e2e(args, torch, pyg, ctx, R, S, nR, nS, world, dist):
         hS.free()
 
 
+# ------------------------------------------------- the other configurations
+
+def _device_timed(torch, stream, fn, steps, warmup, dist):
+    """W untimed calls, then K calls between CUDA events on `stream`; the
+    job's milliseconds are the max over ranks."""
+    for _ in range(warmup):
+        fn()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    out = [fn() for _ in range(steps)]
+    t1.record(stream)
+    torch.cuda.synchronize()
+    return max_over_ranks(t0.elapsed_time(t1), dist, "cuda"), out
+
+
+def _reference_rows(rels, plan_fn, steps):
+    """Times the reference engine on host arrays {name: (array, types)} with
+    all host cores; plan_fn(T, files) builds the plan text."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refrun
+    if not refrun.available():
+        return None
+    T = min(os.cpu_count() or 1, 127)
+    times = []
+    with tempfile.TemporaryDirectory(dir=os.environ.get("PYG_TMP")) as d:
+        files = {}
+        for name, (arr, types) in rels.items():
+            files[name] = refrun.write_rel(d, name, arr, T)
+        plan = plan_fn(T, files)
+        for _ in range(steps):
+            _, rt, _ = refrun.run(d, plan, timeout=900)
+            times.append(rt)
+    return T, times
+
+
+def main_workload(args):
+    import torch
+    import pyg
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    torch.cuda.set_stream(torch.cuda.Stream(local))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    ctx = pyg.Ctx(local)
+    stream = torch.cuda.current_stream(local)
+    hbm, peak_kind = peaks()
+    sh = args.scale_shift
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1234 + rank)
+    I64 = pyg.INT64
+    cpu = None
+    extra = {}
+
+    if args.workload == "join-small":
+        # R: permutation of 1..2^20, payload = 7 key; S: 2^24 fk ~ U over R's keys, val ~ U{0..999}.
+        nR, nS = (1 << 20) >> sh, (1 << 24) >> sh
+        R = torch.empty(nR * 2, dtype=torch.int64, device="cuda")
+        S = torch.empty(nS * 2, dtype=torch.int64, device="cuda")
+        ctx.gen_pk(R, nR, 7, SEED_KEYS)
+        ctx.gen_fk(S, nS, nR, 0.0, SEED_KEYS, 1000, SEED_PROBE + rank)
+        Rr, Sr = pyg.Rel(R, nR, [I64, I64]), pyg.Rel(S, nS, [I64, I64])
+        fn = lambda: ctx.hashjoin_agg(Rr, [0], Sr, [0], [(1, 1)])  # noqa: E731
+        cnt, sums = fn()
+        Sv = S.view(nS, 2)
+        assert cnt == nS and sums[0] & 0xFFFFFFFFFFFFFFFF == int(Sv[:, 1].sum().item()) & 0xFFFFFFFFFFFFFFFF
+        units, abytes = nR + nS, (nR + nS) * 16 + 16
+        metric = "join+sum tuples/sec (R 2^20 PK, S 2^24 FK, projection P$1)"
+        workload = {"workload": "hash join + sum of P$1", "build_tuples": nR, "probe_tuples": nS}
+        if rank == 0 and world == 1 and not args.no_cpu:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import refrun
+            dt = np.dtype([("c0", np.int64), ("c1", np.int64)])
+            Rh, Sh = R.view(nR, 2).cpu().numpy(), S.view(nS, 2).cpu().numpy()
+            r = _reference_rows({"R": (Rh.view(dt).reshape(-1), 2), "S": (Sh.view(dt).reshape(-1), 2)},
+                                lambda T, f: refrun.plan_join_sum(T, f["R"], [2, 2], f["S"], [2, 2], [(1, 1)], 0, nR), 3)
+            if r:
+                cpu = {"value": units * len(r[1]) / sum(r[1]), "unit": UNIT, "cores": r[0], "kind": "reference",
+                       "sample": f"the whole workload, executequery ResponseTimeInSec, {r[0]} threads"}
+    elif args.workload == "groupby":
+        # N = 2^28 (int64 group id, int64 value); ids ~ U[0, G) or Zipf(1.0); sum and count per group, sorted.
+        N, G = (1 << 28) >> sh, args.groups
+        if args.zipf:
+            w = torch.arange(1, G + 1, dtype=torch.float64, device="cuda").pow(-1.0)
+            ids = torch.multinomial(w / w.sum(), N, replacement=True, generator=g) if N <= (1 << 24) else \
+                torch.cat([torch.multinomial(w / w.sum(), 1 << 24, replacement=True, generator=g)
+                           for _ in range(N >> 24)])
+        else:
+            ids = torch.randint(0, G, (N,), device="cuda", generator=g)
+        vals = torch.randint(0, 1 << 20, (N,), device="cuda", generator=g)
+        A = torch.stack([ids, vals], 1).contiguous().view(-1)
+        del ids, vals
+        rel = pyg.Rel(A, N, [I64, I64])
+        out = torch.empty(G * 3, dtype=torch.int64, device="cuda")
+
+        def fn():
+            rc, ng = ctx.groupby(rel, [0], pyg.AGG_SUM | pyg.AGG_COUNT, 1, True, G, out, G)
+            assert rc == pyg.PYG_OK
+            return ng
+
+        ng = fn()
+        o = out[: ng * 3].view(ng, 3)
+        Av = A.view(N, 2)
+        assert int(o[:, 2].sum().item()) == N and int(o[:, 1].sum().item()) == int(Av[:, 1].sum().item())
+        assert bool((o[1:, 0] > o[:-1, 0]).all().item())
+        units, abytes = N, N * 16 + ng * 24
+        metric = "group-by tuples/sec (N 2^28, sum + count per group, sorted by key)"
+        workload = {"workload": "group-by sum+count", "tuples": N, "groups": G, "groups_found": ng,
+                    "ids": "zipf1.0" if args.zipf else "uniform"}
+        if rank == 0 and world == 1 and not args.no_cpu:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import refrun
+            dt = np.dtype([("c0", np.int64), ("c1", np.int64)])
+            n_cpu = N >> CPU_SAMPLE_SHIFT
+            Ah = Av[:n_cpu].cpu().numpy()
+            r = _reference_rows({"A": (Ah.view(dt).reshape(-1), 2)},
+                                lambda T, f: refrun.plan_groupby(T, f["A"], [2, 2], [0], "sum", 1, G), 3)
+            if r:
+                cpu = {"value": n_cpu * len(r[1]) / sum(r[1]), "unit": UNIT, "cores": r[0], "kind": "reference",
+                       "sample": f"first 1/{1 << CPU_SAMPLE_SHIFT} of the tuples (aggregate_sum, merge, "
+                                 f"re-aggregate), ResponseTimeInSec, {r[0]} threads"}
+    elif args.workload == "mpsm":
+        # R 2^26 PK, S 2^28 FK ~ Zipf(theta); range partition (learned CDF splitter) -> sort -> merge join.
+        nR, nS = (1 << 26) >> sh, (1 << 28) >> sh
+        R = torch.empty(nR * 2, dtype=torch.int64, device="cuda")
+        S = torch.empty(nS * 2, dtype=torch.int64, device="cuda")
+        ctx.gen_pk(R, nR, 7, SEED_KEYS)
+        ctx.gen_fk(S, nS, nR, args.theta, SEED_KEYS, VMAX, SEED_PROBE + rank)
+        Rr, Sr = pyg.Rel(R, nR, [I64, I64]), pyg.Rel(S, nS, [I64, I64])
+        kind = {"learned": pyg.MPSM_LEARNED, "sampled": pyg.MPSM_SAMPLED, "exactrange": pyg.MPSM_EXACTRANGE}[
+            args.splitter]
+        opts = ctx.mpsm_opts(kind, args.fanout, 0.01, 1024)
+        fn = lambda: ctx.mpsm_join_agg(Rr, 0, Sr, 0, [(0, 1), (1, 1)], opts)  # noqa: E731
+        cnt, sums, st = fn()
+        Sv = S.view(nS, 2)
+        expect = int((Sv[:, 0] * 7 + Sv[:, 1]).sum().item()) & 0xFFFFFFFFFFFFFFFF
+        assert cnt == nS and (sums[0] + sums[1]) & 0xFFFFFFFFFFFFFFFF == expect
+        units, abytes = nR + nS, (nR + nS) * 16
+        metric = "MPSM join+agg tuples/sec (R 2^26 PK, S 2^28 FK, range partition + sort + merge)"
+        workload = {"workload": "MPSM sort-merge join + count + checksum", "build_tuples": nR, "probe_tuples": nS,
+                    "theta": args.theta, "splitter": args.splitter, "fanout": args.fanout}
+        extra["mpsm"] = {"max_partition_imbalance": round(st.max_partition_imbalance, 3),
+                         "splitter_ms": round(st.splitter_ms, 3), "partition_ms": round(st.partition_ms, 3),
+                         "sort_ms": round(st.sort_ms, 3), "merge_ms": round(st.merge_ms, 3)}
+    else:  # batch
+        # 256 fragments: build n_i = 2^U(12, 22), probe n_i x U{4..32}; keys uniform or Zipf(1.0); PK-FK + sum.
+        rng = np.random.default_rng(99 + rank)
+        pairs, keep, units = [], [], 0
+        for i in range(256):
+            nb = max(1, int(2 ** rng.uniform(12, 22)) >> sh)
+            npr = nb * int(rng.integers(4, 33))
+            Rb = torch.empty(nb * 2, dtype=torch.int64, device="cuda")
+            Sb = torch.empty(npr * 2, dtype=torch.int64, device="cuda")
+            ctx.gen_pk(Rb, nb, 7, 1000 + i)
+            ctx.gen_fk(Sb, npr, nb, 1.0 if i % 2 else 0.0, 1000 + i, VMAX, 5000 + i)
+            pairs.append((Rb, nb, Sb, npr))
+            keep += [Rb, Sb]
+            units += nb + npr
+        frags = ctx.fragments(pairs)
+        tuning = ctx.autotune(frags)
+        b = ctx.batch_create(frags, tuning)
+
+        def fn():
+            rc, c, sm, lat = ctx.batch_run(b, len(pairs))
+            assert rc == pyg.PYG_OK
+            return c, lat
+
+        c, _ = fn()
+        assert all(int(c[i]) == pairs[i][3] for i in range(len(pairs)))
+        abytes = units * 16
+        metric = "batched fragments tuples/sec (256 PK-FK join+sum fragments, persistent kernel in a CUDA graph)"
+        workload = {"workload": "256 join fragments", "fragments": 256, "tuples": units,
+                    "tuning": {"block_threads": tuning.block_threads, "blocks_per_sm": tuning.blocks_per_sm}}
+
+    ms, outs = _device_timed(torch, stream, fn, args.steps, args.warmup, dist)
+    # A second timed run with the clock sampler on; the line reports it.
+    launches0 = ctx.launches()
+    with Clocks(local) as clk:
+        ms, _ = _device_timed(torch, stream, fn, args.steps, 0, dist)
+    launches = ctx.launches() - launches0
+    step_ms = ms / args.steps
+    if args.workload == "batch":
+        lat = np.concatenate([o[1] for o in outs])
+        extra["fragment_latency_ms"] = {"p50": round(float(np.percentile(lat, 50)), 4),
+                                        "p99": round(float(np.percentile(lat, 99)), 4)}
+        plain_ms, _ = _device_timed(torch, stream, lambda: ctx.batch_run_plain(frags), max(1, args.steps // 2), 1,
+                                    dist)
+        extra["plain_launches_ms_per_step"] = round(plain_ms / max(1, args.steps // 2), 4)
+        ctx.batch_free(b)
+    achieved = abytes / (step_ms / 1e3) / 1e9
+    if rank == 0:
+        line = {"metric": metric, "value": units * args.steps * world / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded, device-generated)",
+                "config": dict(workload, parallelism=f"replicas{world}", scale_shift=sh),
+                "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                             "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": None,
+                             "algorithmic_bytes_per_step": abytes, "scope": "whole step"},
+                "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches, "clocks": clk.summary()}
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         main_reference(args)
+    elif args.workload != "join":
+        main_workload(args)
     else:
         main_gpu(args)
 
