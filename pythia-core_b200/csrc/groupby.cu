@@ -15,6 +15,7 @@
 #include <string.h>
 
 #include "primitives.cuh"
+#include "gbradix.cuh"
 
 namespace pyg {
 
@@ -325,6 +326,11 @@ extern "C" int pyg_groupby(pyg_ctx* ctx, const pyg_rel* in, const int32_t* key_c
     bool use_smem = expected_groups > 0 && expected_groups <= GB_SMEM_MAX_GROUPS;
     size_t smem = use_smem ? GB_SMEM_SLOTS * (2 * sizeof(unsigned long long) + sizeof(unsigned)) : 0;
     if (use_smem) PYG_CUDA(cudaFuncSetAttribute(groupby_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // 16-byte (int64 key @0, int64 value @8) tuples with a group estimate
+    // are aggregated in shared memory (gbradix.cu).
+    const bool fast16 = a.tb == 16 && ks.nkeys == 1 && ks.off0 == 0 && ks.type0 == PYG_INT64 &&
+                        (!want_sum || (a.sum_off == 8 && a.sum_type == PYG_INT64)) && (uintptr_t)a.base % 16 == 0 &&
+                        groupby16_eligible(expected_groups);
     ulonglong4* table = nullptr;
     uint64_t groups = 0, sent_sum = 0, sent_cnt = 0;
     for (;;) {
@@ -334,7 +340,9 @@ extern "C" int pyg_groupby(pyg_ctx* ctx, const pyg_rel* in, const int32_t* key_c
         PYG_CUDA(cudaMemsetAsync(a.flags, 0, 4 * sizeof(unsigned long long), ctx->stream));
         a.table = table;
         a.cap = cap;
-        if (a.n > 0) {
+        if (a.n > 0 && fast16) {
+            if ((rc = groupby16_fill(ctx, a.base, a.n, want_sum, expected_groups, table, cap, a.flags))) break;
+        } else if (a.n > 0) {
             int grid = grid_for(ctx, a.n, threads, 16, use_smem ? 2 : 8);
             if (use_smem) groupby_kernel<true><<<grid, threads, smem, ctx->stream>>>(a);
             else groupby_kernel<false><<<grid, threads, 0, ctx->stream>>>(a);

@@ -3,14 +3,15 @@
 #include <stdint.h>
 
 #include "pyg.h"
+#include "radixpart.cuh"
 
 struct pyg_ctx;
 
 namespace pyg {
 
-// Largest fine partition count (log2): the histogram kernel keeps 2^bits
-// 32-bit counters in shared memory.
-constexpr int RJ_MAX_FINE_BITS = 15;
+
+
+
 
 // Joins 16-byte (int64 key, int64 payload) device relations R and S on the
 // key and returns out = {match count, wrapped sum of R payloads, wrapped sum

@@ -1,0 +1,423 @@
+// Hash partitioning shared by the radix operators: kernels and host
+// helpers (declared in radixpart.cuh).
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "bulk.cuh"
+#include "radixpart.cuh"
+
+namespace pyg {
+
+#ifndef PYG_RJ_WARP_RANK
+#define PYG_RJ_WARP_RANK 0
+#endif
+constexpr int RJ_STAGES = 2;                               // input tiles in flight per partition CTA
+constexpr unsigned long long kBulkWaitNs = 2000000000ULL;  // 2 s
+
+__device__ __forceinline__ unsigned rj_bin(uint64_t h, int shift, unsigned mask)
+{
+    return shift >= 64 ? 0u : (unsigned)(h >> shift) & mask;
+}
+
+
+// ---------------------------------------------------------------------------
+// 1. Histogram of the top `bits` hash bits (bits <= 15: 128 KB of shared
+// counters per CTA).
+
+__global__ void __launch_bounds__(1024) rj_hist_kernel(const longlong2* __restrict__ in, int64_t n, int64_t step,
+                                                       int bits, unsigned long long* __restrict__ hist)
+{
+    // Counts in[0], in[step], in[2 step], ... (step 1: every tuple).
+    extern __shared__ unsigned rj_sh_hist[];
+    const int P = 1 << bits;
+    const int shift = 64 - bits;
+    const int64_t m = (n + step - 1) / step;
+    for (int b = threadIdx.x; b < P; b += blockDim.x) rj_sh_hist[b] = 0;
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    constexpr int U = 8;
+    for (; i + (U - 1) * stride < m; i += U * stride) {
+        longlong2 t[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) t[u] = __ldcs(&in[(i + u * stride) * step]);
+#pragma unroll
+        for (int u = 0; u < U; ++u) atomicAdd(&rj_sh_hist[rj_bin(mix64((uint64_t)t[u].x), shift, P - 1)], 1u);
+    }
+    for (; i < m; i += stride)
+        atomicAdd(&rj_sh_hist[rj_bin(mix64((uint64_t)__ldcs(&in[i * step]).x), shift, P - 1)], 1u);
+    __syncthreads();
+    for (int b = threadIdx.x; b < P; b += blockDim.x)
+        if (rj_sh_hist[b]) atomicAdd(&hist[b], (unsigned long long)rj_sh_hist[b]);
+}
+
+// Tiles per segment, as an exclusive prefix (one thread; at most 2^8
+// segments): tiles[C] is the pass's tile count.  Counts are first clamped
+// to their region's capacity, so a region that overflowed (its result is
+// discarded and redone) is never read past its end.
+__global__ void rj_tile_prefix_kernel(unsigned long long* __restrict__ count, const unsigned long long* __restrict__ cap,
+                                      int C, unsigned long long* __restrict__ tiles)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long t = 0;
+    tiles[0] = 0;
+    for (int c = 0; c < C; ++c) {
+        const unsigned long long n = count[c] < cap[c] ? count[c] : cap[c];
+        count[c] = n;
+        t += (n + RJ_TILE - 1) / RJ_TILE;
+        tiles[c + 1] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 2. Tile partition pass with exact offsets.  The input is a sequence of
+// segments (one for the first pass; the coarse partitions for the second);
+// tiles never straddle a segment.  Output bin of a tuple = (segment <<
+// lbits) | ((mix64(key) >> shift) & mask).
+
+struct RJPass {
+    const longlong2* in;
+    longlong2* out;
+    const unsigned long long* seg_start;  // nseg + 1 exact segment bounds in `in`
+    const unsigned long long* seg_tile0;  // nseg + 1 prefix of tiles per segment
+    int nseg;
+    int shift;
+    unsigned mask;
+    int lbits;
+    const unsigned long long* bin_start;  // output region start per output bin
+    unsigned long long* cursor;           // per output bin, zeroed before the pass
+    unsigned* err;                        // set if a tile's bulk copy never completed
+    // Optional (null when offsets are exact):
+    const unsigned long long* seg_count;  // tuples in each segment (segment end = start + count)
+    const unsigned long long* bin_cap;    // region capacity per output bin
+    unsigned* ovf;                        // set when a bin outgrows its region (the run is not written)
+    const unsigned long long* ntiles_dev; // tile count read on the device
+};
+
+struct RJTileRange {
+    long long begin, end;
+    int seg;
+};
+
+__device__ RJTileRange rj_tile_range(const RJPass& a, long long tile)
+{
+    int lo = 0, hi = a.nseg;  // seg_tile0[lo] <= tile < seg_tile0[hi]
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if ((long long)a.seg_tile0[mid] <= tile) lo = mid;
+        else hi = mid;
+    }
+    RJTileRange r;
+    r.seg = lo;
+    r.begin = (long long)a.seg_start[lo] + (tile - (long long)a.seg_tile0[lo]) * RJ_TILE;
+    const long long seg_end =
+        a.seg_count ? (long long)a.seg_start[lo] + (long long)a.seg_count[lo] : (long long)a.seg_start[lo + 1];
+    r.end = min(r.begin + RJ_TILE, seg_end);
+    return r;
+}
+
+// Shared memory of one partition CTA: a ring of RJ_STAGES input tiles that
+// bulk copies fill ahead of use, the grouped (staged) tile, and per-bin
+// counters.
+struct RJPartSmem {
+    longlong2 in[RJ_STAGES][RJ_TILE];
+    longlong2 stage[RJ_TILE];
+    unsigned short stage_bin[RJ_TILE];
+    unsigned hist[RJ_LMAX];
+    unsigned loff[RJ_LMAX];
+    unsigned long long gbase[RJ_LMAX];
+    uint64_t bar[RJ_STAGES];
+    RJTileRange info[RJ_STAGES];
+    unsigned warp_tot[RJ_PT_THREADS / 32];
+    int ok;
+};
+
+// Thread 0: starts the bulk copy of tile `tile` into ring slot `slot`.
+__device__ __forceinline__ void rj_issue_tile(const RJPass& a, RJPartSmem& sm, int slot, long long tile)
+{
+    const RJTileRange r = rj_tile_range(a, tile);
+    sm.info[slot] = r;
+    const unsigned bytes = (unsigned)(r.end - r.begin) * 16u;
+    mbar_arrive_expect_tx(&sm.bar[slot], bytes);
+    bulk_load(sm.in[slot], a.in + r.begin, bytes, &sm.bar[slot]);
+}
+
+__global__ void __launch_bounds__(RJ_PT_THREADS, 2) rj_partition_kernel(RJPass a, long long ntiles)
+{
+    if (a.ntiles_dev) ntiles = (long long)*a.ntiles_dev;
+    extern __shared__ __align__(128) unsigned char rj_pt_raw[];
+    RJPartSmem& sm = *reinterpret_cast<RJPartSmem*>(rj_pt_raw);
+    constexpr int PER = RJ_TILE / RJ_PT_THREADS;
+    const int L = 1 << a.lbits;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    for (int b = tid; b < RJ_LMAX; b += RJ_PT_THREADS) sm.hist[b] = 0;
+    if (tid == 0) {
+        for (int s = 0; s < RJ_STAGES; ++s) mbar_init(&sm.bar[s], 1);
+        mbar_fence_init();
+        for (int s = 0; s < RJ_STAGES; ++s)
+            if (blockIdx.x + (long long)s * gridDim.x < ntiles) rj_issue_tile(a, sm, s, blockIdx.x + (long long)s * gridDim.x);
+        sm.ok = 1;
+    }
+    __syncthreads();
+#if PYG_RJ_WARP_RANK
+    const unsigned lt_mask = (1u << lane) - 1u;
+#endif
+    long long k = 0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k) {
+        const int slot = (int)(k % RJ_STAGES);
+        const unsigned parity = (unsigned)((k / RJ_STAGES) & 1);
+        // Every thread waits for the tile; a wait that runs out marks the
+        // CTA failed and that thread's tuples are left out, so nothing is
+        // written from memory the copy did not fill.
+        const bool landed = mbar_wait(&sm.bar[slot], parity, kBulkWaitNs);
+        if (!landed) sm.ok = 0;
+        const RJTileRange cur = sm.info[slot];
+        const unsigned n = (unsigned)(cur.end - cur.begin);
+        // (1) Bin and rank every tuple; one shared atomic per (warp, bin).
+        longlong2 t[PER];
+        unsigned bin[PER], rank[PER];
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const unsigned i = j * RJ_PT_THREADS + tid;
+            const bool valid = landed && i < n;
+            bin[j] = 0xFFFFFFFFu;
+            if (valid) {
+                t[j] = sm.in[slot][i];
+                bin[j] = rj_bin(mix64((uint64_t)t[j].x), a.shift, a.mask);
+            }
+#if PYG_RJ_WARP_RANK
+            const unsigned peers = __match_any_sync(0xffffffffu, bin[j]);
+            const int leader = __ffs(peers) - 1;
+            unsigned base = 0;
+            if (valid && lane == leader) base = atomicAdd(&sm.hist[bin[j]], (unsigned)__popc(peers));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            rank[j] = base + __popc(peers & lt_mask);
+#else
+            if (valid) rank[j] = atomicAdd(&sm.hist[bin[j]], 1u);
+#endif
+        }
+        __syncthreads();  // A: histogram complete
+        if (!sm.ok) break;
+        // (2) Exclusive scan over bins (thread b owns bin b), reservation
+        // of each non-empty bin's run, and reset of the counter.
+        unsigned c = tid < L ? sm.hist[tid] : 0u;
+        unsigned incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) sm.warp_tot[w] = incl;
+        __syncthreads();  // B
+        unsigned excl = incl - c, total = 0;
+        for (int v = 0; v < RJ_PT_THREADS / 32; ++v) {
+            if (v == w) excl += total;
+            total += sm.warp_tot[v];
+        }
+        // The reservation's result (a global atomic, about a microsecond
+        // away) is first needed after the tile is staged.
+        unsigned long long resv = 0, bstart = 0, bcap = ~0ULL;
+        if (tid < L) {
+            sm.loff[tid] = excl;
+            if (c) {
+                const unsigned ob = ((unsigned)cur.seg << a.lbits) | (unsigned)tid;
+                bstart = a.bin_start[ob];
+                if (a.bin_cap) bcap = a.bin_cap[ob];
+                resv = atomicAdd(&a.cursor[ob], (unsigned long long)c);
+            }
+            sm.hist[tid] = 0;
+        }
+        __syncthreads();  // C: in-tile offsets ready
+        // (3) Group the tile by bin in shared memory.
+#pragma unroll
+        for (int j = 0; j < PER; ++j)
+            if (bin[j] != 0xFFFFFFFFu) {
+                const unsigned s = sm.loff[bin[j]] + rank[j];
+                sm.stage[s] = t[j];
+                sm.stage_bin[s] = (unsigned short)bin[j];
+            }
+        if (tid < L && c) {
+            unsigned long long gb = bstart + resv;
+            if (resv + c > bcap) {  // outgrew its region: not written; the host redoes the pass exactly
+                atomicOr(a.ovf, 1u);
+                gb = ~0ULL;
+            }
+            sm.gbase[tid] = gb;
+        }
+        __syncthreads();  // D: ring slot consumed, stage and global offsets complete
+        if (tid == 0) {
+            const long long nt = tile + (long long)RJ_STAGES * gridDim.x;
+            if (nt < ntiles) {
+                fence_proxy_async_smem();
+                rj_issue_tile(a, sm, slot, nt);
+            }
+        }
+        // (4) Write each bin's run contiguously.
+        for (unsigned i = tid; i < total; i += RJ_PT_THREADS) {
+            const unsigned b = sm.stage_bin[i];
+            const unsigned long long gb = sm.gbase[b];
+            if (gb != ~0ULL) __stcs(&a.out[gb + (i - sm.loff[b])], sm.stage[i]);
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && !sm.ok) atomicOr(a.err, 1u);
+}
+
+
+namespace {
+
+int launch_pass(pyg_ctx* ctx, const RJPass& p, long long ntiles)
+{
+    if (ntiles <= 0) return PYG_OK;
+    const size_t smem = sizeof(RJPartSmem);
+    PYG_CUDA(cudaFuncSetAttribute(rj_partition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rj_partition_kernel, RJ_PT_THREADS, smem));
+    if (per_sm < 1) per_sm = 1;
+    long long grid = std::min<long long>(ntiles, (long long)ctx->sm_count * per_sm);
+    rj_partition_kernel<<<(unsigned)grid, RJ_PT_THREADS, smem, ctx->stream>>>(p, ntiles);
+    PYG_LAUNCHED(ctx);
+    return PYG_OK;
+}
+
+// Host-side layout of one relation's partitions.  Exact layouts come from a
+// full histogram (dense, contiguous partitions); sampled layouts size each
+// partition's region from a strided sample with six standard deviations of
+
+}  // namespace
+
+void layout_exact(const std::vector<unsigned long long>& h, int C, int sub, RJLayout& L)
+{
+    const size_t F = h.size();
+    L.sampled = false;
+    L.fstart.assign(F + 1, 0);
+    for (size_t f = 0; f < F; ++f) L.fstart[f + 1] = L.fstart[f] + h[f];
+    L.cstart.assign(C + 1, 0);
+    for (int c = 0; c <= C; ++c) L.cstart[c] = L.fstart[(size_t)c << sub];
+    L.tiles2.assign(C + 1, 0);
+    for (int c = 0; c < C; ++c) L.tiles2[c + 1] = L.tiles2[c] + (L.cstart[c + 1] - L.cstart[c] + RJ_TILE - 1) / RJ_TILE;
+    L.fcap.clear();
+    L.ccap.clear();
+    L.count = h;
+    L.p1 = L.p2 = L.fstart[F];
+    L.tiles2_max = L.tiles2[C];
+}
+
+unsigned long long sampled_cap(unsigned long long c, long long step, unsigned long long extra)
+{
+    const double x = (double)c;
+    return (unsigned long long)std::ceil((x + 6.0 * std::sqrt(x) + 8.0) * (double)step) + extra;
+}
+
+void layout_sampled(const std::vector<unsigned long long>& sc, long long step, int C, int sub, RJLayout& L)
+{
+    const size_t F = sc.size();
+    L.sampled = true;
+    L.fcap.assign(F, 0);
+    L.fstart.assign(F + 1, 0);
+    for (size_t f = 0; f < F; ++f) {
+        L.fcap[f] = sampled_cap(sc[f], step, 64);
+        L.fstart[f + 1] = L.fstart[f] + L.fcap[f];
+    }
+    L.ccap.assign(C, 0);
+    L.cstart.assign(C + 1, 0);
+    L.tiles2_max = 0;
+    for (int c = 0; c < C; ++c) {
+        unsigned long long cc = 0;
+        for (size_t f = (size_t)c << sub; f < (size_t)(c + 1) << sub; ++f) cc += sc[f];
+        L.ccap[c] = sampled_cap(cc, step, 1024);
+        L.cstart[c + 1] = L.cstart[c] + L.ccap[c];
+        L.tiles2_max += (L.ccap[c] + RJ_TILE - 1) / RJ_TILE;
+    }
+    L.tiles2.clear();
+    L.count.clear();
+    L.p1 = L.cstart[C];
+    L.p2 = L.fstart[F];
+}
+
+int upload_layout(pyg_ctx* ctx, const RJLayout& L, const RJSideDev& d, int F, int C, int64_t n)
+{
+    PYG_CUDA(cudaMemcpyAsync(d.fstart, L.fstart.data(), (size_t)(F + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    PYG_CUDA(cudaMemcpyAsync(d.cstart, L.cstart.data(), (size_t)(C + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    if (L.sampled) {
+        PYG_CUDA(cudaMemcpyAsync(d.fcap, L.fcap.data(), (size_t)F * 8, cudaMemcpyHostToDevice, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(d.ccap, L.ccap.data(), (size_t)C * 8, cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+        PYG_CUDA(cudaMemcpyAsync(d.tiles2, L.tiles2.data(), (size_t)(C + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    PYG_CUDA(cudaMemsetAsync(d.cur1, 0, (size_t)(C + F) * 8, ctx->stream));  // cur1 and cur2 are adjacent
+    const unsigned long long w[4] = {0, (unsigned long long)n, 0, (unsigned long long)((n + RJ_TILE - 1) / RJ_TILE)};
+    PYG_CUDA(cudaMemcpyAsync(d.whole, w, sizeof(w), cudaMemcpyHostToDevice, ctx->stream));
+    return PYG_OK;
+}
+
+// Runs the partition pass(es) of one relation into P1 (and P2).
+int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, const RJSideDev& d, bool two, int FB,
+               int CB, void* P1, void* P2, unsigned* err, unsigned* ovf)
+{
+    const int C = 1 << CB, sub = FB - CB;
+    RJPass p;
+    memset(&p, 0, sizeof(p));
+    p.in = in;
+    p.out = (longlong2*)P1;
+    p.seg_start = d.whole;
+    p.seg_tile0 = d.wtiles;
+    p.nseg = 1;
+    p.shift = 64 - CB;
+    p.mask = (unsigned)(C - 1);
+    p.lbits = CB;
+    p.bin_start = two ? d.cstart : d.fstart;
+    p.bin_cap = L.sampled ? (two ? d.ccap : d.fcap) : nullptr;
+    p.cursor = two ? d.cur1 : d.cur2;
+    p.err = err;
+    p.ovf = ovf;
+    int rc = launch_pass(ctx, p, (n + RJ_TILE - 1) / RJ_TILE);
+    if (rc || !two) return rc;
+    long long ntiles2;
+    if (L.sampled) {
+        // Second-pass segments are the first pass's regions, filled to the
+        // counts its cursors reached; the tile prefix is formed on the device.
+        rj_tile_prefix_kernel<<<1, 32, 0, ctx->stream>>>(d.cur1, d.ccap, C, d.tiles2);
+        PYG_LAUNCHED(ctx);
+        p.seg_count = d.cur1;
+        p.ntiles_dev = d.tiles2 + C;
+        ntiles2 = (long long)L.tiles2_max;
+    } else {
+        ntiles2 = (long long)L.tiles2[C];
+    }
+    p.in = (const longlong2*)P1;
+    p.out = (longlong2*)P2;
+    p.seg_start = d.cstart;
+    p.seg_tile0 = d.tiles2;
+    p.nseg = C;
+    p.shift = 64 - FB;
+    p.mask = (unsigned)((1 << sub) - 1);
+    p.lbits = sub;
+    p.bin_start = d.fstart;
+    p.bin_cap = L.sampled ? d.fcap : nullptr;
+    p.cursor = d.cur2;
+    return launch_pass(ctx, p, ntiles2);
+}
+
+int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int FB, unsigned long long* hist)
+{
+    const size_t hsm = (size_t)4 << FB;
+    PYG_CUDA(cudaFuncSetAttribute(rj_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
+    int per = 0;
+    PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rj_hist_kernel, 1024, hsm));
+    if (per < 1) per = 1;
+    const int64_t m = (n + step - 1) / step;
+    const int64_t want = (m + 1024 * 8 - 1) / (1024 * 8);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->sm_count * per));
+    PYG_CUDA(cudaMemsetAsync(hist, 0, (size_t)8 << FB, ctx->stream));
+    rj_hist_kernel<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, FB, hist);
+    PYG_LAUNCHED(ctx);
+    return PYG_OK;
+}
+
+}  // namespace pyg

@@ -1,0 +1,89 @@
+// Hash partitioning of 16-byte (int64 key, int64 payload) tuples by the
+// top bits of mix64(key), shared by the radix operators (join, group-by).
+//
+//   histogram   rj_hist_kernel counts the top `bits` bits of every tuple (or
+//               of a strided sample) in shared memory.
+//   layout      exact (dense partitions from a full histogram) or sampled
+//               (regions sized from the sample with six standard deviations
+//               of slack; a region that overflows is reported and the caller
+//               redoes the side exactly).
+//   passes      one tile pass (<= 9 bits) or two (coarse bits, then the rest
+//               inside each coarse partition).  A CTA receives 2048-tuple
+//               tiles by bulk copy into a two-deep shared-memory ring, groups
+//               a tile by bin in shared memory and writes each bin's run
+//               contiguously after one global reservation per (tile, bin).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "pyg_internal.cuh"
+
+namespace pyg {
+
+constexpr int RJ_TILE = 2048;            // tuples per partition tile
+constexpr int RJ_PT_THREADS = 512;       // partition CTA
+constexpr int RJ_MAX_LOCAL_BITS = 9;     // bins of one partition pass
+constexpr int RJ_LMAX = 1 << RJ_MAX_LOCAL_BITS;
+// Largest fine partition count (log2): the histogram kernel keeps 2^bits
+// 32-bit counters in shared memory.
+constexpr int RJ_MAX_FINE_BITS = 15;
+
+// Host-side layout of one relation's partitions.
+struct RJLayout {
+    bool sampled = false;
+    std::vector<unsigned long long> fstart;  // F + 1 fine region starts
+    std::vector<unsigned long long> fcap;    // F fine region capacities (sampled)
+    std::vector<unsigned long long> cstart;  // C + 1 coarse region starts
+    std::vector<unsigned long long> ccap;    // C coarse region capacities (sampled)
+    std::vector<unsigned long long> tiles2;  // C + 1 tile prefix of the second pass (exact)
+    std::vector<unsigned long long> count;   // F tuples per fine partition, once known
+    unsigned long long p1 = 0, p2 = 0;       // tuples in the pass-1 / pass-2 buffers
+    unsigned long long tiles2_max = 0;       // upper bound of the second pass's tiles (sampled)
+};
+
+// Exact layout from exact per-fine-partition counts h (F = h.size()).
+void layout_exact(const std::vector<unsigned long long>& h, int C, int sub, RJLayout& L);
+// Sampled layout from the counts sc of every step-th tuple: each region is
+// sized with six standard deviations of slack.
+void layout_sampled(const std::vector<unsigned long long>& sc, long long step, int C, int sub, RJLayout& L);
+
+// Device copy of one relation's partition metadata (u64 words).
+struct RJSideDev {
+    unsigned long long *fstart, *fcap, *cstart, *ccap, *cur1, *cur2, *tiles2, *whole, *wtiles;
+    static size_t words(int F, int C) { return (size_t)(F + 1) + F + (C + 1) + C + C + F + (C + 1) + 4; }
+    void carve(unsigned long long* m, int F, int C)
+    {
+        fstart = m;
+        fcap = fstart + F + 1;
+        cstart = fcap + F;
+        ccap = cstart + C + 1;
+        cur1 = ccap + C;
+        cur2 = cur1 + C;
+        tiles2 = cur2 + F;
+        whole = tiles2 + C + 1;
+        wtiles = whole + 2;
+    }
+};
+
+// Copies a layout to the device and zeroes its cursors.
+int upload_layout(pyg_ctx* ctx, const RJLayout& L, const RJSideDev& d, int F, int C, int64_t n);
+// Histogram of the top FB hash bits of in[0], in[step], ... into hist
+// (2^FB device words, zeroed here).
+int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int FB, unsigned long long* hist);
+// Partition pass(es) of one relation into P1 (and P2 when two): *err is set
+// if a tile's bulk copy never landed, *ovf if a sampled region overflowed.
+// Afterwards d.cur2 holds the tuples written per fine partition.
+int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, const RJSideDev& d, bool two, int FB,
+               int CB, void* P1, void* P2, unsigned* err, unsigned* ovf);
+
+// Slot of a key in a shared-memory table of TS slots: multiply-high of the
+// 32 hash bits below the fine partition bits (all keys of one partition
+// share the top fine_bits bits).
+__device__ __forceinline__ unsigned rj_slot(uint64_t h, int fb, unsigned TS)
+{
+    return __umulhi((unsigned)(h >> (32 - fb)), TS);
+}
+
+}  // namespace pyg

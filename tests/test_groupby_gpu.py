@@ -52,6 +52,36 @@ def test_groupby_random_vs_oracle(ctx, torch_cuda, G, expected, zipf):
     assert rows(out) == rows(ref)
 
 
+@pytest.mark.parametrize("G,expected,n", [(1 << 21, 1 << 21, (1 << 25) + 777),  # two passes, sampled layout
+                                          (1 << 18, 1 << 12, 1 << 22),          # estimate 64x too small
+                                          (3000, 3000, 1 << 22)])                # one shared table per CTA
+def test_groupby_shared_memory_paths(ctx, torch_cuda, G, expected, n):
+    """16-byte (int64, int64) tuples with a group estimate are aggregated in
+    shared memory, partitioned by hash when the estimate is large; keys that
+    do not fit a shared table go to the HBM table, so a wrong estimate only
+    costs time."""
+    rng = np.random.default_rng(G + n)
+    gid = rng.integers(0, G, n)
+    perm = rng.permutation(G).astype(np.int64) * 7919 - (1 << 50)
+    A = struct([perm[gid], rng.integers(-(1 << 62), 1 << 62, n)], [I64, I64])
+    out = run_groupby(ctx, torch_cuda, A, [I64, I64], [0], 3, 1, expected)
+    assert rows(out) == rows(O.groupby(A, [I64, I64], [0], 3, 1, buckets=G))
+
+
+def test_groupby_uniform_warps_and_sentinel(ctx, torch_cuda):
+    """Runs of one key (whole warps fold with one reduction) mixed with the
+    INT64_MIN group and count-only output."""
+    mn = np.iinfo(np.int64).min
+    rng = np.random.default_rng(5)
+    n = (1 << 20) + 100
+    k = np.repeat(rng.integers(0, 50, n // 64 + 1), 64)[:n].astype(np.int64)
+    k[rng.random(n) < 0.01] = mn
+    A = struct([k, rng.integers(0, 1 << 40, n)], [I64, I64])
+    for flags in (3, 2, 1):
+        out = run_groupby(ctx, torch_cuda, A, [I64, I64], [0], flags, 1, 64)
+        assert rows(out) == rows(O.groupby(A, [I64, I64], [0], flags, 1))
+
+
 def test_groupby_edge_cases(ctx, torch_cuda):
     mn = np.iinfo(np.int64).min
     A = struct([np.array([mn, 3, mn, 3, 9, -1], dtype=np.int64), np.array([1, 2, 3, 4, 5, 6], dtype=np.int64)],
