@@ -497,13 +497,14 @@ def main_workload(args):
         ctx.gen_pk(R, nR, 7, SEED_KEYS)
         ctx.gen_fk(S, nS, nR, 0.0, SEED_KEYS, 1000, SEED_PROBE + rank)
         Rr, Sr = pyg.Rel(R, nR, [I64, I64]), pyg.Rel(S, nS, [I64, I64])
-        fn = lambda: ctx.hashjoin_agg(Rr, [0], Sr, [0], [(1, 1)])  # noqa: E731
+        algo = {"radix": pyg.JOIN_RADIX, "direct": pyg.JOIN_DIRECT, "auto": pyg.JOIN_AUTO}[args.algo]
+        fn = lambda: ctx.hashjoin_agg(Rr, [0], Sr, [0], [(1, 1)], algo)  # noqa: E731
         cnt, sums = fn()
         Sv = S.view(nS, 2)
         assert cnt == nS and sums[0] & 0xFFFFFFFFFFFFFFFF == int(Sv[:, 1].sum().item()) & 0xFFFFFFFFFFFFFFFF
         units, abytes = nR + nS, (nR + nS) * 16 + 16
         metric = "join+sum tuples/sec (R 2^20 PK, S 2^24 FK, projection P$1)"
-        workload = {"workload": "hash join + sum of P$1", "build_tuples": nR, "probe_tuples": nS}
+        workload = {"workload": "hash join + sum of P$1", "build_tuples": nR, "probe_tuples": nS, "algo": args.algo}
         if rank == 0 and world == 1 and not args.no_cpu:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
             import refrun

@@ -16,7 +16,13 @@ namespace pyg {
 #ifndef PYG_RJ_WARP_RANK
 #define PYG_RJ_WARP_RANK 0
 #endif
-constexpr int RJ_STAGES = 2;                               // input tiles in flight per partition CTA
+#ifndef PYG_RJ_PT_MINB
+#define PYG_RJ_PT_MINB 2
+#endif
+#ifndef PYG_RJ_STAGES
+#define PYG_RJ_STAGES 2
+#endif
+constexpr int RJ_STAGES = PYG_RJ_STAGES;                               // input tiles in flight per partition CTA
 constexpr unsigned long long kBulkWaitNs = 2000000000ULL;  // 2 s
 
 __device__ __forceinline__ unsigned rj_bin(uint64_t h, int shift, unsigned mask)
@@ -147,7 +153,7 @@ __device__ __forceinline__ void rj_issue_tile(const RJPass& a, RJPartSmem& sm, i
     bulk_load(sm.in[slot], a.in + r.begin, bytes, &sm.bar[slot]);
 }
 
-__global__ void __launch_bounds__(RJ_PT_THREADS, 2) rj_partition_kernel(RJPass a, long long ntiles)
+__global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_kernel(RJPass a, long long ntiles)
 {
     if (a.ntiles_dev) ntiles = (long long)*a.ntiles_dev;
     extern __shared__ __align__(128) unsigned char rj_pt_raw[];

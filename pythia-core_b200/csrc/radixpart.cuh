@@ -22,8 +22,14 @@
 
 namespace pyg {
 
-constexpr int RJ_TILE = 2048;            // tuples per partition tile
-constexpr int RJ_PT_THREADS = 512;       // partition CTA
+#ifndef PYG_RJ_TILE
+#define PYG_RJ_TILE 2048
+#endif
+#ifndef PYG_RJ_PT_THREADS
+#define PYG_RJ_PT_THREADS 512
+#endif
+constexpr int RJ_TILE = PYG_RJ_TILE;            // tuples per partition tile
+constexpr int RJ_PT_THREADS = PYG_RJ_PT_THREADS;  // partition CTA
 constexpr int RJ_MAX_LOCAL_BITS = 9;     // bins of one partition pass
 constexpr int RJ_LMAX = 1 << RJ_MAX_LOCAL_BITS;
 // Largest fine partition count (log2): the histogram kernel keeps 2^bits
