@@ -25,6 +25,7 @@
 
 #include "../../include/pyg_learned.h"
 #include "../../include/pyg_mpsm.h"
+#include "mpsm16.cuh"
 #include "partition.cuh"
 #include "primitives.cuh"
 
@@ -452,11 +453,23 @@ static int mpsm_run(pyg_ctx* ctx, const pyg_rel* build, int32_t bkey, const pyg_
     longlong2 *Ri, *Si;
     if ((rc = items_of(build, Rd.rel, bkey, bcol, nR, &Ri)) || (rc = items_of(probe, Sd.rel, pkey, pcol, nS, &Si)))
         return fail(rc);
+    // Aggregate sink over 16-byte (int64 key, int64 payload) device tuples
+    // summing column 1 of either side: range partitions small enough to be
+    // sorted in shared memory (mpsm16.cu), with splitters of the same kind
+    // at that finer fan-out.
+    auto is16 = [](const pyg_rel* r, int key, int col) {
+        return r->on_device && r->tuple_bytes == 16 && r->col_offset[key] == 0 && r->col_type[key] == PYG_INT64 &&
+               (col < 0 || (col == 1 && r->col_offset[1] == 8 && r->col_type[1] == PYG_INT64)) &&
+               (uintptr_t)r->base % 16 == 0;
+    };
+    const bool fast = !materialize && is16(build, bkey, bcol) && is16(probe, pkey, pcol) && nR > 0 && nS > 0;
+    const int FBf = fast ? mpsm16_fine_bits(nR, nS) : 0;
+    const int Fs = fast ? (1 << FBf) : F;
 
     // ---- 1. splitters
-    std::vector<int64_t> spl(F > 1 ? F - 1 : 0);
+    std::vector<int64_t> spl(Fs > 1 ? Fs - 1 : 0);
     unsigned long long* h = (unsigned long long*)ctx->pinned + 256;
-    if (F > 1 && nR + nS > 0) {
+    if (Fs > 1 && nR + nS > 0) {
         if (o->splitter_kind == PYG_MPSM_SPLIT_EXACTRANGE || nS == 0) {
             unsigned long long* mm = ctx->dcounters + 96;
             unsigned long long init[2] = {~0ULL, 0ULL};
@@ -471,8 +484,8 @@ static int mpsm_run(pyg_ctx* ctx, const pyg_rel* build, int32_t bkey, const pyg_
             // ExactRangeValueHasher(min, max, F) (hash.h:452-487): bucket
             // range br = (max - min + F) / F, bucket = (v - min) / br, i.e.
             // splitter j = min + j * br (clamped to the int64 range).
-            __int128 br = ((__int128)mx - (__int128)mn + F) / F;
-            for (int j = 1; j < F; ++j) {
+            __int128 br = ((__int128)mx - (__int128)mn + Fs) / Fs;
+            for (int j = 1; j < Fs; ++j) {
                 __int128 v = (__int128)mn + (__int128)j * br;
                 spl[j - 1] = v > (__int128)INT64_MAX ? INT64_MAX : (int64_t)v;
             }
@@ -491,7 +504,7 @@ static int mpsm_run(pyg_ctx* ctx, const pyg_rel* build, int32_t bkey, const pyg_
             mp_sample_kernel<<<grid_for(ctx, ns, 256, 4, 4), 256, 0, ctx->stream>>>(Si, nS, stride, offset, ns, sample);
             PYG_LAUNCHED(ctx);
             if (o->splitter_kind == PYG_MPSM_SPLIT_SAMPLED || ns < 2) {
-                if ((rc = pyg_sampled_splitters(ctx, sample, ns, F, spl.data()))) return fail(rc);
+                if ((rc = pyg_sampled_splitters(ctx, sample, ns, Fs, spl.data()))) return fail(rc);
             } else {
                 pyg_cdf_train_opts to;
                 to.leaves = o->cdf_leaves > 0 ? o->cdf_leaves : 1024;
@@ -500,13 +513,44 @@ static int mpsm_run(pyg_ctx* ctx, const pyg_rel* build, int32_t bkey, const pyg_
                 to.seed = o->seed;
                 pyg_cdf* model = nullptr;
                 if ((rc = pyg_cdf_train(ctx, sample, ns, &to, &model))) return fail(rc);
-                rc = pyg_cdf_splitters(ctx, model, F, spl.data());
+                rc = pyg_cdf_splitters(ctx, model, Fs, spl.data());
                 pyg_cdf_free(ctx, model);
                 if (rc) return fail(rc);
             }
         }
     }
     cudaEventRecord(ev[1], ctx->stream);
+    if (fast) {
+        unsigned long long o3[3];
+        std::vector<unsigned long long> sizes;
+        float part_ms = 0.f, join_ms = 0.f;
+        if ((rc = mpsm16_agg(ctx, Ri, nR, Si, nS, spl.data(), FBf, o3, &sizes, &part_ms, &join_ms))) return fail(rc);
+        memset(res, 0, sizeof(*res));
+        res->count = (int64_t)o3[0];
+        for (int p = 0; p < nproj; ++p) res->sums[p] = (int64_t)(proj[p].side ? o3[2] : o3[1]);
+        if (stats) {
+            // Imbalance over the caller's fan-out: its ranges are unions of
+            // 2^FB / F consecutive fine ranges when F divides 2^FB.
+            memset(stats, 0, sizeof(*stats));
+            const int G = (Fs % F == 0) ? F : Fs;
+            const int per = Fs / G;
+            int64_t mx = 0;
+            for (int g = 0; g < G; ++g) {
+                int64_t t = 0;
+                for (int q = 0; q < per; ++q) t += (int64_t)sizes[(size_t)g * per + q];
+                mx = std::max(mx, t);
+            }
+            stats->max_partition = mx;
+            stats->max_partition_imbalance = (double)mx / ((double)nS / G);
+            float spl_ms = 0.f;
+            cudaEventElapsedTime(&spl_ms, ev[0], ev[1]);
+            stats->splitter_ms = spl_ms;
+            stats->partition_ms = part_ms;
+            stats->sort_ms = 0;  // the sort runs inside the merge kernel
+            stats->merge_ms = join_ms;
+        }
+        return fail(0);
+    }
 
     // ---- 2. range partition both sides
     longlong2 *Rp, *Sp, *Rt, *St;

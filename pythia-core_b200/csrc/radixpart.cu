@@ -13,9 +13,6 @@
 
 namespace pyg {
 
-#ifndef PYG_RJ_WARP_RANK
-#define PYG_RJ_WARP_RANK 0
-#endif
 #ifndef PYG_RJ_PT_MINB
 #define PYG_RJ_PT_MINB 2
 #endif
@@ -103,6 +100,10 @@ struct RJPass {
     const unsigned long long* bin_cap;    // region capacity per output bin
     unsigned* ovf;                        // set when a bin outgrows its region (the run is not written)
     const unsigned long long* ntiles_dev; // tile count read on the device
+    // Range mode (nsplit > 0): bin = number of splitters <= key among the
+    // segment's nsplit splitters, split + seg * 2^lbits (one segment: split).
+    const long long* split;
+    int nsplit;
 };
 
 struct RJTileRange {
@@ -140,8 +141,60 @@ struct RJPartSmem {
     uint64_t bar[RJ_STAGES];
     RJTileRange info[RJ_STAGES];
     unsigned warp_tot[RJ_PT_THREADS / 32];
+    long long split[2][RJ_SPLIT_MAX];  // range mode: the splitters of this tile and the next
     int ok;
 };
+static_assert(2 * (sizeof(RJPartSmem) + 1024) <= 233472, "two partition CTAs per SM");
+
+__device__ __forceinline__ unsigned rj_range_bin(const long long* sp, int n, long long k)
+{
+    int lo = 0;
+    while (n > 0) {
+        const int half = n >> 1;
+        if (k >= sp[lo + half]) {
+            lo += half + 1;
+            n -= half + 1;
+        } else {
+            n = half;
+        }
+    }
+    return (unsigned)lo;
+}
+
+// All threads: the splitters of segment seg into dst.
+__device__ __forceinline__ void rj_load_split(const RJPass& a, long long* dst, int seg)
+{
+    const long long* src = a.split + (a.nseg > 1 ? ((long long)seg << a.lbits) : 0);
+    for (int i = threadIdx.x; i < a.nsplit; i += RJ_PT_THREADS) dst[i] = src[i];
+}
+
+// Histogram of range bins of in[0], in[step], ...: fine bin = coarse bin
+// (among C - 1 coarse splitters held in shared memory) * 2^sub + bin among
+// that coarse range's 2^sub - 1 fine splitters (read from global memory).
+__global__ void __launch_bounds__(1024) rj_hist_range_kernel(const longlong2* __restrict__ in, int64_t n, int64_t step,
+                                                             int CB, int sub, const long long* __restrict__ csplit,
+                                                             const long long* __restrict__ fsplit,
+                                                             unsigned long long* __restrict__ hist)
+{
+    extern __shared__ __align__(16) unsigned char rj_hr_raw[];
+    const int F = 1 << (CB + sub), C = 1 << CB, L = 1 << sub;
+    long long* cs = (long long*)rj_hr_raw;
+    unsigned* h = (unsigned*)(cs + RJ_SPLIT_MAX);
+    for (int b = threadIdx.x; b < F; b += blockDim.x) h[b] = 0;
+    for (int i = threadIdx.x; i < C - 1; i += blockDim.x) cs[i] = csplit[i];
+    __syncthreads();
+    const int64_t m = (n + step - 1) / step;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += stride) {
+        const long long k = __ldcs(&in[i * step]).x;
+        unsigned f = rj_range_bin(cs, C - 1, k);
+        if (sub) f = (f << sub) | rj_range_bin(fsplit + ((long long)f << sub), L - 1, k);
+        atomicAdd(&h[f], 1u);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < F; b += blockDim.x)
+        if (h[b]) atomicAdd(&hist[b], (unsigned long long)h[b]);
+}
 
 // Thread 0: starts the bulk copy of tile `tile` into ring slot `slot`.
 __device__ __forceinline__ void rj_issue_tile(const RJPass& a, RJPartSmem& sm, int slot, long long tile)
@@ -170,9 +223,10 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
         sm.ok = 1;
     }
     __syncthreads();
-#if PYG_RJ_WARP_RANK
-    const unsigned lt_mask = (1u << lane) - 1u;
-#endif
+    if (a.nsplit) {
+        rj_load_split(a, sm.split[0], sm.info[0].seg);
+        __syncthreads();
+    }
     long long k = 0;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k) {
         const int slot = (int)(k % RJ_STAGES);
@@ -194,18 +248,10 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
             bin[j] = 0xFFFFFFFFu;
             if (valid) {
                 t[j] = sm.in[slot][i];
-                bin[j] = rj_bin(mix64((uint64_t)t[j].x), a.shift, a.mask);
+                bin[j] = a.nsplit ? rj_range_bin(sm.split[a.nseg > 1 ? (k & 1) : 0], a.nsplit, t[j].x)
+                                  : rj_bin(mix64((uint64_t)t[j].x), a.shift, a.mask);
             }
-#if PYG_RJ_WARP_RANK
-            const unsigned peers = __match_any_sync(0xffffffffu, bin[j]);
-            const int leader = __ffs(peers) - 1;
-            unsigned base = 0;
-            if (valid && lane == leader) base = atomicAdd(&sm.hist[bin[j]], (unsigned)__popc(peers));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            rank[j] = base + __popc(peers & lt_mask);
-#else
             if (valid) rank[j] = atomicAdd(&sm.hist[bin[j]], 1u);
-#endif
         }
         __syncthreads();  // A: histogram complete
         if (!sm.ok) break;
@@ -247,6 +293,10 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
                 sm.stage[s] = t[j];
                 sm.stage_bin[s] = (unsigned short)bin[j];
             }
+        // Range mode over several segments: the next tile's splitters
+        // (its copy was issued a tile ago, so its segment is known).
+        if (a.nsplit && a.nseg > 1 && tile + gridDim.x < ntiles)
+            rj_load_split(a, sm.split[(k + 1) & 1], sm.info[(k + 1) % RJ_STAGES].seg);
         if (tid < L && c) {
             unsigned long long gb = bstart + resv;
             if (resv + c > bcap) {  // outgrew its region: not written; the host redoes the pass exactly
@@ -364,7 +414,8 @@ int upload_layout(pyg_ctx* ctx, const RJLayout& L, const RJSideDev& d, int F, in
 
 // Runs the partition pass(es) of one relation into P1 (and P2).
 int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, const RJSideDev& d, bool two, int FB,
-               int CB, void* P1, void* P2, unsigned* err, unsigned* ovf)
+               int CB, void* P1, void* P2, unsigned* err, unsigned* ovf, const long long* csplit,
+               const long long* fsplit)
 {
     const int C = 1 << CB, sub = FB - CB;
     RJPass p;
@@ -382,6 +433,10 @@ int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, 
     p.cursor = two ? d.cur1 : d.cur2;
     p.err = err;
     p.ovf = ovf;
+    if (csplit) {
+        p.split = csplit;
+        p.nsplit = C - 1;
+    }
     int rc = launch_pass(ctx, p, (n + RJ_TILE - 1) / RJ_TILE);
     if (rc || !two) return rc;
     long long ntiles2;
@@ -407,6 +462,10 @@ int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, 
     p.bin_start = d.fstart;
     p.bin_cap = L.sampled ? d.fcap : nullptr;
     p.cursor = d.cur2;
+    if (fsplit) {
+        p.split = fsplit;
+        p.nsplit = (1 << sub) - 1;
+    }
     return launch_pass(ctx, p, ntiles2);
 }
 
@@ -424,6 +483,89 @@ int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int 
     rj_hist_kernel<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, FB, hist);
     PYG_LAUNCHED(ctx);
     return PYG_OK;
+}
+
+int hist_launch_range(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int CB, int sub,
+                      const long long* csplit, const long long* fsplit, unsigned long long* hist)
+{
+    const int F = 1 << (CB + sub);
+    const size_t hsm = (size_t)RJ_SPLIT_MAX * 8 + (size_t)4 * F;
+    PYG_CUDA(cudaFuncSetAttribute(rj_hist_range_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
+    int per = 0;
+    PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rj_hist_range_kernel, 1024, hsm));
+    if (per < 1) per = 1;
+    const int64_t m = (n + step - 1) / step;
+    const int64_t want = (m + 1024 * 8 - 1) / (1024 * 8);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->sm_count * per));
+    PYG_CUDA(cudaMemsetAsync(hist, 0, (size_t)8 * F, ctx->stream));
+    rj_hist_range_kernel<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, CB, sub, csplit, fsplit, hist);
+    PYG_LAUNCHED(ctx);
+    return PYG_OK;
+}
+
+int rp_partition(pyg_ctx* ctx, const longlong2* in, int64_t n, int FB, bool two, bool allow_sample,
+                 const long long* csplit, const long long* fsplit, RJLayout& L, void** P1, void** P2,
+                 unsigned* flags, unsigned* hflags)
+{
+    const int CB = two ? (FB + 1) / 2 : FB;
+    const int F = 1 << FB, C = 1 << CB, sub = FB - CB;
+    const bool sample = allow_sample && two && n >= ((int64_t)1 << 25);
+    const int64_t step = sample ? std::max<int64_t>(1, n >> 24) : 1;
+    const size_t side = RJSideDev::words(F, C);
+    unsigned long long* meta = nullptr;
+    *P1 = *P2 = nullptr;
+    int rc = PYG_OK;
+    auto hist_of = [&](int64_t st, unsigned long long* hist) {
+        return csplit ? hist_launch_range(ctx, in, n, st, CB, sub, csplit, fsplit, hist)
+                      : hist_launch(ctx, in, n, st, FB, hist);
+    };
+    do {
+        if ((rc = dalloc(ctx, (void**)&meta, (side + F) * 8))) break;
+        RJSideDev d;
+        d.carve(meta, F, C);
+        unsigned long long* hist = meta + side;
+        PYG_CUDA(cudaMemsetAsync(flags, 0, 8, ctx->stream));
+        if ((rc = hist_of(step, hist))) break;
+        std::vector<unsigned long long> h(F);
+        PYG_CUDA(cudaMemcpyAsync(h.data(), hist, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (sample) layout_sampled(h, step, C, sub, L);
+        else layout_exact(h, C, sub, L);
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            if ((rc = upload_layout(ctx, L, d, F, C, n))) break;
+            dfree(ctx, *P1);
+            dfree(ctx, *P2);
+            *P1 = *P2 = nullptr;
+            if ((rc = dalloc(ctx, P1, (size_t)L.p1 * 16))) break;
+            if (two && (rc = dalloc(ctx, P2, (size_t)L.p2 * 16))) break;
+            if ((rc = run_passes(ctx, in, n, L, d, two, FB, CB, *P1, *P2, flags, flags + 1, csplit, fsplit))) break;
+            PYG_CUDA(cudaMemcpyAsync(hflags, flags, 8, cudaMemcpyDeviceToHost, ctx->stream));
+            if (L.sampled) {
+                L.count.resize(F);
+                PYG_CUDA(cudaMemcpyAsync(L.count.data(), d.cur2, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            }
+            PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+            if (hflags[0]) {
+                set_error("partition: a tile copy did not complete in time");
+                rc = PYG_ERR_TIMEOUT;
+                break;
+            }
+            if (!hflags[1]) break;
+            // A sampled region overflowed: redo from an exact histogram.
+            if ((rc = hist_of(1, hist))) break;
+            PYG_CUDA(cudaMemcpyAsync(h.data(), hist, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+            layout_exact(h, C, sub, L);
+            PYG_CUDA(cudaMemsetAsync(flags, 0, 8, ctx->stream));
+        }
+    } while (0);
+    dfree(ctx, meta);
+    if (rc) {
+        dfree(ctx, *P1);
+        dfree(ctx, *P2);
+        *P1 = *P2 = nullptr;
+    }
+    return rc;
 }
 
 }  // namespace pyg

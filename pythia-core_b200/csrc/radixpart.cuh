@@ -32,6 +32,7 @@ constexpr int RJ_TILE = PYG_RJ_TILE;            // tuples per partition tile
 constexpr int RJ_PT_THREADS = PYG_RJ_PT_THREADS;  // partition CTA
 constexpr int RJ_MAX_LOCAL_BITS = 9;     // bins of one partition pass
 constexpr int RJ_LMAX = 1 << RJ_MAX_LOCAL_BITS;
+constexpr int RJ_SPLIT_MAX = 256;        // range mode: splitters per pass segment (<= 2^8 bins)
 // Largest fine partition count (log2): the histogram kernel keeps 2^bits
 // 32-bit counters in shared memory.
 constexpr int RJ_MAX_FINE_BITS = 15;
@@ -81,8 +82,25 @@ int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int 
 // Partition pass(es) of one relation into P1 (and P2 when two): *err is set
 // if a tile's bulk copy never landed, *ovf if a sampled region overflowed.
 // Afterwards d.cur2 holds the tuples written per fine partition.
+// Range mode when csplit is set: pass 1 bins by the 2^CB - 1 coarse
+// splitters, pass 2 by the fine splitters (F - 1, ascending; coarse
+// splitter i = fine splitter (i + 1) * 2^(FB - CB) - 1).
 int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, const RJSideDev& d, bool two, int FB,
-               int CB, void* P1, void* P2, unsigned* err, unsigned* ovf);
+               int CB, void* P1, void* P2, unsigned* err, unsigned* ovf, const long long* csplit = nullptr,
+               const long long* fsplit = nullptr);
+// Histogram of range bins (see run_passes) of in[0], in[step], ...
+int hist_launch_range(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int CB, int sub,
+                      const long long* csplit, const long long* fsplit, unsigned long long* hist);
+// Partitions one relation into 2^FB partitions (hash bits, or ranges when
+// csplit is set; two passes when `two`): histogram (sampled when allowed
+// and n >= 2^25), layout, passes, and an exact redo if a sampled region
+// overflowed.  On success the partitions are in (two ? *P2 : *P1) at
+// L.fstart with L.count tuples each; the caller frees *P1 and *P2.  flags:
+// two device words (bulk copy never landed, region overflow); hflags: two
+// pinned host words.
+int rp_partition(pyg_ctx* ctx, const longlong2* in, int64_t n, int FB, bool two, bool allow_sample,
+                 const long long* csplit, const long long* fsplit, RJLayout& L, void** P1, void** P2,
+                 unsigned* flags, unsigned* hflags);
 
 // Slot of a key in a shared-memory table of TS slots: multiply-high of the
 // 32 hash bits below the fine partition bits (all keys of one partition
