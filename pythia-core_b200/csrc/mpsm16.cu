@@ -196,7 +196,7 @@ int mpsm16_fine_bits(int64_t nR, int64_t nS)
 {
     // Ranges of about 8K probe and at most ~3K build tuples on uniform data.
     int fb = 1;
-    while (fb < RJ_MAX_FINE_BITS && ((double)nS / (double)(1 << fb) > 8192.0 || (double)nR / (double)(1 << fb) > 3072.0))
+    while (fb < RJ_MAX_RANGE_BITS && ((double)nS / (double)(1 << fb) > 8192.0 || (double)nR / (double)(1 << fb) > 3072.0))
         ++fb;
     return fb;
 }

@@ -285,7 +285,7 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
     const longlong2* S = (const longlong2*)Sv;
     out[0] = out[1] = out[2] = 0;
     if (fine_bits <= 0) {
-        // Fine partitions of about 0.7 x the table's build capacity.
+        // Partitions of about 0.7 x the table's build capacity.
         fine_bits = 1;
         while (fine_bits < RJ_MAX_FINE_BITS && (double)nR / (double)(1 << fine_bits) > 0.7 * RJ_RCAP_UNIQUE)
             ++fine_bits;
@@ -296,87 +296,33 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
     }
     const int FB = fine_bits;
     const bool two = FB > RJ_MAX_LOCAL_BITS;
-    const int CB = two ? (FB + 1) / 2 : FB;
-    const int F = 1 << FB, C = 1 << CB, sub = FB - CB;
+    const int F = 1 << FB;
     if (stats) {
         stats->algorithm = PYG_JOIN_RADIX;
         stats->radix_bits = FB;
     }
     if (nR == 0 || nS == 0) return PYG_OK;
-    // The probe side of a two-pass join is laid out from a sample of about
-    // 2^24 tuples instead of a full histogram read.
-    const bool sample_s = two && nS >= ((int64_t)1 << 25);
-    const int64_t sstep = sample_s ? std::max<int64_t>(1, nS >> 24) : 1;
 
     RJEvents tm;
     tm.start(ctx, stats != nullptr);
-    const size_t side_words = RJSideDev::words(F, C);
-    unsigned long long* meta = nullptr;
     void *R1 = nullptr, *R2 = nullptr, *S1 = nullptr, *S2 = nullptr;
     RJItem* ditems = nullptr;
     int rc = PYG_OK;
     do {
-        if ((rc = dalloc(ctx, (void**)&meta, (2 * side_words + 2 * (size_t)F) * 8))) break;
-        RJSideDev dR, dS;
-        dR.carve(meta, F, C);
-        dS.carve(meta + side_words, F, C);
-        unsigned long long* histR = meta + 2 * side_words;
-        unsigned long long* histS = histR + F;
         unsigned* flags = (unsigned*)(ctx->dcounters + 202);  // [0] a bulk copy never landed, [1] region overflow
-        PYG_CUDA(cudaMemsetAsync(flags, 0, 8, ctx->stream));
         unsigned long long* h = (unsigned long long*)ctx->pinned;
-
-        // 1. Histograms: exact for the build side, sampled or exact for the
-        // probe side.
-        if ((rc = hist_launch(ctx, R, nR, 1, FB, histR))) break;
-        if ((rc = hist_launch(ctx, S, nS, sstep, FB, histS))) break;
-        std::vector<unsigned long long> hr(F), hs(F);
-        PYG_CUDA(cudaMemcpyAsync(hr.data(), histR, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        PYG_CUDA(cudaMemcpyAsync(hs.data(), histS, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        unsigned* hflags = (unsigned*)(h + 6);
+        // 1-2. Partition both sides (histograms sampled for large inputs).
         RJLayout LR, LS;
-        layout_exact(hr, C, sub, LR);
-        if (sample_s) layout_sampled(hs, sstep, C, sub, LS);
-        else layout_exact(hs, C, sub, LS);
-        if (LR.fstart[F] != (unsigned long long)nR || (!sample_s && LS.fstart[F] != (unsigned long long)nS)) {
-            set_error("pyg_hashjoin_agg: partition histogram does not add up");
-            rc = PYG_ERR_CUDA;
+        float rh_ms = 0.f, sh_ms = 0.f;
+        int64_t rh_n = 0, sh_n = 0;
+        if ((rc = rp_partition(ctx, R, nR, FB, two, true, nullptr, nullptr, LR, &R1, &R2, flags, hflags, &rh_ms,
+                               &rh_n)))
             break;
-        }
-        if ((rc = upload_layout(ctx, LR, dR, F, C, nR)) || (rc = upload_layout(ctx, LS, dS, F, C, nS))) break;
-        tm.mark(ctx, 1);
-
-        // 2. Partition passes.
-        if ((rc = dalloc(ctx, &R1, (size_t)LR.p1 * 16))) break;
-        if (two && (rc = dalloc(ctx, &R2, (size_t)LR.p2 * 16))) break;
-        if ((rc = run_passes(ctx, R, nR, LR, dR, two, FB, CB, R1, R2, flags, flags + 1))) break;
         tm.mark(ctx, 2);
-        for (int attempt = 0; attempt < 2; ++attempt) {
-            dfree(ctx, S1);
-            dfree(ctx, S2);
-            S1 = S2 = nullptr;
-            if ((rc = dalloc(ctx, &S1, (size_t)LS.p1 * 16))) break;
-            if (two && (rc = dalloc(ctx, &S2, (size_t)LS.p2 * 16))) break;
-            if ((rc = run_passes(ctx, S, nS, LS, dS, two, FB, CB, S1, S2, flags, flags + 1))) break;
-            if (!LS.sampled) break;
-            // Exact per-partition counts of the sampled layout (and whether
-            // any region overflowed).
-            LS.count.resize(F);
-            PYG_CUDA(cudaMemcpyAsync(LS.count.data(), dS.cur2, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
-            PYG_CUDA(cudaMemcpyAsync(h + 6, flags, 8, cudaMemcpyDeviceToHost, ctx->stream));
-            PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-            if (((unsigned*)(h + 6))[1] == 0) break;
-            // A region overflowed (the sample misjudged a partition): redo the
-            // probe side from an exact histogram.
-            if ((rc = hist_launch(ctx, S, nS, 1, FB, histS))) break;
-            PYG_CUDA(cudaMemcpyAsync(hs.data(), histS, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
-            PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-            layout_exact(hs, C, sub, LS);
-            if ((rc = upload_layout(ctx, LS, dS, F, C, nS))) break;
-            PYG_CUDA(cudaMemsetAsync(flags + 1, 0, 4, ctx->stream));
-        }
-        if (rc) break;
-        if (stats) stats->overflow_tuples = LS.sampled ? 0 : (sample_s ? 1 : 0);
+        if ((rc = rp_partition(ctx, S, nS, FB, two, true, nullptr, nullptr, LS, &S1, &S2, flags, hflags, &sh_ms,
+                               &sh_n)))
+            break;
         tm.mark(ctx, 3);
 
         // 3. Join: distinct build keys first (16-byte slots); on a repeated
@@ -386,8 +332,8 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
         unsigned long long* acc = ctx->dcounters + 8;
         unsigned* next = (unsigned*)(ctx->dcounters + 200);  // word 200: queue head, word 201: dup flag
         unsigned* dupf = (unsigned*)(ctx->dcounters + 201);
-        std::vector<unsigned long long> rstart(LR.fstart.begin(), LR.fstart.end() - 1);
-        std::vector<unsigned long long> sstart(LS.fstart.begin(), LS.fstart.end() - 1);
+        std::vector<unsigned long long> rstart(LR.fstart.begin(), LR.fstart.begin() + F);
+        std::vector<unsigned long long> sstart(LS.fstart.begin(), LS.fstart.begin() + F);
         std::vector<RJItem> items;
         for (int pass = 0; pass < 2; ++pass) {
             const bool unique = pass == 0;
@@ -417,18 +363,7 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
             PYG_LAUNCHED(ctx);
             PYG_CUDA(cudaMemcpyAsync(h, acc, 3 * 8, cudaMemcpyDeviceToHost, ctx->stream));
             PYG_CUDA(cudaMemcpyAsync(h + 3, next, 16, cudaMemcpyDeviceToHost, ctx->stream));
-            PYG_CUDA(cudaMemcpyAsync(h + 6, flags, 8, cudaMemcpyDeviceToHost, ctx->stream));
             PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-            if (((unsigned*)(h + 6))[0]) {
-                set_error("pyg_hashjoin_agg: a partition tile copy did not complete in time");
-                rc = PYG_ERR_TIMEOUT;
-                break;
-            }
-            if (((unsigned*)(h + 6))[1]) {
-                set_error("pyg_hashjoin_agg: a partition outgrew its exact region");
-                rc = PYG_ERR_CUDA;
-                break;
-            }
             out[0] = h[0];
             out[1] = h[1];
             out[2] = h[2];
@@ -438,13 +373,17 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
         tm.mark(ctx, 4);
         if (stats) {
             cudaEventSynchronize(tm.ev[4]);
-            stats->histogram_ms = tm.ms(0, 1);
-            stats->build_partition_ms = tm.ms(1, 2);
+            // Partition phases include their histograms; histogram_ms
+            // reports the histograms' own time.
+            stats->histogram_ms = rh_ms + sh_ms;
+            stats->histogram_tuples = rh_n + sh_n;
+            stats->build_partition_ms = tm.ms(0, 2);
             stats->build_ms = 0;
             stats->probe_partition_ms = tm.ms(2, 3);
             stats->probe_ms = tm.ms(3, 4);
-            stats->padded_tuples = (int64_t)(LS.p2 - (unsigned long long)nS);
-            stats->histogram_tuples = nR + (nS + sstep - 1) / sstep;
+            stats->padded_tuples = (int64_t)((LR.p2 + LS.p2) - (unsigned long long)(nR + nS));
+            stats->overflow_tuples = (LR.sampled || nR < ((int64_t)1 << 25) || !two ? 0 : 1) +
+                                     (LS.sampled || nS < ((int64_t)1 << 25) || !two ? 0 : 1);
         }
     } while (0);
     dfree(ctx, ditems);
@@ -452,7 +391,6 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
     dfree(ctx, R2);
     dfree(ctx, S1);
     dfree(ctx, S2);
-    dfree(ctx, meta);
     return rc;
 }
 

@@ -33,30 +33,35 @@ __device__ __forceinline__ unsigned rj_bin(uint64_t h, int shift, unsigned mask)
 // counters per CTA).
 
 __global__ void __launch_bounds__(1024) rj_hist_kernel(const longlong2* __restrict__ in, int64_t n, int64_t step,
-                                                       int bits, unsigned long long* __restrict__ hist)
+                                                       int bits, int base, int span,
+                                                       unsigned long long* __restrict__ hist)
 {
-    // Counts in[0], in[step], in[2 step], ... (step 1: every tuple).
+    // Counts the bins [base, base + span) of in[0], in[step], in[2 step],
+    // ... (step 1: every tuple); span 32-bit counters in shared memory.
     extern __shared__ unsigned rj_sh_hist[];
     const int P = 1 << bits;
     const int shift = 64 - bits;
     const int64_t m = (n + step - 1) / step;
-    for (int b = threadIdx.x; b < P; b += blockDim.x) rj_sh_hist[b] = 0;
+    for (int b = threadIdx.x; b < span; b += blockDim.x) rj_sh_hist[b] = 0;
     __syncthreads();
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    auto count = [&](long long k) {
+        const unsigned r = rj_bin(mix64((uint64_t)k), shift, P - 1) - (unsigned)base;
+        if (r < (unsigned)span) atomicAdd(&rj_sh_hist[r], 1u);
+    };
     constexpr int U = 8;
     for (; i + (U - 1) * stride < m; i += U * stride) {
         longlong2 t[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) t[u] = __ldcs(&in[(i + u * stride) * step]);
 #pragma unroll
-        for (int u = 0; u < U; ++u) atomicAdd(&rj_sh_hist[rj_bin(mix64((uint64_t)t[u].x), shift, P - 1)], 1u);
+        for (int u = 0; u < U; ++u) count(t[u].x);
     }
-    for (; i < m; i += stride)
-        atomicAdd(&rj_sh_hist[rj_bin(mix64((uint64_t)__ldcs(&in[i * step]).x), shift, P - 1)], 1u);
+    for (; i < m; i += stride) count(__ldcs(&in[i * step]).x);
     __syncthreads();
-    for (int b = threadIdx.x; b < P; b += blockDim.x)
-        if (rj_sh_hist[b]) atomicAdd(&hist[b], (unsigned long long)rj_sh_hist[b]);
+    for (int b = threadIdx.x; b < span; b += blockDim.x)
+        if (rj_sh_hist[b]) atomicAdd(&hist[base + b], (unsigned long long)rj_sh_hist[b]);
 }
 
 // Tiles per segment, as an exclusive prefix (one thread; at most 2^8
@@ -471,7 +476,9 @@ int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, 
 
 int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int FB, unsigned long long* hist)
 {
-    const size_t hsm = (size_t)4 << FB;
+    // At most 2^15 counters (128 KB) per launch: 2^16 bins take two.
+    const int F = 1 << FB, span = F < (1 << 15) ? F : (1 << 15);
+    const size_t hsm = (size_t)4 * span;
     PYG_CUDA(cudaFuncSetAttribute(rj_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
     int per = 0;
     PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rj_hist_kernel, 1024, hsm));
@@ -479,9 +486,11 @@ int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int 
     const int64_t m = (n + step - 1) / step;
     const int64_t want = (m + 1024 * 8 - 1) / (1024 * 8);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->sm_count * per));
-    PYG_CUDA(cudaMemsetAsync(hist, 0, (size_t)8 << FB, ctx->stream));
-    rj_hist_kernel<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, FB, hist);
-    PYG_LAUNCHED(ctx);
+    PYG_CUDA(cudaMemsetAsync(hist, 0, (size_t)8 * F, ctx->stream));
+    for (int base = 0; base < F; base += span) {
+        rj_hist_kernel<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, FB, base, span, hist);
+        PYG_LAUNCHED(ctx);
+    }
     return PYG_OK;
 }
 
@@ -505,7 +514,7 @@ int hist_launch_range(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step
 
 int rp_partition(pyg_ctx* ctx, const longlong2* in, int64_t n, int FB, bool two, bool allow_sample,
                  const long long* csplit, const long long* fsplit, RJLayout& L, void** P1, void** P2,
-                 unsigned* flags, unsigned* hflags)
+                 unsigned* flags, unsigned* hflags, float* hist_ms, int64_t* hist_tuples)
 {
     const int CB = two ? (FB + 1) / 2 : FB;
     const int F = 1 << FB, C = 1 << CB, sub = FB - CB;
@@ -525,10 +534,23 @@ int rp_partition(pyg_ctx* ctx, const longlong2* in, int64_t n, int FB, bool two,
         d.carve(meta, F, C);
         unsigned long long* hist = meta + side;
         PYG_CUDA(cudaMemsetAsync(flags, 0, 8, ctx->stream));
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (hist_ms) {
+            cudaEventCreate(&e0);
+            cudaEventCreate(&e1);
+            cudaEventRecord(e0, ctx->stream);
+        }
         if ((rc = hist_of(step, hist))) break;
+        if (hist_ms) cudaEventRecord(e1, ctx->stream);
+        if (hist_tuples) *hist_tuples = (n + step - 1) / step;
         std::vector<unsigned long long> h(F);
         PYG_CUDA(cudaMemcpyAsync(h.data(), hist, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
         PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (hist_ms) {
+            cudaEventElapsedTime(hist_ms, e0, e1);
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+        }
         if (sample) layout_sampled(h, step, C, sub, L);
         else layout_exact(h, C, sub, L);
         for (int attempt = 0; attempt < 2; ++attempt) {

@@ -33,9 +33,10 @@ constexpr int RJ_PT_THREADS = PYG_RJ_PT_THREADS;  // partition CTA
 constexpr int RJ_MAX_LOCAL_BITS = 9;     // bins of one partition pass
 constexpr int RJ_LMAX = 1 << RJ_MAX_LOCAL_BITS;
 constexpr int RJ_SPLIT_MAX = 256;        // range mode: splitters per pass segment (<= 2^8 bins)
-// Largest fine partition count (log2): the histogram kernel keeps 2^bits
-// 32-bit counters in shared memory.
-constexpr int RJ_MAX_FINE_BITS = 15;
+// Largest fine partition counts (log2); the histogram kernels keep up to
+// 2^15 32-bit counters in shared memory.
+constexpr int RJ_MAX_FINE_BITS = 16;   // hash mode (histograms run in halves above 2^15 bins)
+constexpr int RJ_MAX_RANGE_BITS = 15;  // range mode (one 2^15-counter histogram)
 
 // Host-side layout of one relation's partitions.
 struct RJLayout {
@@ -97,10 +98,11 @@ int hist_launch_range(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step
 // overflowed.  On success the partitions are in (two ? *P2 : *P1) at
 // L.fstart with L.count tuples each; the caller frees *P1 and *P2.  flags:
 // two device words (bulk copy never landed, region overflow); hflags: two
-// pinned host words.
+// pinned host words.  hist_ms / hist_tuples (optional): the histogram's
+// time and the tuples it read.
 int rp_partition(pyg_ctx* ctx, const longlong2* in, int64_t n, int FB, bool two, bool allow_sample,
                  const long long* csplit, const long long* fsplit, RJLayout& L, void** P1, void** P2,
-                 unsigned* flags, unsigned* hflags);
+                 unsigned* flags, unsigned* hflags, float* hist_ms = nullptr, int64_t* hist_tuples = nullptr);
 
 // Slot of a key in a shared-memory table of TS slots: multiply-high of the
 // 32 hash bits below the fine partition bits (all keys of one partition
