@@ -26,7 +26,7 @@
 
 namespace pyg {
 
-constexpr int MP16_THREADS = 1024;
+constexpr int MP16_THREADS = 512;          // two CTAs per SM: one sorts while the other merges
 constexpr int MP16_RCHUNK = 4096;         // build tuples sorted per work item
 constexpr int64_t MP16_SCHUNK = 1 << 16;  // probe tuples per work item
 constexpr int MP16_SMEM = MP16_RCHUNK * 8 * 2 + (MP16_RCHUNK + 1) * 8;
@@ -46,7 +46,7 @@ struct Mp16Args {
     unsigned long long* acc;  // count, build sum, probe sum
 };
 
-__global__ void __launch_bounds__(MP16_THREADS, 1) mp16_join_kernel(Mp16Args a)
+__global__ void __launch_bounds__(MP16_THREADS, 2) mp16_join_kernel(Mp16Args a)
 {
     extern __shared__ __align__(16) unsigned char mp16_smem[];
     long long* keys = (long long*)mp16_smem;
@@ -87,9 +87,17 @@ __global__ void __launch_bounds__(MP16_THREADS, 1) mp16_join_kernel(Mp16Args a)
             pays[i] = p;
         }
         __syncthreads();
-        // Bitonic sort of (key, payload) by key, ascending.
+        // Bitonic sort of (key, payload) by key, ascending.  At stride
+        // j <= 32 every compare-exchange a warp does stays inside that
+        // warp's own 64-element blocks, so those stages need only a warp
+        // barrier; a CTA barrier precedes every stage that follows or uses
+        // a longer stride.
+        bool wide = true;
         for (int kk = 2; kk <= N; kk <<= 1) {
             for (int j = kk >> 1; j > 0; j >>= 1) {
+                if (wide || j >= 64) __syncthreads();
+                else __syncwarp();
+                wide = j >= 64;
                 for (int i = tid; i < N / 2; i += MP16_THREADS) {
                     const int lo = 2 * i - (i & (j - 1));
                     const int hi = lo + j;
@@ -103,9 +111,9 @@ __global__ void __launch_bounds__(MP16_THREADS, 1) mp16_join_kernel(Mp16Args a)
                         pays[hi] = p0;
                     }
                 }
-                __syncthreads();
             }
         }
+        __syncthreads();
         // Exclusive prefix sum of the sorted payloads: thread t owns a
         // contiguous run of N / MP16_THREADS (or one) entries.
         const int per = N >= MP16_THREADS ? N / MP16_THREADS : 1;
@@ -264,7 +272,7 @@ int mpsm16_agg(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t
             ja.next = next;
             ja.acc = acc;
             PYG_CUDA(cudaFuncSetAttribute(mp16_join_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MP16_SMEM));
-            const unsigned grid = (unsigned)std::min<long long>((long long)ctx->sm_count, ja.nitems);
+            const unsigned grid = (unsigned)std::min<long long>(2LL * ctx->sm_count, ja.nitems);
             mp16_join_kernel<<<grid, MP16_THREADS, MP16_SMEM, ctx->stream>>>(ja);
             PYG_LAUNCHED(ctx);
         }
