@@ -21,6 +21,7 @@ namespace pyg {
 #endif
 constexpr int RJ_STAGES = PYG_RJ_STAGES;                               // input tiles in flight per partition CTA
 constexpr unsigned long long kBulkWaitNs = 2000000000ULL;  // 2 s
+constexpr unsigned long long kSkipRun = 1ULL << 63;          // gdelta of a run that is not written
 
 __device__ __forceinline__ unsigned rj_bin(uint64_t h, int shift, unsigned mask)
 {
@@ -142,7 +143,7 @@ struct RJPartSmem {
     unsigned short stage_bin[RJ_TILE];
     unsigned hist[RJ_LMAX];
     unsigned loff[RJ_LMAX];
-    unsigned long long gbase[RJ_LMAX];
+    unsigned long long gdelta[RJ_LMAX];  // output position of staged slot i = gdelta[bin] + i
     uint64_t bar[RJ_STAGES];
     RJTileRange info[RJ_STAGES];
     unsigned warp_tot[RJ_PT_THREADS / 32];
@@ -271,11 +272,17 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
         }
         if (lane == 31) sm.warp_tot[w] = incl;
         __syncthreads();  // B
-        unsigned excl = incl - c, total = 0;
-        for (int v = 0; v < RJ_PT_THREADS / 32; ++v) {
-            if (v == w) excl += total;
-            total += sm.warp_tot[v];
+        // Prefix over the warp totals, by one more shuffle scan per warp.
+        constexpr int NW = RJ_PT_THREADS / 32;
+        const unsigned wt = lane < NW ? sm.warp_tot[lane] : 0u;
+        unsigned wincl = wt;
+#pragma unroll
+        for (int o = 1; o < NW; o <<= 1) {
+            const unsigned v = __shfl_up_sync(0xffffffffu, wincl, o);
+            if (lane >= o) wincl += v;
         }
+        const unsigned excl = incl - c + __shfl_sync(0xffffffffu, wincl - wt, w);
+        const unsigned total = __shfl_sync(0xffffffffu, wincl, NW - 1);
         // The reservation's result (a global atomic, about a microsecond
         // away) is first needed after the tile is staged.
         unsigned long long resv = 0, bstart = 0, bcap = ~0ULL;
@@ -302,13 +309,14 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
         // (its copy was issued a tile ago, so its segment is known).
         if (a.nsplit && a.nseg > 1 && tile + gridDim.x < ntiles)
             rj_load_split(a, sm.split[(k + 1) & 1], sm.info[(k + 1) % RJ_STAGES].seg);
+        // Per bin, the output position of staged slot i is gdelta + i.
         if (tid < L && c) {
-            unsigned long long gb = bstart + resv;
+            unsigned long long gd = bstart + resv - excl;
             if (resv + c > bcap) {  // outgrew its region: not written; the host redoes the pass exactly
                 atomicOr(a.ovf, 1u);
-                gb = ~0ULL;
+                gd = kSkipRun;
             }
-            sm.gbase[tid] = gb;
+            sm.gdelta[tid] = gd;
         }
         __syncthreads();  // D: ring slot consumed, stage and global offsets complete
         if (tid == 0) {
@@ -320,9 +328,8 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
         }
         // (4) Write each bin's run contiguously.
         for (unsigned i = tid; i < total; i += RJ_PT_THREADS) {
-            const unsigned b = sm.stage_bin[i];
-            const unsigned long long gb = sm.gbase[b];
-            if (gb != ~0ULL) __stcs(&a.out[gb + (i - sm.loff[b])], sm.stage[i]);
+            const unsigned long long gd = sm.gdelta[sm.stage_bin[i]];
+            if (gd != kSkipRun) __stcs(&a.out[gd + i], sm.stage[i]);
         }
     }
     __syncthreads();
