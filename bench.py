@@ -392,9 +392,10 @@ def run_e2e(args, torch, pyg, ctx, R, S, nR, nS, world, dist):
         avail = psutil.virtual_memory().available
     except Exception:
         avail = 0
-    need = (nR + nS) * 16
+    # Every rank on this node pins its own copy of the inputs.
+    need = (nR + nS) * 16 * world
     if avail and avail < 3 * need:
-        return {"value": None, "unit": UNIT, "skipped": f"host RAM {avail >> 30} GiB < 3x inputs"}
+        return {"value": None, "unit": UNIT, "skipped": f"host RAM {avail >> 30} GiB < 3x the ranks' inputs"}
     hR = pyg.HostBuf(nR * 16)
     hS = pyg.HostBuf(nS * 16)
     try:
