@@ -392,10 +392,16 @@ def run_e2e(args, torch, pyg, ctx, R, S, nR, nS, world, dist):
         avail = psutil.virtual_memory().available
     except Exception:
         avail = 0
-    # Every rank on this node pins its own copy of the inputs.
+    # Every rank on this node pins its own copy of the inputs; all ranks
+    # take the same decision (they share the collectives below).
     need = (nR + nS) * 16 * world
-    if avail and avail < 3 * need:
-        return {"value": None, "unit": UNIT, "skipped": f"host RAM {avail >> 30} GiB < 3x the ranks' inputs"}
+    ok = not (avail and avail < 3 * need)
+    if dist:
+        t = torch.tensor([1 if ok else 0], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        ok = bool(t.item())
+    if not ok:
+        return {"value": None, "unit": UNIT, "skipped": "host RAM below 3x the inputs of the node's ranks"}
     hR = pyg.HostBuf(nR * 16)
     hS = pyg.HostBuf(nS * 16)
     try:
