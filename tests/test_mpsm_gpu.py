@@ -48,6 +48,27 @@ def test_mpsm_agg_vs_oracle(ctx, torch_cuda, fan, kind):
     assert st.max_partition_imbalance >= 1.0 or m == 0
 
 
+@pytest.mark.parametrize("kind", KINDS)
+def test_mpsm_agg_two_passes_and_chunked_ranges(ctx, torch_cuda, kind):
+    """The aggregate sink on 16-byte device tuples: two range-partition
+    passes (2^22 probe tuples), one build key repeated 20000 times (its range
+    spans several sorted build chunks), INT64_MAX keys on both sides."""
+    mx = np.iinfo(np.int64).max
+    rng = np.random.default_rng(40 + kind)
+    n, m = 1 << 18, 1 << 22
+    rk = rng.integers(-(1 << 40), 1 << 40, n)
+    rk[:20000] = 12345
+    rk[20000:20003] = mx
+    R = struct([rk, rng.integers(-(1 << 50), 1 << 50, n)], [I64, I64])
+    sk = rk[rng.integers(0, n, m)]
+    sk[::101] = rng.integers(-(1 << 40), 1 << 40, sk[::101].shape[0])  # mostly misses
+    S = struct([sk, rng.integers(-(1 << 50), 1 << 50, m)], [I64, I64])
+    proj = [(0, 1), (1, 1)]
+    cnt, sums, _ = ctx.mpsm_join_agg(dev_rel(torch_cuda, R, [I64, I64]), 0, dev_rel(torch_cuda, S, [I64, I64]), 0,
+                                     proj, ctx.mpsm_opts(kind, 4096, 0.01, 256))
+    assert (cnt, sums) == O.mpsm_join(R, [I64, I64], 0, S, [I64, I64], 0, proj)
+
+
 def test_mpsm_materialize_duplicates_int32_and_host(ctx, torch_cuda):
     rng = np.random.default_rng(6)
     R = struct([rng.integers(-30, 30, 3000).astype(np.int32), np.arange(3000, dtype=np.int64)], [I32, I64])
