@@ -83,6 +83,15 @@ struct RJJoinArgs {
     unsigned* dup;              // set when a build key repeats (UNIQUE)
 };
 
+// Slot of key k in a table of TS slots: multiply-high of the top 32 bits of
+// a multiplicative (Fibonacci) hash.  Partition membership comes from
+// mix64, so within one partition these bits are as good as random, for one
+// multiply instead of the full mix.
+__device__ __forceinline__ unsigned rj_join_slot(uint64_t k, unsigned TS)
+{
+    return __umulhi((unsigned)((k * 0x9E3779B97F4A7C15ULL) >> 32), TS);
+}
+
 // Warms L2 with [p, p + bytes) (16-byte aligned start; bytes rounded down
 // to a multiple of 16); no registers are held for it.
 __device__ __forceinline__ void rj_prefetch_l2(const void* p, unsigned long long bytes)
@@ -106,7 +115,6 @@ __global__ void __launch_bounds__(RJ_JOIN_THREADS, RJ_JOIN_BLOCKS) rj_join_kerne
     ulonglong4* T4 = reinterpret_cast<ulonglong4*>(rj_table);  // counted slots
     uint64_t cnt = 0, bsum = 0, psum = 0;
     bool dup = false;
-    const int fb = a.fine_bits;
     // One item of look-ahead: while this CTA works on an item, the next
     // one is already claimed and its build partition (and the head of its
     // probe chunk) is being pulled into L2.
@@ -143,7 +151,7 @@ __global__ void __launch_bounds__(RJ_JOIN_THREADS, RJ_JOIN_BLOCKS) rj_join_kerne
                 atomicAdd(&side_sum, (unsigned long long)t.y);
                 continue;
             }
-            unsigned pos = rj_slot(mix64(k), fb, TS);
+            unsigned pos = rj_join_slot(k, TS);
             for (unsigned steps = 0; steps < TS; ++steps) {
                 unsigned long long* key = UNIQUE ? &T2[pos].x : &T4[pos].x;
                 const unsigned long long prev = atomicCAS(key, kEmptyKey, k);
@@ -173,7 +181,7 @@ __global__ void __launch_bounds__(RJ_JOIN_THREADS, RJ_JOIN_BLOCKS) rj_join_kerne
                 psum += scnt * (uint64_t)t.y;
                 return;
             }
-            unsigned pos = rj_slot(mix64(k), fb, TS);
+            unsigned pos = rj_join_slot(k, TS);
             for (unsigned steps = 0; steps < TS; ++steps) {
                 if constexpr (UNIQUE) {
                     const ulonglong2 e = T2[pos];
