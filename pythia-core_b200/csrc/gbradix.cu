@@ -74,6 +74,14 @@ __device__ __forceinline__ bool gbr_global_add(const GbrArgs& a, uint64_t k, uin
     return false;
 }
 
+// Slot of key k in a shared table of TS slots: multiply-high of the top 32
+// bits of a multiplicative (Fibonacci) hash.  Partitions come from mix64,
+// so within one partition these bits are as good as random.
+__device__ __forceinline__ unsigned gbr_slot(uint64_t k, unsigned TS)
+{
+    return __umulhi((unsigned)((k * 0x9E3779B97F4A7C15ULL) >> 32), TS);
+}
+
 struct GbrTable {
     unsigned long long* key;
     unsigned long long* sum;
@@ -81,9 +89,9 @@ struct GbrTable {
 };
 
 // Folds one tuple into the shared table; false if the table is full.
-__device__ __forceinline__ bool gbr_fold(const GbrTable& t, uint64_t k, uint64_t v, int fb, int want_sum)
+__device__ __forceinline__ bool gbr_fold(const GbrTable& t, uint64_t k, uint64_t v, int want_sum)
 {
-    unsigned pos = fb ? rj_slot(mix64(k), fb, GBR_SLOTS) : __umulhi((unsigned)(mix64(k) >> 32), GBR_SLOTS);
+    unsigned pos = gbr_slot(k, GBR_SLOTS);
     for (unsigned steps = 0; steps < GBR_SLOTS; ++steps) {
         unsigned long long prev = t.key[pos];
         if (prev == kEmptyKey) prev = atomicCAS(&t.key[pos], kEmptyKey, (unsigned long long)k);
@@ -104,7 +112,6 @@ __device__ void gbr_fold_range(const GbrArgs& a, const GbrTable& t, const longlo
 {
     constexpr int U = COMBINE ? 4 : 8;
     const int lane = threadIdx.x & 31;
-    const int fb = a.fine_bits;
     // With COMBINE, lanes holding the same key as a leader lane (the lowest
     // unplaced lane) are combined with one shuffle reduction and folded
     // once, for up to two leaders per warp: hot keys (skew, very few groups)
@@ -128,7 +135,7 @@ __device__ void gbr_fold_range(const GbrArgs& a, const GbrTable& t, const longlo
 #pragma unroll
             for (int o = 16; o; o >>= 1) sv += __shfl_xor_sync(0xffffffffu, sv, o);
             if (lane == leader) {
-                unsigned pos = fb ? rj_slot(mix64(kl), fb, GBR_SLOTS) : __umulhi((unsigned)(mix64(kl) >> 32), GBR_SLOTS);
+                unsigned pos = gbr_slot(kl, GBR_SLOTS);
                 bool done = false;
                 for (unsigned steps = 0; steps < GBR_SLOTS && !done; ++steps) {
                     unsigned long long prev = t.key[pos];
@@ -145,7 +152,7 @@ __device__ void gbr_fold_range(const GbrArgs& a, const GbrTable& t, const longlo
             rem &= ~m;
         }
         if ((rem >> lane) & 1) {
-            if (!gbr_fold(t, k, v, fb, a.want_sum) && !gbr_global_add(a, k, v, 1, fresh)) full = true;
+            if (!gbr_fold(t, k, v, a.want_sum) && !gbr_global_add(a, k, v, 1, fresh)) full = true;
         }
     };
     // Loop bounds are uniform across each warp (the whole-warp test in
@@ -249,7 +256,7 @@ __global__ void __launch_bounds__(GBR_THREADS, 1) gbr_tiny_kernel(GbrArgs a)
     // lane adds its tuple with shared atomics, but only into its own warp's
     // table, so atomics of different warps never meet.
     auto add = [&](uint64_t k, uint64_t s, unsigned c) {
-        unsigned pos = (unsigned)(mix64(k) >> 57);  // 128 slots
+        unsigned pos = gbr_slot(k, GBR_TINY_SLOTS);
         for (int steps = 0; steps < GBR_TINY_SLOTS; ++steps) {
             unsigned long long prev = keys[pos];
             if (prev == kEmptyKey) prev = atomicCAS(&keys[pos], kEmptyKey, (unsigned long long)k);
