@@ -257,7 +257,20 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
                 bin[j] = a.nsplit ? rj_range_bin(sm.split[a.nseg > 1 ? (k & 1) : 0], a.nsplit, t[j].x)
                                   : rj_bin(mix64((uint64_t)t[j].x), a.shift, a.mask);
             }
-            if (valid) rank[j] = atomicAdd(&sm.hist[bin[j]], 1u);
+            // Skewed keys put many lanes of a warp into one bin: when at
+            // least 8 lanes share lane 0's bin, they take their ranks from
+            // one atomic (lane order), the others one atomic each.
+            const unsigned b0 = __shfl_sync(0xffffffffu, bin[j], 0);
+            const unsigned m0 = __ballot_sync(0xffffffffu, valid && bin[j] == b0);
+            if (__popc(m0) >= 8) {
+                unsigned base = 0;
+                if (lane == 0) base = atomicAdd(&sm.hist[b0], (unsigned)__popc(m0));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if ((m0 >> lane) & 1) rank[j] = base + __popc(m0 & ((1u << lane) - 1u));
+                else if (valid) rank[j] = atomicAdd(&sm.hist[bin[j]], 1u);
+            } else if (valid) {
+                rank[j] = atomicAdd(&sm.hist[bin[j]], 1u);
+            }
         }
         __syncthreads();  // A: histogram complete
         if (!sm.ok) break;
