@@ -106,16 +106,24 @@ __device__ __forceinline__ bool gbr_fold(const GbrTable& t, uint64_t k, uint64_t
 }
 
 // Folds tuples [0, n) of p into the shared table.
-template <bool COMBINE>
+// Lane combining in gbr_fold_range: never, always, or adaptive (a warp
+// stops combining after four batches in a row whose rounds found no key
+// group of three or more lanes, and tries again 64 batches later).
+enum GbrFold { kFoldPlain = 0, kFoldCombine = 1, kFoldAdaptive = 2 };
+
+template <int MODE>
 __device__ void gbr_fold_range(const GbrArgs& a, const GbrTable& t, const longlong2* __restrict__ p, int64_t n,
                                uint64_t& sent_sum, uint64_t& sent_cnt, unsigned long long& fresh, bool& full)
 {
-    constexpr int U = COMBINE ? 4 : 8;
+    constexpr int U = MODE == kFoldPlain ? 8 : 4;
     const int lane = threadIdx.x & 31;
-    // With COMBINE, lanes holding the same key as a leader lane (the lowest
-    // unplaced lane) are combined with one shuffle reduction and folded
-    // once, for up to two leaders per warp: hot keys (skew, very few groups)
-    // cost one shared atomic per warp instead of one per lane.
+    bool comb = MODE != kFoldPlain, hit = false;
+    int cool = 0, miss = 0;
+    // While combining, the lanes holding the key of a leader lane are combined
+    // with one shuffle reduction and folded once, for up to two leaders per
+    // warp; each round takes the larger key group of two candidates (the
+    // lowest and the highest unplaced lanes).  Hot keys (skew, very few
+    // groups) cost one shared atomic per warp instead of one per lane.
     auto one = [&](const longlong2 x, bool valid) {
         const uint64_t k = (uint64_t)x.x, v = (uint64_t)x.y;
         if (valid && k == kEmptyKey) {
@@ -124,13 +132,21 @@ __device__ void gbr_fold_range(const GbrArgs& a, const GbrTable& t, const longlo
         }
         unsigned rem = __ballot_sync(0xffffffffu, valid && k != kEmptyKey);
 #pragma unroll
-        for (int r = 0; r < (COMBINE ? 2 : 0); ++r) {
-            if (!rem) break;
-            const int leader = __ffs(rem) - 1;
-            const uint64_t kl = __shfl_sync(0xffffffffu, k, leader);
-            const unsigned m = __ballot_sync(0xffffffffu, ((rem >> lane) & 1) && k == kl);
+        for (int r = 0; r < (MODE != kFoldPlain ? 2 : 0); ++r) {
+            if (!comb || !rem) break;
+            // Two candidate leaders, the lowest and the highest unplaced
+            // lanes; the larger of their key groups is combined.
+            const int la = __ffs(rem) - 1, lb = 31 - __clz(rem);
+            const uint64_t ka = __shfl_sync(0xffffffffu, k, la), kb = __shfl_sync(0xffffffffu, k, lb);
+            const unsigned ma = __ballot_sync(0xffffffffu, ((rem >> lane) & 1) && k == ka);
+            const unsigned mb = __ballot_sync(0xffffffffu, ((rem >> lane) & 1) && k == kb);
+            const bool pa = __popc(ma) >= __popc(mb);
+            const unsigned m = pa ? ma : mb;
+            const int leader = pa ? la : lb;
+            const uint64_t kl = pa ? ka : kb;
             const int c = __popc(m);
             if (c < 3) break;
+            hit = true;
             uint64_t sv = ((m >> lane) & 1) ? v : 0;
 #pragma unroll
             for (int o = 16; o; o >>= 1) sv += __shfl_xor_sync(0xffffffffu, sv, o);
@@ -164,6 +180,19 @@ __device__ void gbr_fold_range(const GbrArgs& a, const GbrTable& t, const longlo
         for (int u = 0; u < U; ++u) x[u] = __ldcs(&p[wb + lane + (int64_t)u * GBR_THREADS]);
 #pragma unroll
         for (int u = 0; u < U; ++u) one(x[u], true);
+        if (MODE == kFoldAdaptive) {
+            if (comb) {
+                miss = hit ? 0 : miss + 1;
+                hit = false;
+                if (miss == 4) {
+                    comb = false;
+                    miss = 0;
+                    cool = 64;
+                }
+            } else if (--cool == 0) {
+                comb = true;
+            }
+        }
     }
     for (; wb < n; wb += GBR_THREADS) {
         const int64_t j = wb + lane;
@@ -206,7 +235,7 @@ __device__ void gbr_finish(const GbrArgs& a, uint64_t sent_sum, uint64_t sent_cn
 }
 
 // Few groups: CTA b folds the b-th slice of the input, then flushes once.
-template <bool COMBINE>
+template <int MODE>
 __global__ void __launch_bounds__(GBR_THREADS, 1) gbr_direct_kernel(GbrArgs a)
 {
     extern __shared__ __align__(16) unsigned char gbr_smem[];
@@ -220,7 +249,7 @@ __global__ void __launch_bounds__(GBR_THREADS, 1) gbr_direct_kernel(GbrArgs a)
     const int64_t per = (a.n + gridDim.x - 1) / gridDim.x;
     const int64_t b0 = (int64_t)blockIdx.x * per;
     const int64_t b1 = min(a.n, b0 + per);
-    if (b0 < b1) gbr_fold_range<COMBINE>(a, t, a.in + b0, b1 - b0, sent_sum, sent_cnt, fresh, full);
+    if (b0 < b1) gbr_fold_range<MODE>(a, t, a.in + b0, b1 - b0, sent_sum, sent_cnt, fresh, full);
     __syncthreads();
     gbr_flush(a, t, fresh, full);
     gbr_finish(a, sent_sum, sent_cnt, fresh, full);
@@ -331,8 +360,10 @@ __global__ void __launch_bounds__(GBR_THREADS, 1) gbr_part_kernel(GbrArgs a)
         __syncthreads();
         const long long it = item;
         if (it >= a.nitems) break;
-        // Partitions are where skew concentrates: always combine.
-        gbr_fold_range<true>(a, t, a.in + a.item_start[it], (int64_t)a.item_len[it], sent_sum, sent_cnt, fresh, full);
+        // Skew concentrates in partitions: warps combine lanes wherever they
+        // find repeated keys.
+        gbr_fold_range<kFoldAdaptive>(a, t, a.in + a.item_start[it], (int64_t)a.item_len[it], sent_sum, sent_cnt, fresh,
+                                      full);
         __syncthreads();
         gbr_flush(a, t, fresh, full);
         __syncthreads();
@@ -365,12 +396,12 @@ int groupby16_fill(pyg_ctx* ctx, const void* in, int64_t n, int want_sum, int64_
             return PYG_OK;
         }
         const bool combine = expected_groups <= GBR_COMBINE_GROUPS;
-        void* fn = combine ? (void*)gbr_direct_kernel<true> : (void*)gbr_direct_kernel<false>;
+        void* fn = combine ? (void*)gbr_direct_kernel<kFoldCombine> : (void*)gbr_direct_kernel<kFoldPlain>;
         PYG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, GBR_SMEM));
         const int64_t want = (n + 64 * GBR_THREADS - 1) / (64 * GBR_THREADS);
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, ctx->sm_count));
-        if (combine) gbr_direct_kernel<true><<<grid, GBR_THREADS, GBR_SMEM, ctx->stream>>>(a);
-        else gbr_direct_kernel<false><<<grid, GBR_THREADS, GBR_SMEM, ctx->stream>>>(a);
+        if (combine) gbr_direct_kernel<kFoldCombine><<<grid, GBR_THREADS, GBR_SMEM, ctx->stream>>>(a);
+        else gbr_direct_kernel<kFoldPlain><<<grid, GBR_THREADS, GBR_SMEM, ctx->stream>>>(a);
         PYG_LAUNCHED(ctx);
         return PYG_OK;
     }
