@@ -74,14 +74,6 @@ __device__ __forceinline__ bool gbr_global_add(const GbrArgs& a, uint64_t k, uin
     return false;
 }
 
-// Slot of key k in a shared table of TS slots: multiply-high of the top 32
-// bits of a multiplicative (Fibonacci) hash.  Partitions come from mix64,
-// so within one partition these bits are as good as random.
-__device__ __forceinline__ unsigned gbr_slot(uint64_t k, unsigned TS)
-{
-    return __umulhi((unsigned)((k * 0x9E3779B97F4A7C15ULL) >> 32), TS);
-}
-
 struct GbrTable {
     unsigned long long* key;
     unsigned long long* sum;
@@ -89,9 +81,9 @@ struct GbrTable {
 };
 
 // Folds one tuple into the shared table; false if the table is full.
-__device__ __forceinline__ bool gbr_fold(const GbrTable& t, uint64_t k, uint64_t v, int want_sum)
+__device__ __forceinline__ bool gbr_fold(const GbrTable& t, uint64_t k, uint64_t v, int want_sum, int fb)
 {
-    unsigned pos = gbr_slot(k, GBR_SLOTS);
+    unsigned pos = rj_slot(k, fb, GBR_SLOTS);
     for (unsigned steps = 0; steps < GBR_SLOTS; ++steps) {
         unsigned long long prev = t.key[pos];
         if (prev == kEmptyKey) prev = atomicCAS(&t.key[pos], kEmptyKey, (unsigned long long)k);
@@ -151,7 +143,7 @@ __device__ void gbr_fold_range(const GbrArgs& a, const GbrTable& t, const longlo
 #pragma unroll
             for (int o = 16; o; o >>= 1) sv += __shfl_xor_sync(0xffffffffu, sv, o);
             if (lane == leader) {
-                unsigned pos = gbr_slot(kl, GBR_SLOTS);
+                unsigned pos = rj_slot(kl, a.fine_bits, GBR_SLOTS);
                 bool done = false;
                 for (unsigned steps = 0; steps < GBR_SLOTS && !done; ++steps) {
                     unsigned long long prev = t.key[pos];
@@ -168,7 +160,7 @@ __device__ void gbr_fold_range(const GbrArgs& a, const GbrTable& t, const longlo
             rem &= ~m;
         }
         if ((rem >> lane) & 1) {
-            if (!gbr_fold(t, k, v, a.want_sum) && !gbr_global_add(a, k, v, 1, fresh)) full = true;
+            if (!gbr_fold(t, k, v, a.want_sum, a.fine_bits) && !gbr_global_add(a, k, v, 1, fresh)) full = true;
         }
     };
     // Loop bounds are uniform across each warp (the whole-warp test in
@@ -285,7 +277,7 @@ __global__ void __launch_bounds__(GBR_THREADS, 1) gbr_tiny_kernel(GbrArgs a)
     // lane adds its tuple with shared atomics, but only into its own warp's
     // table, so atomics of different warps never meet.
     auto add = [&](uint64_t k, uint64_t s, unsigned c) {
-        unsigned pos = gbr_slot(k, GBR_TINY_SLOTS);
+        unsigned pos = rj_slot(k, 0, GBR_TINY_SLOTS);
         for (int steps = 0; steps < GBR_TINY_SLOTS; ++steps) {
             unsigned long long prev = keys[pos];
             if (prev == kEmptyKey) prev = atomicCAS(&keys[pos], kEmptyKey, (unsigned long long)k);

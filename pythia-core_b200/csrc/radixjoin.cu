@@ -5,7 +5,7 @@
 // for the 16-byte (int64 key, int64 payload) case, B200-first:
 //
 //   1. histogram  one read of each relation counts the top `fine_bits`
-//                 bits of mix64(key) in a shared-memory histogram per CTA;
+//                 bits of rj_hash(key) in a shared-memory histogram per CTA;
 //                 the host turns the counts into exact partition offsets.
 //   2. partition  one or two tile passes (coarse bits, then the remaining
 //                 bits inside each coarse partition).  A CTA groups a
@@ -83,15 +83,6 @@ struct RJJoinArgs {
     unsigned* dup;              // set when a build key repeats (UNIQUE)
 };
 
-// Slot of key k in a table of TS slots: multiply-high of the top 32 bits of
-// a multiplicative (Fibonacci) hash.  Partition membership comes from
-// mix64, so within one partition these bits are as good as random, for one
-// multiply instead of the full mix.
-__device__ __forceinline__ unsigned rj_join_slot(uint64_t k, unsigned TS)
-{
-    return __umulhi((unsigned)((k * 0x9E3779B97F4A7C15ULL) >> 32), TS);
-}
-
 // Warms L2 with [p, p + bytes) (16-byte aligned start; bytes rounded down
 // to a multiple of 16); no registers are held for it.
 __device__ __forceinline__ void rj_prefetch_l2(const void* p, unsigned long long bytes)
@@ -151,7 +142,7 @@ __global__ void __launch_bounds__(RJ_JOIN_THREADS, RJ_JOIN_BLOCKS) rj_join_kerne
                 atomicAdd(&side_sum, (unsigned long long)t.y);
                 continue;
             }
-            unsigned pos = rj_join_slot(k, TS);
+            unsigned pos = rj_slot(k, a.fine_bits, TS);
             for (unsigned steps = 0; steps < TS; ++steps) {
                 unsigned long long* key = UNIQUE ? &T2[pos].x : &T4[pos].x;
                 const unsigned long long prev = atomicCAS(key, kEmptyKey, k);
@@ -181,7 +172,7 @@ __global__ void __launch_bounds__(RJ_JOIN_THREADS, RJ_JOIN_BLOCKS) rj_join_kerne
                 psum += scnt * (uint64_t)t.y;
                 return;
             }
-            unsigned pos = rj_join_slot(k, TS);
+            unsigned pos = rj_slot(k, a.fine_bits, TS);
             for (unsigned steps = 0; steps < TS; ++steps) {
                 if constexpr (UNIQUE) {
                     const ulonglong2 e = T2[pos];

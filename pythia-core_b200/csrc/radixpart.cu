@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(1024) rj_hist_kernel(const longlong2* __restri
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     auto count = [&](long long k) {
-        const unsigned r = rj_bin(mix64((uint64_t)k), shift, P - 1) - (unsigned)base;
+        const unsigned r = rj_bin(rj_hash((uint64_t)k), shift, P - 1) - (unsigned)base;
         if (r < (unsigned)span) atomicAdd(&rj_sh_hist[r], 1u);
     };
     constexpr int U = 8;
@@ -87,7 +87,7 @@ __global__ void rj_tile_prefix_kernel(unsigned long long* __restrict__ count, co
 // 2. Tile partition pass with exact offsets.  The input is a sequence of
 // segments (one for the first pass; the coarse partitions for the second);
 // tiles never straddle a segment.  Output bin of a tuple = (segment <<
-// lbits) | ((mix64(key) >> shift) & mask).
+// lbits) | ((rj_hash(key) >> shift) & mask).
 
 struct RJPass {
     const longlong2* in;
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
             if (valid) {
                 t[j] = sm.in[slot][i];
                 bin[j] = a.nsplit ? rj_range_bin(sm.split[a.nseg > 1 ? (k & 1) : 0], a.nsplit, t[j].x)
-                                  : rj_bin(mix64((uint64_t)t[j].x), a.shift, a.mask);
+                                  : rj_bin(rj_hash((uint64_t)t[j].x), a.shift, a.mask);
             }
             // Skewed keys put many lanes of a warp into one bin: when at
             // least 8 lanes share lane 0's bin, they take their ranks from

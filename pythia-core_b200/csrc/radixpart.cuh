@@ -1,5 +1,6 @@
 // Hash partitioning of 16-byte (int64 key, int64 payload) tuples by the
-// top bits of mix64(key), shared by the radix operators (join, group-by).
+// top bits of a multiplicative hash of the key, shared by the radix
+// operators (join, group-by).
 //
 //   histogram   rj_hist_kernel counts the top `bits` bits of every tuple (or
 //               of a strided sample) in shared memory.
@@ -104,12 +105,23 @@ int rp_partition(pyg_ctx* ctx, const longlong2* in, int64_t n, int FB, bool two,
                  const long long* csplit, const long long* fsplit, RJLayout& L, void** P1, void** P2,
                  unsigned* flags, unsigned* hflags, float* hist_ms = nullptr, int64_t* hist_tuples = nullptr);
 
-// Slot of a key in a shared-memory table of TS slots: multiply-high of the
-// 32 hash bits below the fine partition bits (all keys of one partition
-// share the top fine_bits bits).
-__device__ __forceinline__ unsigned rj_slot(uint64_t h, int fb, unsigned TS)
+// Hash of the radix operators: multiplication by 2^64 / golden ratio
+// (Fibonacci hashing).  Bit j of the product depends on key bits 0..j, so
+// the top bits mix the whole key: partitions take the top `fb` bits and
+// shared-memory tables the 32 bits below them.  Keys of one partition
+// differ in those 32 bits unless they differ only above bit 63 - fb - 32
+// of the product, and then they fall in different partitions.  Dense key
+// ranges spread almost evenly over the partitions and over the slots of a
+// partition's table (consecutive multiples of an irrational fraction).
+constexpr uint64_t kRjHashMul = 0x9E3779B97F4A7C15ULL;
+__host__ __device__ __forceinline__ uint64_t rj_hash(uint64_t k) { return k * kRjHashMul; }
+
+// Slot of key k in a shared-memory table of TS slots, for keys of one
+// partition of 2^fb (fb = 0: one partition): multiply-high of the 32 hash
+// bits below the partition bits.
+__device__ __forceinline__ unsigned rj_slot(uint64_t k, int fb, unsigned TS)
 {
-    return __umulhi((unsigned)(h >> (32 - fb)), TS);
+    return __umulhi((unsigned)(rj_hash(k) >> (32 - fb)), TS);
 }
 
 }  // namespace pyg
