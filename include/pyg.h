@@ -158,13 +158,13 @@ typedef struct pyg_join_opts {
 typedef struct pyg_join_stats {
     int32_t algorithm;
     int32_t radix_bits;
-    double build_partition_ms;  /* partition the build side (RADIX)     */
+    double build_partition_ms;  /* build side partition passes (RADIX)  */
     double build_ms;            /* table init + inserts                 */
-    double probe_partition_ms;  /* partition the probe side (RADIX)     */
+    double probe_partition_ms;  /* probe side partition passes (RADIX)  */
     double probe_ms;            /* probes + fused aggregation           */
     int64_t overflow_tuples;
     int64_t padded_tuples;
-    double histogram_ms;        /* partition histograms (RADIX)         */
+    double histogram_ms;        /* both relations' histograms (RADIX)   */
     int64_t histogram_tuples;   /* tuples the histograms read (RADIX)   */
 } pyg_join_stats;
 

@@ -174,7 +174,7 @@ int pyg_ctx_create(int device, pyg_ctx** out)
         return cuda_status(e, "cudaStreamCreate");
     }
     c->stream = c->own_stream;
-    c->pinned_bytes = 1 << 16;
+    c->pinned_bytes = kPinnedScalarBytes + kPinnedStageBytes;
     e = cudaMallocHost(&c->pinned, c->pinned_bytes);
     if (e == cudaSuccess) e = cudaMalloc((void**)&c->dcounters, 4096);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);

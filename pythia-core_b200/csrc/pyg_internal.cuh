@@ -8,13 +8,17 @@
 
 #include "../../include/pyg.h"
 
+constexpr size_t kPinnedScalarBytes = (size_t)1 << 16;  // scalar read-backs (fixed word offsets)
+constexpr size_t kPinnedStageBytes = (size_t)1 << 21;   // two relations x 2^16 partition counts x 8 B, x2
+
 struct pyg_ctx {
     int device;
     int sm_count;
     cudaStream_t own_stream;
     cudaStream_t stream;
     int64_t launches;
-    // Small pinned host staging area for scalar results read back per call.
+    // Pinned host staging: kPinnedScalarBytes for scalar results read back
+    // per call, then kPinnedStageBytes for per-partition counts.
     void* pinned;
     size_t pinned_bytes;
     // Device scratch for scalar counters (zeroed per use).

@@ -308,21 +308,26 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
     RJItem* ditems = nullptr;
     int rc = PYG_OK;
     do {
-        unsigned* flags = (unsigned*)(ctx->dcounters + 202);  // [0] a bulk copy never landed, [1] region overflow
+        // Words 202-203: per relation, [0] a bulk copy never landed, [1] region overflow.
+        unsigned* flags = (unsigned*)(ctx->dcounters + 202);
         unsigned long long* h = (unsigned long long*)ctx->pinned;
         unsigned* hflags = (unsigned*)(h + 6);
         // 1-2. Partition both sides (histograms sampled for large inputs).
-        RJLayout LR, LS;
-        float rh_ms = 0.f, sh_ms = 0.f;
-        int64_t rh_n = 0, sh_n = 0;
-        if ((rc = rp_partition(ctx, R, nR, FB, two, true, nullptr, nullptr, LR, &R1, &R2, flags, hflags, &rh_ms,
-                               &rh_n)))
-            break;
-        tm.mark(ctx, 2);
-        if ((rc = rp_partition(ctx, S, nS, FB, two, true, nullptr, nullptr, LS, &S1, &S2, flags, hflags, &sh_ms,
-                               &sh_n)))
-            break;
-        tm.mark(ctx, 3);
+        RPSide side[2];
+        side[0].in = R;
+        side[0].n = nR;
+        side[0].done = tm.on ? tm.ev[2] : nullptr;
+        side[1].in = S;
+        side[1].n = nS;
+        side[1].done = tm.on ? tm.ev[3] : nullptr;
+        rc = rp_partition_sides(ctx, side, 2, FB, two, flags, hflags, tm.on ? tm.ev[1] : nullptr);
+        R1 = side[0].P1;
+        R2 = side[0].P2;
+        S1 = side[1].P1;
+        S2 = side[1].P2;
+        if (rc) break;
+        const RJLayout& LR = side[0].L;
+        const RJLayout& LS = side[1].L;
 
         // 3. Join: distinct build keys first (16-byte slots); on a repeated
         // key, again with counted 32-byte slots and smaller build chunks.
@@ -372,17 +377,17 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
         tm.mark(ctx, 4);
         if (stats) {
             cudaEventSynchronize(tm.ev[4]);
-            // Partition phases include their histograms; histogram_ms
-            // reports the histograms' own time.
-            stats->histogram_ms = rh_ms + sh_ms;
-            stats->histogram_tuples = rh_n + sh_n;
-            stats->build_partition_ms = tm.ms(0, 2);
+            // Histograms of both relations, then the build side's passes
+            // (after the host round trip that lays out both), then the
+            // probe side's passes.
+            stats->histogram_ms = tm.ms(0, 1);
+            stats->histogram_tuples = side[0].hist_tuples + side[1].hist_tuples;
+            stats->build_partition_ms = tm.ms(1, 2);
             stats->build_ms = 0;
             stats->probe_partition_ms = tm.ms(2, 3);
             stats->probe_ms = tm.ms(3, 4);
             stats->padded_tuples = (int64_t)((LR.p2 + LS.p2) - (unsigned long long)(nR + nS));
-            stats->overflow_tuples = (LR.sampled || nR < ((int64_t)1 << 25) || !two ? 0 : 1) +
-                                     (LS.sampled || nS < ((int64_t)1 << 25) || !two ? 0 : 1);
+            stats->overflow_tuples = (side[0].overflowed ? 1 : 0) + (side[1].overflowed ? 1 : 0);
         }
     } while (0);
     dfree(ctx, ditems);

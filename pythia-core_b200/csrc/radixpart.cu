@@ -532,81 +532,142 @@ int hist_launch_range(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step
     return PYG_OK;
 }
 
-int rp_partition(pyg_ctx* ctx, const longlong2* in, int64_t n, int FB, bool two, bool allow_sample,
-                 const long long* csplit, const long long* fsplit, RJLayout& L, void** P1, void** P2,
-                 unsigned* flags, unsigned* hflags, float* hist_ms, int64_t* hist_tuples)
+int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsigned* flags, unsigned* hflags,
+                       cudaEvent_t hist_done)
 {
     const int CB = two ? (FB + 1) / 2 : FB;
     const int F = 1 << FB, C = 1 << CB, sub = FB - CB;
-    const bool sample = allow_sample && two && n >= ((int64_t)1 << 25);
-    const int64_t step = sample ? std::max<int64_t>(1, n >> 24) : 1;
     const size_t side = RJSideDev::words(F, C);
+    if (ns < 1 || ns > 2 || (size_t)ns * F * 8 > ctx->pinned_bytes - kPinnedScalarBytes) {
+        set_error("partition: %d relations of 2^%d partitions exceed the staging area", ns, FB);
+        return PYG_ERR_ARG;
+    }
+    // Per-partition counts come back through pinned memory, so that both
+    // relations' histograms cost one host round trip and both relations'
+    // passes another.
+    unsigned long long* hh = (unsigned long long*)((char*)ctx->pinned + kPinnedScalarBytes);
     unsigned long long* meta = nullptr;
-    *P1 = *P2 = nullptr;
+    RJSideDev d[2];
+    bool sample[2] = {false, false};
     int rc = PYG_OK;
-    auto hist_of = [&](int64_t st, unsigned long long* hist) {
-        return csplit ? hist_launch_range(ctx, in, n, st, CB, sub, csplit, fsplit, hist)
-                      : hist_launch(ctx, in, n, st, FB, hist);
+    for (int s = 0; s < ns; ++s) sd[s].P1 = sd[s].P2 = nullptr;
+    auto hist_of = [&](int s, int64_t st, unsigned long long* hist) {
+        return sd[s].csplit ? hist_launch_range(ctx, sd[s].in, sd[s].n, st, CB, sub, sd[s].csplit, sd[s].fsplit, hist)
+                            : hist_launch(ctx, sd[s].in, sd[s].n, st, FB, hist);
+    };
+    auto hist_at = [&](int s) { return meta + (size_t)s * (side + F) + side; };
+    auto launch = [&](int s) {
+        int r;
+        if ((r = upload_layout(ctx, sd[s].L, d[s], F, C, sd[s].n))) return r;
+        dfree(ctx, sd[s].P1);
+        dfree(ctx, sd[s].P2);
+        sd[s].P1 = sd[s].P2 = nullptr;
+        if ((r = dalloc(ctx, &sd[s].P1, (size_t)sd[s].L.p1 * 16))) return r;
+        if (two && (r = dalloc(ctx, &sd[s].P2, (size_t)sd[s].L.p2 * 16))) return r;
+        if ((r = run_passes(ctx, sd[s].in, sd[s].n, sd[s].L, d[s], two, FB, CB, sd[s].P1, sd[s].P2, flags + 2 * s,
+                            flags + 2 * s + 1, sd[s].csplit, sd[s].fsplit)))
+            return r;
+        if (sd[s].done) cudaEventRecord(sd[s].done, ctx->stream);
+        return PYG_OK;
     };
     do {
-        if ((rc = dalloc(ctx, (void**)&meta, (side + F) * 8))) break;
-        RJSideDev d;
-        d.carve(meta, F, C);
-        unsigned long long* hist = meta + side;
-        PYG_CUDA(cudaMemsetAsync(flags, 0, 8, ctx->stream));
-        cudaEvent_t e0 = nullptr, e1 = nullptr;
-        if (hist_ms) {
-            cudaEventCreate(&e0);
-            cudaEventCreate(&e1);
-            cudaEventRecord(e0, ctx->stream);
+        if ((rc = dalloc(ctx, (void**)&meta, (side + F) * 8 * ns))) break;
+        PYG_CUDA(cudaMemsetAsync(flags, 0, (size_t)8 * ns, ctx->stream));
+        int64_t step[2] = {1, 1};
+        for (int s = 0; s < ns && !rc; ++s) {
+            d[s].carve(meta + (size_t)s * (side + F), F, C);
+            sample[s] = sd[s].allow_sample && two && sd[s].n >= ((int64_t)1 << 25);
+            step[s] = sample[s] ? std::max<int64_t>(1, sd[s].n >> 24) : 1;
+            if ((rc = hist_of(s, step[s], hist_at(s)))) break;
+            sd[s].hist_tuples = (sd[s].n + step[s] - 1) / step[s];
         }
-        if ((rc = hist_of(step, hist))) break;
-        if (hist_ms) cudaEventRecord(e1, ctx->stream);
-        if (hist_tuples) *hist_tuples = (n + step - 1) / step;
-        std::vector<unsigned long long> h(F);
-        PYG_CUDA(cudaMemcpyAsync(h.data(), hist, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        if (rc) break;
+        if (hist_done) cudaEventRecord(hist_done, ctx->stream);
+        for (int s = 0; s < ns; ++s)
+            PYG_CUDA(cudaMemcpyAsync(hh + (size_t)s * F, hist_at(s), (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
         PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-        if (hist_ms) {
-            cudaEventElapsedTime(hist_ms, e0, e1);
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
+        // The second relation's layout is formed while the first one's
+        // passes run.
+        for (int s = 0; s < ns && !rc; ++s) {
+            std::vector<unsigned long long> h(hh + (size_t)s * F, hh + (size_t)(s + 1) * F);
+            if (sample[s]) layout_sampled(h, step[s], C, sub, sd[s].L);
+            else layout_exact(h, C, sub, sd[s].L);
+            rc = launch(s);
         }
-        if (sample) layout_sampled(h, step, C, sub, L);
-        else layout_exact(h, C, sub, L);
-        for (int attempt = 0; attempt < 2; ++attempt) {
-            if ((rc = upload_layout(ctx, L, d, F, C, n))) break;
-            dfree(ctx, *P1);
-            dfree(ctx, *P2);
-            *P1 = *P2 = nullptr;
-            if ((rc = dalloc(ctx, P1, (size_t)L.p1 * 16))) break;
-            if (two && (rc = dalloc(ctx, P2, (size_t)L.p2 * 16))) break;
-            if ((rc = run_passes(ctx, in, n, L, d, two, FB, CB, *P1, *P2, flags, flags + 1, csplit, fsplit))) break;
-            PYG_CUDA(cudaMemcpyAsync(hflags, flags, 8, cudaMemcpyDeviceToHost, ctx->stream));
-            if (L.sampled) {
-                L.count.resize(F);
-                PYG_CUDA(cudaMemcpyAsync(L.count.data(), d.cur2, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
-            }
-            PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-            if (hflags[0]) {
+        if (rc) break;
+        PYG_CUDA(cudaMemcpyAsync(hflags, flags, (size_t)8 * ns, cudaMemcpyDeviceToHost, ctx->stream));
+        for (int s = 0; s < ns; ++s)
+            if (sd[s].L.sampled)
+                PYG_CUDA(cudaMemcpyAsync(hh + (size_t)s * F, d[s].cur2, (size_t)F * 8, cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (int s = 0; s < ns && !rc; ++s) {
+            if (hflags[2 * s]) {
                 set_error("partition: a tile copy did not complete in time");
                 rc = PYG_ERR_TIMEOUT;
                 break;
             }
-            if (!hflags[1]) break;
-            // A sampled region overflowed: redo from an exact histogram.
-            if ((rc = hist_of(1, hist))) break;
-            PYG_CUDA(cudaMemcpyAsync(h.data(), hist, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            if (sd[s].L.sampled) sd[s].L.count.assign(hh + (size_t)s * F, hh + (size_t)(s + 1) * F);
+            if (!hflags[2 * s + 1]) continue;
+            // A sampled region overflowed: redo this relation from an exact
+            // histogram (exact regions cannot overflow).
+            sd[s].overflowed = true;
+            sd[s].done = nullptr;  // the redo's time is not attributed to the relation
+            if ((rc = hist_of(s, 1, hist_at(s)))) break;
+            PYG_CUDA(cudaMemcpyAsync(hh, hist_at(s), (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
             PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-            layout_exact(h, C, sub, L);
-            PYG_CUDA(cudaMemsetAsync(flags, 0, 8, ctx->stream));
+            layout_exact(std::vector<unsigned long long>(hh, hh + F), C, sub, sd[s].L);
+            PYG_CUDA(cudaMemsetAsync(flags + 2 * s, 0, 8, ctx->stream));
+            if ((rc = launch(s))) break;
+            PYG_CUDA(cudaMemcpyAsync(hflags + 2 * s, flags + 2 * s, 8, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+            if (hflags[2 * s]) {
+                set_error("partition: a tile copy did not complete in time");
+                rc = PYG_ERR_TIMEOUT;
+            } else if (hflags[2 * s + 1]) {
+                set_error("partition: an exact region overflowed");
+                rc = PYG_ERR_CAPACITY;
+            }
         }
     } while (0);
     dfree(ctx, meta);
     if (rc) {
-        dfree(ctx, *P1);
-        dfree(ctx, *P2);
-        *P1 = *P2 = nullptr;
+        for (int s = 0; s < ns; ++s) {
+            dfree(ctx, sd[s].P1);
+            dfree(ctx, sd[s].P2);
+            sd[s].P1 = sd[s].P2 = nullptr;
+        }
     }
+    return rc;
+}
+
+int rp_partition(pyg_ctx* ctx, const longlong2* in, int64_t n, int FB, bool two, bool allow_sample,
+                 const long long* csplit, const long long* fsplit, RJLayout& L, void** P1, void** P2,
+                 unsigned* flags, unsigned* hflags, float* hist_ms, int64_t* hist_tuples)
+{
+    RPSide s;
+    s.in = in;
+    s.n = n;
+    s.allow_sample = allow_sample;
+    s.csplit = csplit;
+    s.fsplit = fsplit;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (hist_ms) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, ctx->stream);
+    }
+    const int rc = rp_partition_sides(ctx, &s, 1, FB, two, flags, hflags, e1);
+    if (hist_ms) {
+        *hist_ms = 0.f;
+        if (!rc) cudaEventElapsedTime(hist_ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    if (hist_tuples) *hist_tuples = s.hist_tuples;
+    L = std::move(s.L);
+    *P1 = s.P1;
+    *P2 = s.P2;
     return rc;
 }
 

@@ -93,6 +93,35 @@ int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, 
 // Histogram of range bins (see run_passes) of in[0], in[step], ...
 int hist_launch_range(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int CB, int sub,
                       const long long* csplit, const long long* fsplit, unsigned long long* hist);
+// One relation for rp_partition_sides.  In: in, n, allow_sample, the
+// splitters (range mode) and an optional event recorded after the
+// relation's passes.  Out: the layout (counts included), the pass buffers
+// (the caller frees them), the tuples its histogram read and whether a
+// sampled region overflowed (then the relation was redone exactly).
+struct RPSide {
+    const longlong2* in = nullptr;
+    int64_t n = 0;
+    bool allow_sample = true;
+    const long long* csplit = nullptr;
+    const long long* fsplit = nullptr;
+    cudaEvent_t done = nullptr;
+    RJLayout L;
+    void* P1 = nullptr;
+    void* P2 = nullptr;
+    int64_t hist_tuples = 0;
+    bool overflowed = false;
+};
+
+// Partitions one or two relations with the same bits: both histograms, one
+// host round trip, both relations' passes (the second relation's layout is
+// formed while the first one's passes run), one more round trip for the
+// counts and flags, and an exact redo of a relation whose sampled region
+// overflowed.  flags: 2 device words per relation (bulk copy never landed,
+// region overflow); hflags: as many pinned host words.  hist_done
+// (optional) is recorded after the histograms.
+int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsigned* flags, unsigned* hflags,
+                       cudaEvent_t hist_done);
+
 // Partitions one relation into 2^FB partitions (hash bits, or ranges when
 // csplit is set; two passes when `two`): histogram (sampled when allowed
 // and n >= 2^25), layout, passes, and an exact redo if a sampled region
