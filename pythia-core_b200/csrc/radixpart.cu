@@ -34,11 +34,11 @@ __device__ __forceinline__ unsigned rj_bin(uint64_t h, int shift, unsigned mask)
 // counters per CTA).
 
 __global__ void __launch_bounds__(1024) rj_hist_kernel(const longlong2* __restrict__ in, int64_t n, int64_t step,
-                                                       int bits, int base, int span,
-                                                       unsigned long long* __restrict__ hist)
+                                                       int bits, int base, int span, unsigned* __restrict__ part)
 {
     // Counts the bins [base, base + span) of in[0], in[step], in[2 step],
-    // ... (step 1: every tuple); span 32-bit counters in shared memory.
+    // ... (step 1: every tuple); span 32-bit counters in shared memory,
+    // stored to this CTA's row of part (rj_hist_sum_kernel adds the rows).
     extern __shared__ unsigned rj_sh_hist[];
     const int P = 1 << bits;
     const int shift = 64 - bits;
@@ -61,8 +61,21 @@ __global__ void __launch_bounds__(1024) rj_hist_kernel(const longlong2* __restri
     }
     for (; i < m; i += stride) count(__ldcs(&in[i * step]).x);
     __syncthreads();
-    for (int b = threadIdx.x; b < span; b += blockDim.x)
-        if (rj_sh_hist[b]) atomicAdd(&hist[base + b], (unsigned long long)rj_sh_hist[b]);
+    unsigned* row = part + (size_t)blockIdx.x * span;
+    for (int b = threadIdx.x; b < span; b += blockDim.x) row[b] = rj_sh_hist[b];
+}
+
+// hist[b] = sum over the nrow rows of part[row * span + b], b < span: the
+// CTAs' shared-memory histograms added column by column (coalesced and in a
+// fixed order) instead of by atomics from every CTA on each bin.
+__global__ void rj_hist_sum_kernel(const unsigned* __restrict__ part, int nrow, int span,
+                                   unsigned long long* __restrict__ hist)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= span) return;
+    unsigned long long sum = 0;
+    for (int r = 0; r < nrow; ++r) sum += part[(size_t)r * span + b];
+    hist[b] = sum;
 }
 
 // Tiles per segment, as an exclusive prefix (one thread; at most 2^8
@@ -180,7 +193,7 @@ __device__ __forceinline__ void rj_load_split(const RJPass& a, long long* dst, i
 __global__ void __launch_bounds__(1024) rj_hist_range_kernel(const longlong2* __restrict__ in, int64_t n, int64_t step,
                                                              int CB, int sub, const long long* __restrict__ csplit,
                                                              const long long* __restrict__ fsplit,
-                                                             unsigned long long* __restrict__ hist)
+                                                             unsigned* __restrict__ part)
 {
     extern __shared__ __align__(16) unsigned char rj_hr_raw[];
     const int F = 1 << (CB + sub), C = 1 << CB, L = 1 << sub;
@@ -198,8 +211,8 @@ __global__ void __launch_bounds__(1024) rj_hist_range_kernel(const longlong2* __
         atomicAdd(&h[f], 1u);
     }
     __syncthreads();
-    for (int b = threadIdx.x; b < F; b += blockDim.x)
-        if (h[b]) atomicAdd(&hist[b], (unsigned long long)h[b]);
+    unsigned* row = part + (size_t)blockIdx.x * F;
+    for (int b = threadIdx.x; b < F; b += blockDim.x) row[b] = h[b];
 }
 
 // Thread 0: starts the bulk copy of tile `tile` into ring slot `slot`.
@@ -506,11 +519,16 @@ int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int 
     const int64_t m = (n + step - 1) / step;
     const int64_t want = (m + 1024 * 8 - 1) / (1024 * 8);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->sm_count * per));
-    PYG_CUDA(cudaMemsetAsync(hist, 0, (size_t)8 * F, ctx->stream));
+    unsigned* part = nullptr;
+    int rc;
+    if ((rc = dalloc(ctx, (void**)&part, (size_t)grid * span * 4))) return rc;
     for (int base = 0; base < F; base += span) {
-        rj_hist_kernel<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, FB, base, span, hist);
+        rj_hist_kernel<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, FB, base, span, part);
+        PYG_LAUNCHED(ctx);
+        rj_hist_sum_kernel<<<(span + 255) / 256, 256, 0, ctx->stream>>>(part, grid, span, hist + base);
         PYG_LAUNCHED(ctx);
     }
+    dfree(ctx, part);
     return PYG_OK;
 }
 
@@ -526,9 +544,14 @@ int hist_launch_range(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step
     const int64_t m = (n + step - 1) / step;
     const int64_t want = (m + 1024 * 8 - 1) / (1024 * 8);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->sm_count * per));
-    PYG_CUDA(cudaMemsetAsync(hist, 0, (size_t)8 * F, ctx->stream));
-    rj_hist_range_kernel<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, CB, sub, csplit, fsplit, hist);
+    unsigned* part = nullptr;
+    int rc;
+    if ((rc = dalloc(ctx, (void**)&part, (size_t)grid * F * 4))) return rc;
+    rj_hist_range_kernel<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, CB, sub, csplit, fsplit, part);
     PYG_LAUNCHED(ctx);
+    rj_hist_sum_kernel<<<(F + 255) / 256, 256, 0, ctx->stream>>>(part, grid, F, hist);
+    PYG_LAUNCHED(ctx);
+    dfree(ctx, part);
     return PYG_OK;
 }
 
