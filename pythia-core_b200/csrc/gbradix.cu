@@ -404,7 +404,7 @@ int groupby16_fill(pyg_ctx* ctx, const void* in, int64_t n, int want_sum, int64_
     const int CB = two ? (FB + 1) / 2 : FB;
     const int F = 1 << FB, C = 1 << CB, sub = FB - CB;
     const bool sample = two && n >= ((int64_t)1 << 25);
-    const int64_t step = sample ? std::max<int64_t>(1, n >> 24) : 1;
+    const int64_t step = sample ? std::max<int64_t>(1, n >> RJ_SAMPLE_LOG2) : 1;
     const longlong2* src = (const longlong2*)in;
     const size_t side = RJSideDev::words(F, C);
     unsigned long long* meta = nullptr;

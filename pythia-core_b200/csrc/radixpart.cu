@@ -600,7 +600,7 @@ int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsig
         for (int s = 0; s < ns && !rc; ++s) {
             d[s].carve(meta + (size_t)s * (side + F), F, C);
             sample[s] = sd[s].allow_sample && two && sd[s].n >= ((int64_t)1 << 25);
-            step[s] = sample[s] ? std::max<int64_t>(1, sd[s].n >> 24) : 1;
+            step[s] = sample[s] ? std::max<int64_t>(1, sd[s].n >> RJ_SAMPLE_LOG2) : 1;
             if ((rc = hist_of(s, step[s], hist_at(s)))) break;
             sd[s].hist_tuples = (sd[s].n + step[s] - 1) / step[s];
         }

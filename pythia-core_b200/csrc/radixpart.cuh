@@ -38,6 +38,13 @@ constexpr int RJ_SPLIT_MAX = 256;        // range mode: splitters per pass segme
 // 2^15 32-bit counters in shared memory.
 constexpr int RJ_MAX_FINE_BITS = 16;   // hash mode (histograms run in halves above 2^15 bins)
 constexpr int RJ_MAX_RANGE_BITS = 15;  // range mode (one 2^15-counter histogram)
+#ifndef PYG_RJ_SAMPLE_LOG2
+#define PYG_RJ_SAMPLE_LOG2 22
+#endif
+// Sampled layouts count every (n >> RJ_SAMPLE_LOG2)-th tuple (2^22 samples:
+// at most 0.2 ms for two relations; regions get more slack than with a
+// larger sample, which costs device memory, not traffic).
+constexpr int RJ_SAMPLE_LOG2 = PYG_RJ_SAMPLE_LOG2;
 
 // Host-side layout of one relation's partitions.
 struct RJLayout {
