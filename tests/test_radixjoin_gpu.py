@@ -21,6 +21,27 @@ def zipf_keys(rng, n, keys, theta):
     return keys[np.minimum(np.searchsorted(c, rng.random(n)), len(keys) - 1)]
 
 
+@pytest.mark.parametrize("stride", [1 << 16, 1 << 32, 1597, 1000])
+def test_radix_strided_keys(ctx, torch_cuda, stride):
+    """Keys on a regular stride (multiples of 2^16, 2^32, a Fibonacci number,
+    1000): the patterns a plain multiplicative hash handles worst.  Every
+    probe key is a build key (PK-FK), so the result is known in closed form:
+    count = |S|, sums = the build payloads of the drawn rows and the probe
+    payloads (below 2^60: no wrap-around).  The oracle is not used here: it
+    buckets by the key's low bits, as the reference does, and walks one
+    chain of every build key for strides of 2^16 and more."""
+    rng = np.random.default_rng(stride % 1000003)
+    n, m = 1 << 16, 1 << 20
+    k = rng.permutation(n).astype(np.int64) * stride
+    rp, idx, sp = rng.integers(0, 1 << 40, n), rng.integers(0, n, m), rng.integers(0, 1 << 40, m)
+    R = struct([k, rp], [I64, I64])
+    S = struct([k[idx], sp], [I64, I64])
+    want = (m, [int(rp[idx].sum()), int(sp.sum())])
+    got = ctx.hashjoin_agg(dev_rel(torch_cuda, R, [I64, I64]), [0], dev_rel(torch_cuda, S, [I64, I64]), [0], PROJ,
+                           pyg.JOIN_RADIX, 4)
+    assert got == want
+
+
 @pytest.mark.parametrize("theta", [0.0, 0.75, 1.25])
 @pytest.mark.parametrize("bits", [0, 3, 8, 12])
 def test_radix_equals_direct_equals_oracle(ctx, torch_cuda, theta, bits):
