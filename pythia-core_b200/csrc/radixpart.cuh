@@ -142,7 +142,7 @@ int rp_partition(pyg_ctx* ctx, const longlong2* in, int64_t n, int FB, bool two,
                  unsigned* flags, unsigned* hflags, float* hist_ms = nullptr, int64_t* hist_tuples = nullptr);
 
 // Hash of the radix operators: multiplication by 2^64 / golden ratio
-// (Fibonacci hashing) after two xor-shifts.  Bit j of the product depends
+// (Fibonacci hashing) after three xor-shifts.  Bit j of the product depends
 // on bits 0..j of the shifted key, so the top bits mix the whole key:
 // partitions take the top `fb` bits and shared-memory tables the 32 bits
 // below them.  Dense key ranges spread almost evenly over the partitions
@@ -151,11 +151,14 @@ int rp_partition(pyg_ctx* ctx, const longlong2* in, int64_t n, int FB, bool two,
 // onto themselves, so a dense range keeps this).  Without the xor-shifts,
 // keys that are multiples of 2^16 or of a Fibonacci number (987, 1597, ...)
 // see the product's weaker lower bits and pile into long probe chains
-// (30-110 probes per lookup at half load instead of about 1.3).
+// (30-110 probes per insert at a third of the table instead of about 1.3);
+// with these three shifts, strides, Fibonacci multiples and packed
+// (a << s) | b keys stay at 1.0-2.1.
 constexpr uint64_t kRjHashMul = 0x9E3779B97F4A7C15ULL;
 __host__ __device__ __forceinline__ uint64_t rj_hash(uint64_t k)
 {
     k ^= k >> 32;
+    k ^= k >> 21;
     k ^= k >> 16;
     return k * kRjHashMul;
 }
