@@ -6,6 +6,9 @@
 // count of the INT64_MIN key}; compaction and ordering by key are shared.
 // What differs is how the table is filled:
 //
+//   very few     (expected <= GBR_TINY_GROUPS) every warp folds into its own
+//                128-slot table after leader rounds combine its lanes' most
+//                frequent keys, so atomics of different warps never meet.
 //   few groups   (expected <= GBR_DIRECT_GROUPS) every CTA folds its slice
 //                of the input into a 160 KB shared-memory table and flushes
 //                it once: one HBM read of the input, G atomics per CTA.
