@@ -56,7 +56,7 @@ int pyg_cdf_loss_grad(pyg_ctx* ctx, const int64_t* sorted_keys, int64_t n, int32
                       const float* params_host, double key_lo, double key_scale, double* loss,
                       float* grad_host);
 /* Splitters from the quantiles of a device key sample (the fallback, and
- * the judge of the learned splitters' imbalance). */
+ * the yardstick for the learned splitters' imbalance). */
 int pyg_sampled_splitters(pyg_ctx* ctx, const int64_t* sample_keys, int64_t n, int32_t fanout,
                           int64_t* out);
 /* Distinct-key estimate for a population of `population` keys from the
