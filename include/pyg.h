@@ -174,21 +174,26 @@ int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_ke
                      pyg_join_result* out, pyg_join_stats* stats);
 
 /* Hash join + sum that allocates nothing.  No counterpart in the
- * reference: it is for callers that cannot allocate device memory at the
- * point of the call (inside a CUDA graph capture, under another
- * allocator's ownership of device memory, on latency-critical paths).  The
- * table lives in a fixed device array inside the library (about 16 MiB
- * held on every GPU that loads the library until the process exits), so
- * the build side is limited to PYG_NOALLOC_MAX_BUILD tuples; larger inputs
- * are rejected with PYG_ERR_ARG.  Inputs: 16-byte (int64 key, int64
- * payload) device tuples.  Output: out_dev[0..2] (device) = match count,
- * wrapped sum of build payloads, wrapped sum of probe payloads over the
- * joined pairs.  Kernels are only enqueued on `stream` (a cudaStream_t,
- * NULL = legacy default stream) on the current device; nothing is
- * synchronised.  The first call on a device looks up the array's device
- * address: make that first call before any stream capture.  Calls share
+ * reference: it is for callers that cannot call cudaMalloc where they
+ * join, such as an engine whose device memory all belongs to another
+ * allocator (a framework's caching pool, a query runtime's arena) that a
+ * library must not bypass, or a latency-critical path where an allocation
+ * could block on the device.  The table lives in a fixed device array
+ * inside the library (about 16 MiB held on every GPU that loads the
+ * library until the process exits), so the build side is limited to
+ * PYG_NOALLOC_MAX_BUILD tuples; larger inputs are rejected with
+ * PYG_ERR_ARG.  Inputs: 16-byte (int64 key, int64 payload) device tuples.
+ * Output: out_dev[0..2] (device) = match count, wrapped sum of build
+ * payloads, wrapped sum of probe payloads over the joined pairs.  Kernels
+ * are only enqueued on `stream` (a cudaStream_t, NULL = legacy default
+ * stream) on the current device; nothing is synchronised.  The first call
+ * on a device looks up the array's device address once (make that first
+ * call before any stream capture); a device reset (cudaDeviceReset)
+ * invalidates the address, so reload the library after one.  Calls share
  * the array (each clears it first), so calls that overlap on the GPU
- * race: order them on one stream. */
+ * race: order them on one stream.  A CUDA error still pending from an
+ * earlier, unrelated call is reported (and left pending) before anything
+ * is enqueued. */
 #define PYG_NOALLOC_MAX_BUILD (1 << 18)
 int pyg_hashjoin_agg_noalloc(const void* build, int64_t nbuild, const void* probe, int64_t nprobe,
                              int64_t* out_dev, void* stream);

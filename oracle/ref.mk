@@ -5,7 +5,7 @@
 # C oracle (oracle/pyg_oracle.c) and the CPU arm that bench.py times.  It is
 # never part of the product path.
 #
-#   make -f oracle/ref.mk REF=/root/reference        (run from the repo root)
+#   make -f oracle/ref.mk REF=<path of the reference sources>   (from the repo root)
 #
 # The reference's own Makefile is not used (its `all` target runs a
 # pre-init script that needs a missing hdf5 tarball, and libconfig's
@@ -24,7 +24,9 @@
 # is compiled with `resetdata(d,l)` mapped to `clear()` on the command line.
 # The reference sources are not modified.
 
-REF ?= /root/reference
+ifndef REF
+$(error REF is not set: pass REF=<path of the reference sources>)
+endif
 OUT := oracle/_ref
 OBJ := $(OUT)/obj
 

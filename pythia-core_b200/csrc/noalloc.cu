@@ -2,9 +2,8 @@
 // file-scope device array instead of memory obtained from cudaMalloc.
 //
 // For callers that cannot allocate device memory at the point of the call:
-// code running inside a CUDA graph capture that must not add allocation
-// nodes, engines whose memory is owned by another allocator (a framework's
-// pool or a query runtime's arena) that the library must not bypass, or
+// engines whose memory is owned by another allocator (a framework's pool
+// or a query runtime's arena) that the library must not bypass, or
 // real-time paths where an allocation may block on the device.  The
 // caller passes device inputs and a device output; the call only enqueues
 // kernels on the caller's stream.
@@ -114,7 +113,10 @@ __global__ void noalloc_finish_kernel(const unsigned long long* head, int64_t* o
     out[2] = (int64_t)(head[2] + bc * psum);
 }
 
-// Device address of the scratch array, looked up once per device.
+// Device address of the scratch array, looked up once per device (with that
+// device current).  A device reset unloads the module that holds the array,
+// so the cached address is only valid until then: reload the library after
+// cudaDeviceReset.
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_addr[64];
 
@@ -152,6 +154,15 @@ extern "C" int pyg_hashjoin_agg_noalloc(const void* build, int64_t nbuild, const
                   (long long)nbuild, PYG_NOALLOC_MAX_BUILD);
         return PYG_ERR_ARG;
     }
+    // An error left pending by an earlier, unrelated call is reported as
+    // such and left pending for its owner; the launch checks below then
+    // only see errors of this call's own launches.
+    cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        set_error("pyg_hashjoin_agg_noalloc: a CUDA error from an earlier call is pending: %s",
+                  cudaGetErrorString(pending));
+        return PYG_ERR_CUDA;
+    }
     int device = 0;
     PYG_CUDA(cudaGetDevice(&device));
     void* scratch = nullptr;
@@ -162,21 +173,25 @@ extern "C" int pyg_hashjoin_agg_noalloc(const void* build, int64_t nbuild, const
     uint64_t cap = (uint64_t)(2 * nbuild) + 64;
     if (cap > kNoAllocSlots) cap = kNoAllocSlots;
     cudaStream_t s = (cudaStream_t)stream;
-    int threads = 256;
-    int grid = (int)((cap + threads - 1) / threads);
-    if (grid > 4096) grid = 4096;
-    noalloc_clear_kernel<<<grid, threads, 0, s>>>(head, table, cap);
+    const int threads = 256;
+    // Grids are clamped in 64-bit arithmetic before narrowing to int.
+    auto grid_of = [&](int64_t n, int64_t most) {
+        const int64_t g = (n + threads - 1) / threads;
+        return (int)(g < most ? g : most);
+    };
+    noalloc_clear_kernel<<<grid_of((int64_t)cap, 4096), threads, 0, s>>>(head, table, cap);
+    PYG_CUDA(cudaGetLastError());
     if (nbuild > 0) {
-        int g = (int)((nbuild + threads - 1) / threads);
-        noalloc_build_kernel<<<g < 4096 ? g : 4096, threads, 0, s>>>((const longlong2*)build, nbuild, head, table, cap);
+        noalloc_build_kernel<<<grid_of(nbuild, 4096), threads, 0, s>>>((const longlong2*)build, nbuild, head, table,
+                                                                        cap);
+        PYG_CUDA(cudaGetLastError());
     }
     if (nprobe > 0) {
-        int g = (int)((nprobe + threads - 1) / threads);
-        noalloc_probe_kernel<<<g < 8192 ? g : 8192, threads, 0, s>>>((const longlong2*)probe, nprobe, head, table,
-                                                                      cap);
+        noalloc_probe_kernel<<<grid_of(nprobe, 8192), threads, 0, s>>>((const longlong2*)probe, nprobe, head, table,
+                                                                        cap);
+        PYG_CUDA(cudaGetLastError());
     }
     noalloc_finish_kernel<<<1, 1, 0, s>>>(head, out_dev);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_status(e, "pyg_hashjoin_agg_noalloc launch");
+    PYG_CUDA(cudaGetLastError());
     return PYG_OK;
 }

@@ -43,6 +43,9 @@ JOIN_AUTO = 0
 JOIN_DIRECT = 1
 JOIN_RADIX = 2
 
+# Largest build side of pyg_hashjoin_agg_noalloc (PYG_NOALLOC_MAX_BUILD).
+NOALLOC_MAX_BUILD = 1 << 18
+
 MPSM_EXACTRANGE = 0
 MPSM_SAMPLED = 1
 MPSM_LEARNED = 2

@@ -48,7 +48,7 @@ def make_fragments(torch, n, seed, max_log=14):
 def expected(host):
     out = []
     for R, S in host:
-        c, (a, b) = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ, buckets=1024)
+        c, (a, b) = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ, buckets=max(1024, R.shape[0]))
         out.append((c, (a + b + (1 << 63)) % (1 << 64) - (1 << 63)))
     return out
 
@@ -69,6 +69,47 @@ def test_batch_matches_oracle_and_replays(ctx, torch_cuda):
     c, s, lat = ctx.batch_run_plain(frags)
     assert [(int(x), int(y)) for x, y in zip(c, s)] == want
     assert np.all(np.diff(lat) >= 0)
+
+
+def test_batch_config5_sizes_match_oracle(ctx, torch_cuda):
+    """Fragments of the mixed-size batch workload's shape
+    (drivers/executemultiplequery.cpp:134-180 runs each as its own
+    hashjoin -> aggregate_sum plan): builds log-uniform in 2^12..2^22 with the
+    extremes included, probes 4-32x the build, unique build keys (a seeded
+    permutation), uniform or Zipf(1.0) foreign keys, int64 payloads.  Both the
+    batched form and the plain path must equal the oracle per fragment."""
+    torch = torch_cuda
+    rng = np.random.default_rng(55)
+    logs = [12.0, 22.0] + list(rng.uniform(12, 22, 6))
+    host, dev = [], []
+    for i, lg in enumerate(logs):
+        nb = int(2 ** lg)
+        mult = 4 if nb > (1 << 20) else int(rng.integers(4, 33))
+        npr = nb * mult
+        keys = rng.permutation(nb).astype(np.int64) * 5 + 1
+        R = struct([keys, keys * 7], [I64, I64])
+        if i % 2:
+            w = np.arange(1, nb + 1, dtype=np.float64) ** -1.0
+            cdf = np.cumsum(w)
+            cdf /= cdf[-1]
+            rank = np.minimum(np.searchsorted(cdf, rng.random(npr), side="right"), nb - 1)
+        else:
+            rank = rng.integers(0, nb, npr)
+        S = struct([keys[rank], rng.integers(0, 1 << 20, npr)], [I64, I64])
+        host.append((R, S))
+        dev.append((to_device(torch, R), nb, to_device(torch, S), npr))
+    frags = ctx.fragments(dev)
+    want = expected(host)
+    b = ctx.batch_create(frags)
+    try:
+        for _ in range(2):
+            rc, c, s, lat = ctx.batch_run(b, len(dev))
+            assert rc == pyg.PYG_OK
+            assert [(int(x), int(y)) for x, y in zip(c, s)] == want
+    finally:
+        ctx.batch_free(b)
+    c, s, _ = ctx.batch_run_plain(frags)
+    assert [(int(x), int(y)) for x, y in zip(c, s)] == want
 
 
 @pytest.mark.parametrize("tuning", [(256, 1, 0.5, 256), (1024, 2, 0.8, 65536), (512, 4, 0.7, 4096)])

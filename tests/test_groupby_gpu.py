@@ -68,6 +68,43 @@ def test_groupby_shared_memory_paths(ctx, torch_cuda, G, expected, n):
     assert rows(out) == rows(O.groupby(A, [I64, I64], [0], 3, 1, buckets=G))
 
 
+def zipf_ranks(rng, n, G, theta):
+    """Ranks in [0, G) with P(r) ~ (r + 1)^-theta (CDF inversion in fp64)."""
+    w = np.arange(1, G + 1, dtype=np.float64) ** (-theta)
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    return np.minimum(np.searchsorted(cdf, rng.random(n), side="right"), G - 1)
+
+
+@pytest.mark.parametrize("G", [1 << 10, 1 << 16, 1 << 20])
+@pytest.mark.parametrize("zipf", [False, True])
+def test_groupby_composite_config3_cardinalities(ctx, torch_cuda, G, zipf):
+    """Group-by over a composite (int32, int32) key, the second key form of
+    the 2^28-tuple group-by workload (operators/genericaggregate.cpp:247-289
+    with the `bytes` hasher over both columns): 2^22 tuples (int32 hi, int32
+    lo, int64 value) where the group id g (uniform, or Zipf(1.0) ranks
+    through a seeded permutation) is split as hi = g >> ceil(log2 G / 2),
+    lo = g & mask; values uniform in [0, 2^20).  Sum and count per group,
+    ordered by (hi, lo), identical to the oracle."""
+    rng = np.random.default_rng(G * 3 + zipf)
+    n = 1 << 22
+    rank = zipf_ranks(rng, n, G, 1.0) if zipf else rng.integers(0, G, n)
+    g = rng.permutation(G).astype(np.int64)[rank]
+    half = ((G - 1).bit_length() + 1) // 2
+    hi, lo = (g >> half).astype(np.int32), (g & ((1 << half) - 1)).astype(np.int32)
+    # Spread the halves over the signed int32 range so the lexicographic
+    # order of (hi, lo) differs from the order of g.
+    hi = (hi.astype(np.int64) * 2654435761 % (1 << 32) - (1 << 31)).astype(np.int32)
+    lo = (lo.astype(np.int64) * 40503 - (1 << 20)).astype(np.int32)
+    A = struct([hi, lo, rng.integers(0, 1 << 20, n)], [I32, I32, I64])
+    types = [I32, I32, I64]
+    ref = O.groupby(A, types, [0, 1], 3, 2, buckets=G, bytes_hash=True)
+    for expected in (G, 0):
+        out = run_groupby(ctx, torch_cuda, A, types, [0, 1], 3, 2, expected)
+        assert out.shape[0] == ref.shape[0]
+        assert rows(out) == rows(ref)
+
+
 def test_groupby_uniform_warps_and_sentinel(ctx, torch_cuda):
     """Runs of one key (whole warps fold with one reduction) mixed with the
     INT64_MIN group and count-only output."""
