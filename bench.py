@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--scale-shift", type=int, default=0, help="shrink both relations by 2^s (debug only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="join: skip the other configurations measured after the headline")
     ap.add_argument("--workload", default="join", choices=["join", "join-small", "groupby", "mpsm", "batch"],
                     help="join: the headline configuration (default); the others measure the small join, "
                          "group-by, MPSM sort-merge join and batched-fragment configurations")
@@ -309,51 +311,7 @@ def main_gpu(args):
     value = (nR + nS) * args.steps * world / (ms / 1000.0)
 
     hbm, peak_kind = peaks()
-    mean = lambda f: statistics.fmean(getattr(p, f) for p in phase)  # noqa: E731
-    radix = int(phase[0].algorithm) == pyg.JOIN_RADIX
-    two_pass = radix and int(phase[0].radix_bits) > 9
-    # Algorithmic bytes per phase: every tuple read once, and written once
-    # more by each partition pass.
-    if radix:
-        npass = 2 if two_pass else 1
-        # Each partition phase includes its side's histogram (a strided
-        # sample for large inputs), whose reads are not counted as
-        # algorithmic bytes.
-        phases = {
-            "build_partition": (mean("build_partition_ms"), nR * 32 * npass, "rj_partition_kernel", npass),
-            "probe_partition": (mean("probe_partition_ms"), nS * 32 * npass, "rj_partition_kernel", npass),
-            "join": (mean("probe_ms"), (nR + nS) * 16, "rj_join_kernel", 1),
-        }
-    else:
-        phases = {
-            "build": (mean("build_ms"), nR * 16, "ht_build16_kernel", 1),
-            "probe": (mean("probe_ms"), nS * 16, "probe_agg16_kernel", 1),
-        }
-    ph = {k: {"ms": round(v[0], 3), "bytes": v[1], "kernel": v[2], "launches": v[3],
-              "gbs": round(v[1] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else None,
-              "frac": round(v[1] / (v[0] / 1e3) / 1e9 / hbm, 4) if v[0] > 0 else None} for k, v in phases.items()}
-    top = max((k for k in ph if ph[k]["ms"] > 0), key=lambda k: ph[k]["ms"])
-    kernel_name = ph[top]["kernel"]
-    step_bytes = (nR + nS) * 16
-    # achieved = algorithmic bytes per launch / average launch time of the
-    # phase's kernel (equal to the phase's bytes / phase time).
-    roofline = {"bound": "hbm", "kernel": kernel_name, "phase": top, "achieved": ph[top]["gbs"], "peak": hbm,
-                "bytes_per_launch": ph[top]["bytes"] // ph[top]["launches"],
-                "ms_per_launch": round(ph[top]["ms"] / ph[top]["launches"], 4),
-                "unit": "GB/s", "frac": ph[top]["frac"], "peak_source": peak_kind, "traffic": None,
-                "phases": ph, "algorithm": int(phase[0].algorithm), "radix_bits": int(phase[0].radix_bits),
-                "passes": (2 if two_pass else 1) if radix else 0,
-                "histogram_ms": round(mean("histogram_ms"), 3) if radix else None,
-                "histogram_tuples": int(phase[0].histogram_tuples) if radix else None,
-                "step_achieved_gbs": round(step_bytes / (ms / args.steps / 1000.0) / 1e9, 1),
-                "step_frac": round(step_bytes / (ms / args.steps / 1000.0) / 1e9 / hbm, 4)}
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as f:
-            tj = json.load(f)
-        key = f"{kernel_name}@theta={args.theta}"
-        if key in tj:
-            roofline["traffic"] = tj[key]
+    roofline = join_roofline(pyg, phase, nR, nS, ms / args.steps, hbm, peak_kind, args.theta)
 
     # End to end: the same C-ABI calls with host (pinned) buffers; the
     # library copies each relation to the device inside the timed region.
@@ -370,6 +328,13 @@ def main_gpu(args):
         except Exception as ex:  # the CPU leg must not hide the GPU number
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "unavailable", "sample": str(ex)[:200]}
 
+    secondary = None
+    if world == 1 and not args.no_secondary:
+        del R, S, Rr, Sr
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        secondary = run_secondary(args, torch, pyg, ctx, local, stream)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -380,10 +345,88 @@ def main_gpu(args):
                            "l2": "inputs (19.3 GB) larger than L2; no flush needed"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clk.summary()}
+        if secondary is not None:
+            line["secondary"] = secondary
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:
         dist.destroy_process_group()
+
+
+def source_digest(files):
+    """Digest of the kernel sources a committed ncu figure was taken from."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in files:
+        with open(os.path.join(ROOT, "pythia-core_b200", "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+RADIX_SOURCES = ["radixpart.cu", "radixpart.cuh", "radixjoin.cu", "bulk.cuh"]
+
+
+def join_roofline(pyg, phase, nR, nS, step_ms, hbm, peak_kind, theta):
+    """The roofline object of the join line.
+
+    Every kernel launch is charged the workload's algorithmic bytes for the
+    units it processes: 16 B per input tuple read once (a partition pass of
+    S processes |S| tuples, the join |R| + |S|).  `frac` is that figure for
+    the dominant launch over its CUDA-event time, against the measured copy
+    bandwidth.  `kernel_bw_frac` counts the bytes the launch actually moves
+    (its reads and writes in the intermediate format), and `step_frac` the
+    whole step's algorithmic bytes, (|R| + |S|) x 16, over the step time."""
+    mean = lambda f: statistics.fmean(getattr(p, f) for p in phase)  # noqa: E731
+    mean2 = lambda f, i: statistics.fmean(getattr(p, f)[i] for p in phase)  # noqa: E731
+    radix = int(phase[0].algorithm) == pyg.JOIN_RADIX
+    two = radix and int(phase[0].radix_bits) > 9
+    launches = {}
+    if radix:
+        for side, n, packed in (("build", nR, int(phase[0].build_packed)), ("probe", nS, int(phase[0].probe_packed))):
+            e = 8 if packed else 16
+            p1 = mean2(f"{side}_pass_ms", 0)
+            moved1 = n * (16 + e)
+            launches[f"{side}_pass1"] = ("rj_partition_kernel", p1, n * 16, moved1, packed)
+            if two:
+                launches[f"{side}_pass2"] = ("rj_partition_kernel", mean2(f"{side}_pass_ms", 1), n * 16, n * 2 * e,
+                                             packed)
+        eR = 8 if int(phase[0].build_packed) else 16
+        eS = 8 if int(phase[0].probe_packed) else 16
+        launches["join"] = ("rj_join_kernel", mean("probe_ms"), (nR + nS) * 16, nR * eR + nS * eS, None)
+    else:
+        launches["build"] = ("ht_build16_kernel", mean("build_ms"), nR * 16, nR * 16, None)
+        launches["probe"] = ("probe_agg16_kernel", mean("probe_ms"), nS * 16, nS * 16, None)
+    ph = {}
+    for k, (kern, t, alg, moved, packed) in launches.items():
+        ph[k] = {"kernel": kern, "ms": round(t, 4), "algorithmic_bytes": alg, "moved_bytes": moved,
+                 "packed": packed,
+                 "achieved_gbs": round(alg / (t / 1e3) / 1e9, 1) if t > 0 else None,
+                 "frac": round(alg / (t / 1e3) / 1e9 / hbm, 4) if t > 0 else None,
+                 "kernel_bw_frac": round(moved / (t / 1e3) / 1e9 / hbm, 4) if t > 0 else None}
+    top = max((k for k in ph if ph[k]["ms"] > 0), key=lambda k: ph[k]["ms"])
+    step_bytes = (nR + nS) * 16
+    roofline = {"bound": "hbm", "kernel": ph[top]["kernel"], "launch": top, "achieved": ph[top]["achieved_gbs"],
+                "peak": hbm, "unit": "GB/s", "frac": ph[top]["frac"], "kernel_bw_frac": ph[top]["kernel_bw_frac"],
+                "peak_source": peak_kind, "bytes_per_launch": ph[top]["algorithmic_bytes"],
+                "moved_bytes_per_launch": ph[top]["moved_bytes"], "ms_per_launch": ph[top]["ms"], "traffic": None,
+                "launches": ph, "algorithm": int(phase[0].algorithm), "radix_bits": int(phase[0].radix_bits),
+                "histogram_ms": round(mean("histogram_ms"), 3) if radix else None,
+                "histogram_tuples": int(phase[0].histogram_tuples) if radix else None,
+                "step_achieved_gbs": round(step_bytes / (step_ms / 1e3) / 1e9, 1),
+                "step_frac": round(step_bytes / (step_ms / 1e3) / 1e9 / hbm, 4)}
+    # DRAM traffic of the dominant launch from an ncu capture of the same
+    # kernel sources (scaled to this launch's tuples); none if the sources
+    # changed since the capture.
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if radix and os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        ent = tj.get(f"{top}@theta={theta}")
+        if ent and ent.get("sources") == source_digest(RADIX_SOURCES):
+            roofline["traffic"] = ent["bytes_per_tuple"] * (nR + nS if top == "join" else
+                                                           (nR if top.startswith("build") else nS))
+            roofline["traffic_source"] = ent.get("profile")
+    return roofline
 
 
 def run_e2e(args, torch, pyg, ctx, R, S, nR, nS, world, dist):
@@ -491,6 +534,16 @@ def main_workload(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     ctx = pyg.Ctx(local)
     stream = torch.cuda.current_stream(local)
+    line = workload_line(args, torch, pyg, ctx, rank, world, local, dist, stream)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def workload_line(args, torch, pyg, ctx, rank, world, local, dist, stream):
+    """Measures one of the other configurations and returns its JSON line."""
     hbm, peak_kind = peaks()
     sh = args.scale_shift
     g = torch.Generator(device="cuda")
@@ -637,20 +690,55 @@ def main_workload(args):
         extra["plain_launches_ms_per_step"] = round(plain_ms / max(1, args.steps // 2), 4)
         ctx.batch_free(b)
     achieved = abytes / (step_ms / 1e3) / 1e9
-    if rank == 0:
-        line = {"metric": metric, "value": units * args.steps * world / (ms / 1e3), "unit": UNIT, "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded, device-generated)",
-                "config": dict(workload, parallelism=f"replicas{world}", scale_shift=sh),
-                "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                             "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": None,
-                             "algorithmic_bytes_per_step": abytes, "scope": "whole step"},
-                "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches, "clocks": clk.summary()}
-        line.update(extra)
-        print(json.dumps(line), flush=True)
-    ctx.close()
-    if dist:
-        dist.destroy_process_group()
+    line = {"metric": metric, "value": units * args.steps * world / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded, device-generated)",
+            "config": dict(workload, parallelism=f"replicas{world}", scale_shift=sh),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_step": abytes, "scope": "whole step"},
+            "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches, "clocks": clk.summary()}
+    line.update(extra)
+    return line
+
+
+# Configurations measured beside the headline in the default run, with the
+# bench options that select each: the small join, group-by at three
+# cardinalities, the MPSM join with both splitters on skewed keys, and the
+# batched fragments.
+SECONDARY = [
+    ("join_small", dict(workload="join-small")),
+    ("groupby_G16", dict(workload="groupby", groups=16)),
+    ("groupby_G2p16", dict(workload="groupby", groups=1 << 16)),
+    ("groupby_G2p16_zipf", dict(workload="groupby", groups=1 << 16, zipf=True)),
+    ("mpsm_sampled_theta1", dict(workload="mpsm", splitter="sampled", theta=1.0)),
+    ("mpsm_learned_theta1", dict(workload="mpsm", splitter="learned", theta=1.0)),
+    ("batch", dict(workload="batch")),
+]
+
+
+def run_secondary(args, torch, pyg, ctx, local, stream):
+    """Each secondary configuration with 5 timed steps after 3 warm-ups, in
+    this process (rank 0 of a 1-GPU run); a compact summary of its line."""
+    out = {}
+    for name, opts in SECONDARY:
+        a = argparse.Namespace(**vars(args))
+        a.steps, a.warmup, a.no_cpu, a.scale_shift, a.theta, a.zipf = 5, 3, True, 0, 0.0, False
+        a.groups, a.splitter, a.fanout, a.algo = 1 << 16, "learned", 4096, "auto"
+        for k, v in opts.items():
+            setattr(a, k, v)
+        try:
+            line = workload_line(a, torch, pyg, ctx, 0, 1, local, None, stream)
+            out[name] = {"metric": line["metric"], "value": line["value"], "ms_per_step": line["ms_per_step"],
+                         "roofline_frac": line["roofline"]["frac"], "config": line["config"],
+                         "clocks": line["clocks"]}
+            for k in ("mpsm", "fragment_latency_ms", "plain_launches_ms_per_step"):
+                if k in line:
+                    out[name][k] = line[k]
+        except Exception as ex:  # a secondary must not hide the headline
+            out[name] = {"error": str(ex)[:300]}
+        torch.cuda.empty_cache()
+    return out
 
 
 def main():

@@ -166,6 +166,13 @@ typedef struct pyg_join_stats {
     int64_t padded_tuples;
     double histogram_ms;        /* both relations' histograms (RADIX)   */
     int64_t histogram_tuples;   /* tuples the histograms read (RADIX)   */
+    /* RADIX: each partition pass on its own (pass 2 is 0 with one pass);
+     * build_partition_ms / probe_partition_ms also hold the host round
+     * trip that lays the relation out. */
+    double build_pass_ms[2];
+    double probe_pass_ms[2];
+    int32_t build_packed;       /* 8-byte packed intermediates (RADIX)  */
+    int32_t probe_packed;
 } pyg_join_stats;
 
 int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_keys,
@@ -239,6 +246,15 @@ int pyg_partition(pyg_ctx* ctx, const pyg_rel* in, int32_t key_col, const pyg_sp
  * util/buffer.inl:119-452): orders tuples by the signed key column.
  * Stable.  out may not alias in. */
 int pyg_sort(pyg_ctx* ctx, const pyg_rel* in, int32_t key_col, void* out);
+
+/* Replaces SortLimit (operators/sortlimit.cpp:32-262, plan node
+ * `sortlimit`): the first min(limit, n) tuples of the relation in the
+ * order of the key columns (1 or 2 columns of at most 8 bytes together,
+ * lexicographic, signed), ascending when asc != 0 else descending, ties
+ * kept in input order, written to device buffer out.  *out_n receives the
+ * count; PYG_ERR_CAPACITY if it exceeds out_capacity. */
+int pyg_sortlimit(pyg_ctx* ctx, const pyg_rel* in, const int32_t* key_cols, int32_t nkeys, int32_t asc,
+                  int64_t limit, void* out, int64_t out_capacity, int64_t* out_n);
 
 /* Replaces TupleBuffer::findsmallest<KeyT> (util/buffer.inl:~300-452):
  * for each of nq query keys (device array), the index of the first tuple

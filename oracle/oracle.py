@@ -51,6 +51,8 @@ def lib():
         L.orc_sort.argtypes = [R, C.c_int, P]
         L.orc_mpsm_join.argtypes = [R, C.c_int, R, C.c_int, C.POINTER(orc_proj), C.c_int, P, I64, P, P]
         L.orc_mpsm_join.restype = I64
+        L.orc_sortlimit.argtypes = [R, P, C.c_int, C.c_int, I64, P]
+        L.orc_sortlimit.restype = I64
         L.orc_exactrange_bucket.argtypes = [I64, I64, I64, C.c_uint]
         L.orc_exactrange_min_for_bucket.argtypes = [C.c_uint, I64, I64, C.c_uint]
         L.orc_exactrange_min_for_bucket.restype = I64
@@ -170,6 +172,15 @@ def mpsm_join(R, rtypes, rk, S, stypes, sk, proj, materialize=False):
     lib().orc_mpsm_join(C.byref(_rel(R, rtypes)), rk, C.byref(_rel(S, stypes)), sk, _projs(proj), len(proj),
                         out.ctypes.data, cnt.value, None, None)
     return out
+
+
+def sortlimit(A, types, by, asc, limit):
+    """The first `limit` tuples of A in SortLimit order (stable)."""
+    b = (C.c_int * max(1, len(by)))(*by)
+    out = np.zeros(max(0, min(limit, A.shape[0])), dtype=A.dtype)
+    n = lib().orc_sortlimit(C.byref(_rel(A, types)), b, len(by), int(bool(asc)), limit,
+                            out.ctypes.data if out.shape[0] else None)
+    return out[:n]
 
 
 def exactrange_bucket(v, mn, mx, k):

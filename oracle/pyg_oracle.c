@@ -401,3 +401,43 @@ int64_t orc_mpsm_join(const orc_rel* R, int rk, const orc_rel* S, int sk,
     free(Rs); free(Ss);
     return n;
 }
+
+/* SortLimit (operators/sortlimit.cpp:32-120 init, :131-203 sortHelper,
+ * :220-262 scanStart): a list of at most `limit` tuples kept in order.  A
+ * tuple is "ahead of" another when it is lexicographically smaller over
+ * the `by` columns (greater when asc == 0), the first column deciding
+ * unless equal (the allpossible comparator chains, :56-75).  Each arriving
+ * tuple walks the list from the head and goes before the first tuple it is
+ * ahead of (after all tuples it ties with); when the list is full, the tail
+ * drops off, and a tuple that is ahead of none is discarded.  Tuples arrive
+ * in input order (the operator runs on thread 0 only, :224-228).  Output:
+ * the list from the head, min(limit, n) tuples written to out; returns that
+ * count.  The list is held as an index array (insertion by shifting). */
+static int orc_ahead(const orc_rel* r, int64_t a, int64_t b, const int* by, int nby, int asc)
+{
+    for (int c = 0; c < nby; ++c) {
+        const int64_t x = getcol(r, a, by[c]), y = getcol(r, b, by[c]);
+        if (x == y) continue;
+        return asc ? x < y : x > y;
+    }
+    return 0;
+}
+
+int64_t orc_sortlimit(const orc_rel* in, const int* by, int nby, int asc, int64_t limit, uint8_t* out)
+{
+    if (limit <= 0) return 0;
+    int64_t* list = (int64_t*)malloc(sizeof(int64_t) * (size_t)(limit + 1));
+    int64_t size = 0;
+    for (int64_t i = 0; i < in->ntuples; ++i) {
+        int64_t pos = 0;
+        while (pos < size && !orc_ahead(in, i, list[pos], by, nby, asc)) ++pos;
+        if (pos == size && size == limit) continue;  /* ahead of none while full */
+        memmove(list + pos + 1, list + pos, sizeof(int64_t) * (size_t)(size - pos));
+        list[pos] = i;
+        if (size < limit) ++size;                   /* else the tail dropped off */
+    }
+    for (int64_t j = 0; j < size; ++j)
+        memcpy(out + (size_t)j * in->tuple_bytes, in->base + (size_t)list[j] * in->tuple_bytes, in->tuple_bytes);
+    free(list);
+    return size;
+}

@@ -132,6 +132,15 @@ def plan_partition(T, files, types, attr, mn, mx, maxtuples):
             + "treeroot: " + _tree("merge", "tid", "part", leaf='{ name: "scan"; }') + ";\n")
 
 
+def plan_sortlimit(files, types, by, asc, limit):
+    """scan -> sortlimit as the root: SortLimit runs on thread 0 only
+    (operators/sortlimit.cpp:224-228), so the plan has no merge above it."""
+    cols = ", ".join(f'"${c}"' for c in by)
+    return (header() + scan_node("scan", files, types)
+            + f'top: {{ type = "sortlimit"; by = ({cols}); asc = [{asc}]; limit = [{limit}]; }};\n'
+            + 'treeroot: { name: "top"; input: { name: "scan"; }; };\n')
+
+
 def plan_mpsm(T, rfiles, rtypes, sfiles, stypes, proj, mn, mx, maxb, maxp):
     """partition(build, exactrange) -> mpsmjoin(buildprepartitioned) -> merge
     (unit_tests/querypartitionedmpsmpkfkjoin.cpp)."""

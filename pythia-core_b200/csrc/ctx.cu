@@ -209,6 +209,7 @@ int pyg_ctx_destroy(pyg_ctx* ctx)
         cudaEventDestroy(ctx->consumed[i]);
     }
     cudaStreamDestroy(ctx->copy_stream);
+    if (ctx->join_arena) cudaFree(ctx->join_arena);  // synchronous: the caller's stream may be gone
     cudaFree(ctx->dcounters);
     cudaFreeHost(ctx->pinned);
     cudaStreamDestroy(ctx->own_stream);

@@ -244,8 +244,19 @@ __global__ void __launch_bounds__(256, PYG_PROBE_MIN_BLOCKS) probe_agg16_kernel(
                                                           const ulonglong2* __restrict__ slots, uint64_t cap,
                                                           const unsigned long long* __restrict__ counts,
                                                           const uint64_t* __restrict__ side, int64_t nside,
-                                                          unsigned long long* __restrict__ out)
+                                                          unsigned long long* __restrict__ out,
+                                                          const unsigned long long* __restrict__ gate,
+                                                          int64_t side_cap)
 {
+    // gate (optional): the build's flags, read here instead of on the host.
+    // A build with repeated keys (no count array), a full table or more
+    // empty-marker keys than the side list holds is probed again by the
+    // general path, so this launch does nothing.
+    if (gate) {
+        const unsigned long long dup = gate[0], full = gate[1], ns = gate[2];
+        if (dup | full || ns > (unsigned long long)side_cap) return;
+        nside = (int64_t)ns;
+    }
     uint64_t cnt = 0, bsum = 0, psum = 0;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t base = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -524,10 +535,12 @@ static int launch_probe16(pyg_ctx* ctx, const pyg_hashtable* ht, const longlong2
     int grid = grid_for(ctx, n, threads, U, 8);
     if (fillers)
         probe_agg16_kernel<U, true><<<grid, threads, 0, ctx->stream>>>(S, n, (const ulonglong2*)ht->slots, ht->cap,
-                                                                       ht->counts, ht->side, ht->nside, acc);
+                                                                       ht->counts, ht->side, ht->nside, acc, nullptr,
+                                                                       0);
     else
         probe_agg16_kernel<U, false><<<grid, threads, 0, ctx->stream>>>(S, n, (const ulonglong2*)ht->slots, ht->cap,
-                                                                        ht->counts, ht->side, ht->nside, acc);
+                                                                        ht->counts, ht->side, ht->nside, acc, nullptr,
+                                                                        0);
     PYG_LAUNCHED(ctx);
     return PYG_OK;
 }
@@ -596,6 +609,86 @@ struct PhaseTimer {
         for (auto& e : ev) cudaEventDestroy(e);
     }
 };
+
+// Empty table of cap 16-byte slots and nwords zeroed counter words.
+__global__ void dj_clear_kernel(ulonglong2* __restrict__ slots, uint64_t cap, unsigned long long* __restrict__ words,
+                                int nwords)
+{
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < (uint64_t)nwords) words[i] = 0;
+    for (; i < cap; i += (uint64_t)gridDim.x * blockDim.x) slots[i] = make_ulonglong2(kEmptyKey, 0ULL);
+}
+
+// One-shot join + sum of 16-byte (int64 key @0, int64 payload @8) device
+// relations through one table in HBM (L2-resident for build sides up to a
+// few million tuples): clear, build, probe as three launches, one copy of
+// the counter words and one host synchronisation.  The table and its side
+// list live in the context's grow-only arena, so a call allocates nothing
+// once the arena is large enough.  The probe reads the build's flags on
+// the device; when the build side repeated a key, filled the table or had
+// more empty-marker keys than the side list holds, the probe does nothing,
+// *fallback is set and the caller takes the general path.
+// res = {count, build payload sum, probe payload sum}.
+static int direct_join16(pyg_ctx* ctx, const longlong2* R, int64_t nR, const longlong2* S, int64_t nS, float lf,
+                         unsigned long long res[3], bool* fallback, PhaseTimer* tm)
+{
+    *fallback = false;
+    uint64_t cap = (uint64_t)((double)nR / (double)lf) + 1;
+    if (cap < 64) cap = 64;
+    const int64_t side_cap = nR < 1024 ? (nR > 0 ? nR : 1) : 1024;
+    const size_t need = (size_t)cap * 16 + (size_t)side_cap * 16;
+    if (ctx->join_arena_bytes < need) {
+        dfree(ctx, ctx->join_arena);
+        ctx->join_arena = nullptr;
+        ctx->join_arena_bytes = 0;
+        int rc = dalloc(ctx, &ctx->join_arena, need);
+        if (rc) return rc;
+        ctx->join_arena_bytes = need;
+    }
+    ulonglong2* slots = (ulonglong2*)ctx->join_arena;
+    uint64_t* side = (uint64_t*)(slots + cap);
+    unsigned long long* words = ctx->dcounters;  // [0..3] build flags, [8..10] probe sums
+    const int threads = 256;
+    dj_clear_kernel<<<grid_for(ctx, (int64_t)cap, threads, 4, 8), threads, 0, ctx->stream>>>(slots, cap, words, 11);
+    PYG_LAUNCHED(ctx);
+    BuildArgs a;
+    memset(&a, 0, sizeof(a));
+    a.base = (const uint8_t*)R;
+    a.n = nR;
+    a.tb = 16;
+    a.slots = (uint64_t*)slots;
+    a.cap = cap;
+    a.W = 2;
+    a.agg = 1;
+    a.side = side;
+    a.side_cap = side_cap;
+    a.flags = words;
+    tm->mark(ctx, 1);
+    if (nR > 0) {
+        ht_build16_kernel<4><<<grid_for(ctx, nR, threads, 4, 8), threads, 0, ctx->stream>>>(a);
+        PYG_LAUNCHED(ctx);
+    }
+    tm->mark(ctx, 2);
+    tm->mark(ctx, 3);
+    if (nS > 0) {
+        constexpr int U = PYG_PROBE_UNROLL;
+        probe_agg16_kernel<U, false><<<grid_for(ctx, nS, threads, U, 8), threads, 0, ctx->stream>>>(
+            S, nS, slots, cap, nullptr, side, 0, words + 8, words, side_cap);
+        PYG_LAUNCHED(ctx);
+    }
+    tm->mark(ctx, 4);
+    unsigned long long* h = (unsigned long long*)ctx->pinned;
+    PYG_CUDA(cudaMemcpyAsync(h, words, 11 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+    PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (h[0] || h[1] || h[2] > (unsigned long long)side_cap) {
+        *fallback = true;
+        return PYG_OK;
+    }
+    res[0] = h[8];
+    res[1] = h[9];
+    res[2] = h[10];
+    return PYG_OK;
+}
 
 }  // namespace pyg
 
@@ -889,6 +982,28 @@ int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_ke
     bool radix = eligible && (algorithm == PYG_JOIN_RADIX ||
                               (algorithm == PYG_JOIN_AUTO && probe->ntuples >= ((int64_t)1 << 24)));
     PhaseTimer tm;
+    if (!radix && eligible) {
+        // 16-byte device relations: the one-shot direct join (falls back
+        // to the general path below on repeated build keys).
+        tm.start(ctx, stats != nullptr);
+        unsigned long long r3[3];
+        bool fallback = false;
+        if ((rc = direct_join16(ctx, (const longlong2*)build->base, build->ntuples, (const longlong2*)probe->base,
+                                probe->ntuples, lf, r3, &fallback, &tm)))
+            return rc;
+        if (!fallback) {
+            memset(out, 0, sizeof(*out));
+            out->count = (int64_t)r3[0];
+            for (int p = 0; p < nproj; ++p) out->sums[p] = (int64_t)(proj[p].side ? r3[2] : r3[1]);
+            if (stats) {
+                tm.finish(stats);
+                stats->algorithm = PYG_JOIN_DIRECT;
+            }
+            return PYG_OK;
+        }
+        if (stats) tm.finish(stats);
+        tm = PhaseTimer();
+    }
     if (!radix) {
         tm.start(ctx, stats != nullptr);
         pyg_hashtable* ht = nullptr;

@@ -27,6 +27,11 @@ struct pyg_ctx {
     // kernels when an input relation lives in host memory.
     cudaStream_t copy_stream;
     cudaEvent_t copied[2], consumed[2];
+    // Grow-only device buffer reused by the one-shot direct join for its
+    // table and side list (no allocation per call once it is large enough;
+    // freed with the context).
+    void* join_arena;
+    size_t join_arena_bytes;
 };
 
 namespace pyg {

@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "pyg_internal.cuh"
@@ -73,14 +74,44 @@ struct RJItem {
 };
 
 struct RJJoinArgs {
-    const longlong2* R;
-    const longlong2* S;
+    const void* R;              // 16-byte tuples, or packed words when RP
+    const void* S;              // 16-byte tuples, or packed words when SP
     const RJItem* items;
     long long nitems;
     unsigned* next;             // work queue head, zeroed
     int fine_bits;              // the table's slot uses the hash bits below these
     unsigned long long* acc;    // count, build sum, probe sum
     unsigned* dup;              // set when a build key repeats (UNIQUE)
+    unsigned long long rk, rp;  // frame of packed build words: key = rk + low half, payload = rp + high half
+    unsigned long long sk, sp;  // frame of packed probe words
+};
+
+// Tuple i of a partitioned relation as (key, payload).
+template <bool PACKED>
+__device__ __forceinline__ longlong2 rj_tuple(const void* base, unsigned long long i, unsigned long long kb,
+                                              unsigned long long pb)
+{
+    if constexpr (PACKED) {
+        const unsigned long long w = reinterpret_cast<const unsigned long long*>(base)[i];
+        return make_longlong2((long long)(kb + (w & 0xFFFFFFFFULL)), (long long)(pb + (w >> 32)));
+    } else {
+        return reinterpret_cast<const longlong2*>(base)[i];
+    }
+}
+
+// Streaming load of a probe element and its decoding.
+template <bool PACKED>
+struct RJProbeElem {
+    using T = typename std::conditional<PACKED, unsigned long long, longlong2>::type;
+    static __device__ __forceinline__ T load(const void* base, unsigned long long i)
+    {
+        return __ldcs(reinterpret_cast<const T*>(base) + i);
+    }
+    static __device__ __forceinline__ longlong2 decode(const T& e, unsigned long long kb, unsigned long long pb)
+    {
+        if constexpr (PACKED) return make_longlong2((long long)(kb + (e & 0xFFFFFFFFULL)), (long long)(pb + (e >> 32)));
+        else return e;
+    }
 };
 
 // Warms L2 with [p, p + bytes) (16-byte aligned start; bytes rounded down
@@ -94,12 +125,15 @@ __device__ __forceinline__ void rj_prefetch_l2(const void* p, unsigned long long
                  : "memory");
 }
 
-template <bool UNIQUE>
+template <bool UNIQUE, bool RP, bool SP>
 __global__ void __launch_bounds__(RJ_JOIN_THREADS, RJ_JOIN_BLOCKS) rj_join_kernel(RJJoinArgs a)
 {
     extern __shared__ __align__(16) unsigned char rj_table[];
     constexpr unsigned TS = UNIQUE ? RJ_SLOTS_UNIQUE : RJ_SLOTS_COUNTED;
-    constexpr int U = RJ_PROBE_UNROLL;
+    // Probe elements in flight per thread: the same bytes for 8-byte words.
+    constexpr int U = SP ? 2 * RJ_PROBE_UNROLL : RJ_PROBE_UNROLL;
+    constexpr unsigned RB = RP ? 8 : 16, SB = SP ? 8 : 16;  // bytes per build / probe element
+    using PE = RJProbeElem<SP>;
     __shared__ long long item_cur, item_next;
     __shared__ unsigned long long side_cnt, side_sum;
     ulonglong2* T2 = reinterpret_cast<ulonglong2*>(rj_table);  // UNIQUE slots
@@ -119,8 +153,8 @@ __global__ void __launch_bounds__(RJ_JOIN_THREADS, RJ_JOIN_BLOCKS) rj_join_kerne
                 item_next = (long long)atomicAdd(a.next, 1u);
                 if (item_next < a.nitems) {
                     const RJItem nx = a.items[item_next];
-                    rj_prefetch_l2(a.R + nx.r0, (unsigned long long)nx.rn * 16);
-                    rj_prefetch_l2(a.S + nx.s0, (unsigned long long)min(nx.sn, 4096u) * 16);
+                    rj_prefetch_l2((const char*)a.R + nx.r0 * RB, (unsigned long long)nx.rn * RB);
+                    rj_prefetch_l2((const char*)a.S + nx.s0 * SB, (unsigned long long)min(nx.sn, 4096u) * SB);
                 }
             }
         }
@@ -135,7 +169,7 @@ __global__ void __launch_bounds__(RJ_JOIN_THREADS, RJ_JOIN_BLOCKS) rj_join_kerne
         // Build: linear probing with 64-bit shared-memory CAS.  At most
         // TS / 2 tuples per item, so a free slot always exists.
         for (unsigned i = threadIdx.x; i < item.rn; i += RJ_JOIN_THREADS) {
-            const longlong2 t = a.R[item.r0 + i];
+            const longlong2 t = rj_tuple<RP>(a.R, item.r0 + i, a.rk, a.rp);
             const uint64_t k = (uint64_t)t.x;
             if (k == kEmptyKey) {
                 atomicAdd(&side_cnt, 1ULL);
@@ -196,17 +230,17 @@ __global__ void __launch_bounds__(RJ_JOIN_THREADS, RJ_JOIN_BLOCKS) rj_join_kerne
                 pos = pos + 1 == TS ? 0 : pos + 1;
             }
         };
-        const longlong2* S = a.S + item.s0;
+        const unsigned long long s0 = item.s0;
         const unsigned sn = item.sn;
         unsigned i = threadIdx.x;
         for (; i + (U - 1) * RJ_JOIN_THREADS < sn; i += U * RJ_JOIN_THREADS) {
-            longlong2 t[U];
+            typename PE::T t[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) t[u] = __ldcs(&S[i + u * RJ_JOIN_THREADS]);
+            for (int u = 0; u < U; ++u) t[u] = PE::load(a.S, s0 + i + u * RJ_JOIN_THREADS);
 #pragma unroll
-            for (int u = 0; u < U; ++u) probe(t[u]);
+            for (int u = 0; u < U; ++u) probe(PE::decode(t[u], a.sk, a.sp));
         }
-        for (; i < sn; i += RJ_JOIN_THREADS) probe(__ldcs(&S[i]));
+        for (; i < sn; i += RJ_JOIN_THREADS) probe(PE::decode(PE::load(a.S, s0 + i), a.sk, a.sp));
     }
     cnt = warp_sum_u64(cnt);
     bsum = warp_sum_u64(bsum);
@@ -225,7 +259,9 @@ __global__ void __launch_bounds__(RJ_JOIN_THREADS, RJ_JOIN_BLOCKS) rj_join_kerne
 namespace {
 
 struct RJEvents {
-    static constexpr int N = 5;
+    // 0 start, 1 histograms, 2 / 3 build / probe passes done, 4 join done,
+    // 5 / 6 build first pass begins / ends, 7 / 8 the same for the probe side.
+    static constexpr int N = 9;
     cudaEvent_t ev[N] = {};
     bool on = false;
     void start(pyg_ctx* ctx, bool enable)
@@ -275,6 +311,15 @@ void make_items(const std::vector<unsigned long long>& hr, const std::vector<uns
     }
 }
 
+// The join kernel for the partitions' formats (16-byte tuples or packed
+// words on each side) and table kind.
+template <bool UNIQUE>
+void* join_fn(bool rp, bool sp)
+{
+    if (rp) return sp ? (void*)rj_join_kernel<UNIQUE, true, true> : (void*)rj_join_kernel<UNIQUE, true, false>;
+    return sp ? (void*)rj_join_kernel<UNIQUE, false, true> : (void*)rj_join_kernel<UNIQUE, false, false>;
+}
+
 }  // namespace
 
 int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t nS, int fine_bits,
@@ -308,18 +353,22 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
     RJItem* ditems = nullptr;
     int rc = PYG_OK;
     do {
-        // Words 202-203: per relation, [0] a bulk copy never landed, [1] region overflow.
-        unsigned* flags = (unsigned*)(ctx->dcounters + 202);
+        // Words 224-227: per relation, [0] a bulk copy never landed, [1]
+        // region overflow, [2] a tuple outside the packed frame, [3] unused.
+        unsigned* flags = (unsigned*)(ctx->dcounters + 224);
         unsigned long long* h = (unsigned long long*)ctx->pinned;
         unsigned* hflags = (unsigned*)(h + 6);
-        // 1-2. Partition both sides (histograms sampled for large inputs).
+        // 1-2. Partition both sides (histograms sampled for large inputs;
+        // intermediates packed when the key and payload ranges allow).
         RPSide side[2];
-        side[0].in = R;
-        side[0].n = nR;
-        side[0].done = tm.on ? tm.ev[2] : nullptr;
-        side[1].in = S;
-        side[1].n = nS;
-        side[1].done = tm.on ? tm.ev[3] : nullptr;
+        for (int s = 0; s < 2; ++s) {
+            side[s].in = s ? S : R;
+            side[s].n = s ? nS : nR;
+            side[s].allow_pack = true;
+            side[s].begin = tm.on ? tm.ev[5 + 2 * s] : nullptr;
+            side[s].mid = tm.on ? tm.ev[6 + 2 * s] : nullptr;
+            side[s].done = tm.on ? tm.ev[2 + s] : nullptr;
+        }
         rc = rp_partition_sides(ctx, side, 2, FB, two, flags, hflags, tm.on ? tm.ev[1] : nullptr);
         R1 = side[0].P1;
         R2 = side[0].P2;
@@ -331,8 +380,6 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
 
         // 3. Join: distinct build keys first (16-byte slots); on a repeated
         // key, again with counted 32-byte slots and smaller build chunks.
-        const longlong2* Rf = (const longlong2*)(two ? R2 : R1);
-        const longlong2* Sf = (const longlong2*)(two ? S2 : S1);
         unsigned long long* acc = ctx->dcounters + 8;
         unsigned* next = (unsigned*)(ctx->dcounters + 200);  // word 200: queue head, word 201: dup flag
         unsigned* dupf = (unsigned*)(ctx->dcounters + 201);
@@ -348,22 +395,26 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
             if ((rc = dalloc(ctx, (void**)&ditems, items.size() * sizeof(RJItem)))) break;
             PYG_CUDA(cudaMemcpyAsync(ditems, items.data(), items.size() * sizeof(RJItem), cudaMemcpyHostToDevice,
                                      ctx->stream));
-            void* fn = unique ? (void*)rj_join_kernel<true> : (void*)rj_join_kernel<false>;
+            void* fn = unique ? join_fn<true>(LR.packed, LS.packed) : join_fn<false>(LR.packed, LS.packed);
             PYG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, RJ_TABLE_BYTES));
             PYG_CUDA(cudaMemsetAsync(acc, 0, 3 * 8, ctx->stream));
             PYG_CUDA(cudaMemsetAsync(next, 0, 16, ctx->stream));
             RJJoinArgs ja;
-            ja.R = Rf;
-            ja.S = Sf;
+            ja.R = two ? R2 : R1;
+            ja.S = two ? S2 : S1;
             ja.items = ditems;
             ja.nitems = (long long)items.size();
             ja.next = next;
             ja.fine_bits = FB;
             ja.acc = acc;
             ja.dup = dupf;
+            ja.rk = LR.kbase;
+            ja.rp = LR.pbase;
+            ja.sk = LS.kbase;
+            ja.sp = LS.pbase;
             const unsigned grid = (unsigned)std::min<long long>((long long)ctx->sm_count * RJ_JOIN_BLOCKS, ja.nitems);
-            if (unique) rj_join_kernel<true><<<grid, RJ_JOIN_THREADS, RJ_TABLE_BYTES, ctx->stream>>>(ja);
-            else rj_join_kernel<false><<<grid, RJ_JOIN_THREADS, RJ_TABLE_BYTES, ctx->stream>>>(ja);
+            void* args[] = {&ja};
+            PYG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(RJ_JOIN_THREADS), args, RJ_TABLE_BYTES, ctx->stream));
             PYG_LAUNCHED(ctx);
             PYG_CUDA(cudaMemcpyAsync(h, acc, 3 * 8, cudaMemcpyDeviceToHost, ctx->stream));
             PYG_CUDA(cudaMemcpyAsync(h + 3, next, 16, cudaMemcpyDeviceToHost, ctx->stream));
@@ -386,6 +437,19 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
             stats->build_ms = 0;
             stats->probe_partition_ms = tm.ms(2, 3);
             stats->probe_ms = tm.ms(3, 4);
+            for (int s = 0; s < 2; ++s) {
+                double* pm = s ? stats->probe_pass_ms : stats->build_pass_ms;
+                pm[0] = pm[1] = 0;
+                if (!side[s].begin) continue;  // the relation was redone: no per-pass times
+                if (two) {
+                    pm[0] = tm.ms(5 + 2 * s, 6 + 2 * s);
+                    pm[1] = tm.ms(6 + 2 * s, 2 + s);
+                } else {
+                    pm[0] = tm.ms(5 + 2 * s, 2 + s);
+                }
+            }
+            stats->build_packed = LR.packed ? 1 : 0;
+            stats->probe_packed = LS.packed ? 1 : 0;
             stats->padded_tuples = (int64_t)((LR.p2 + LS.p2) - (unsigned long long)(nR + nS));
             stats->overflow_tuples = (side[0].overflowed ? 1 : 0) + (side[1].overflowed ? 1 : 0);
         }

@@ -5,7 +5,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "bulk.cuh"
@@ -34,22 +36,31 @@ __device__ __forceinline__ unsigned rj_bin(uint64_t h, int shift, unsigned mask)
 // counters per CTA).
 
 __global__ void __launch_bounds__(1024) rj_hist_kernel(const longlong2* __restrict__ in, int64_t n, int64_t step,
-                                                       int bits, int base, int span, unsigned* __restrict__ part)
+                                                       int bits, int base, int span, unsigned* __restrict__ part,
+                                                       long long* __restrict__ mm)
 {
     // Counts the bins [base, base + span) of in[0], in[step], in[2 step],
     // ... (step 1: every tuple); span 32-bit counters in shared memory,
     // stored to this CTA's row of part (rj_hist_sum_kernel adds the rows).
+    // With mm: also the key and payload ranges of the tuples read.
     extern __shared__ unsigned rj_sh_hist[];
+    __shared__ long long sh_mm[4];
     const int P = 1 << bits;
     const int shift = 64 - bits;
     const int64_t m = (n + step - 1) / step;
     for (int b = threadIdx.x; b < span; b += blockDim.x) rj_sh_hist[b] = 0;
+    if (threadIdx.x < 4) sh_mm[threadIdx.x] = (threadIdx.x & 1) ? LLONG_MIN : LLONG_MAX;
     __syncthreads();
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    auto count = [&](long long k) {
-        const unsigned r = rj_bin(rj_hash((uint64_t)k), shift, P - 1) - (unsigned)base;
+    long long kmin = LLONG_MAX, kmax = LLONG_MIN, pmin = LLONG_MAX, pmax = LLONG_MIN;
+    auto count = [&](const longlong2 t) {
+        const unsigned r = rj_bin(rj_hash((uint64_t)t.x), shift, P - 1) - (unsigned)base;
         if (r < (unsigned)span) atomicAdd(&rj_sh_hist[r], 1u);
+        kmin = min(kmin, t.x);
+        kmax = max(kmax, t.x);
+        pmin = min(pmin, t.y);
+        pmax = max(pmax, t.y);
     };
     constexpr int U = 8;
     for (; i + (U - 1) * stride < m; i += U * stride) {
@@ -57,12 +68,39 @@ __global__ void __launch_bounds__(1024) rj_hist_kernel(const longlong2* __restri
 #pragma unroll
         for (int u = 0; u < U; ++u) t[u] = __ldcs(&in[(i + u * stride) * step]);
 #pragma unroll
-        for (int u = 0; u < U; ++u) count(t[u].x);
+        for (int u = 0; u < U; ++u) count(t[u]);
     }
-    for (; i < m; i += stride) count(__ldcs(&in[i * step]).x);
+    for (; i < m; i += stride) count(__ldcs(&in[i * step]));
+    if (mm) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+            kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+            pmin = min(pmin, __shfl_xor_sync(0xffffffffu, pmin, o));
+            pmax = max(pmax, __shfl_xor_sync(0xffffffffu, pmax, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&sh_mm[0], kmin);
+            atomicMax(&sh_mm[1], kmax);
+            atomicMin(&sh_mm[2], pmin);
+            atomicMax(&sh_mm[3], pmax);
+        }
+    }
     __syncthreads();
     unsigned* row = part + (size_t)blockIdx.x * span;
     for (int b = threadIdx.x; b < span; b += blockDim.x) row[b] = rj_sh_hist[b];
+    if (mm && threadIdx.x == 0) {
+        atomicMin(&mm[0], sh_mm[0]);
+        atomicMax(&mm[1], sh_mm[1]);
+        atomicMin(&mm[2], sh_mm[2]);
+        atomicMax(&mm[3], sh_mm[3]);
+    }
+}
+
+// mm = {LLONG_MAX, LLONG_MIN, LLONG_MAX, LLONG_MIN}: empty key / payload ranges.
+__global__ void rj_mm_init_kernel(long long* mm)
+{
+    if (threadIdx.x < 4) mm[threadIdx.x] = (threadIdx.x & 1) ? LLONG_MIN : LLONG_MAX;
 }
 
 // hist[b] = sum over the nrow rows of part[row * span + b], b < span: the
@@ -78,12 +116,12 @@ __global__ void rj_hist_sum_kernel(const unsigned* __restrict__ part, int nrow, 
     hist[b] = sum;
 }
 
-// Tiles per segment, as an exclusive prefix (one thread; at most 2^8
-// segments): tiles[C] is the pass's tile count.  Counts are first clamped
-// to their region's capacity, so a region that overflowed (its result is
-// discarded and redone) is never read past its end.
+// Tiles of `tile` elements per segment, as an exclusive prefix (one thread;
+// at most 2^8 segments): tiles[C] is the pass's tile count.  Counts are
+// first clamped to their region's capacity, so a region that overflowed
+// (its result is discarded and redone) is never read past its end.
 __global__ void rj_tile_prefix_kernel(unsigned long long* __restrict__ count, const unsigned long long* __restrict__ cap,
-                                      int C, unsigned long long* __restrict__ tiles)
+                                      int C, int tile, unsigned long long* __restrict__ tiles)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     unsigned long long t = 0;
@@ -91,7 +129,7 @@ __global__ void rj_tile_prefix_kernel(unsigned long long* __restrict__ count, co
     for (int c = 0; c < C; ++c) {
         const unsigned long long n = count[c] < cap[c] ? count[c] : cap[c];
         count[c] = n;
-        t += (n + RJ_TILE - 1) / RJ_TILE;
+        t += (n + tile - 1) / tile;
         tiles[c + 1] = t;
     }
 }
@@ -123,13 +161,36 @@ struct RJPass {
     // segment's nsplit splitters, split + seg * 2^lbits (one segment: split).
     const long long* split;
     int nsplit;
+    // Packed elements: frame of the 8-byte words, and the flag set when a
+    // 16-byte input tuple falls outside it.
+    unsigned long long kbase, pbase;
+    unsigned* frame;
 };
+
+// Element formats: a pass reads 16-byte tuples (the relation, or unpacked
+// intermediates) or packed 8-byte words, and writes either.  Packed input
+// tiles hold 4096 words (bins of at most 2^8, so the staged bin index is
+// one byte); 16-byte tiles hold 2048 tuples.  Both fit two CTAs per SM.
+template <bool IN8, bool OUT8>
+struct RJFmt {
+    using In = typename std::conditional<IN8, unsigned long long, longlong2>::type;
+    using Out = typename std::conditional<OUT8, unsigned long long, longlong2>::type;
+    using Bin = typename std::conditional<IN8, unsigned char, unsigned short>::type;
+    static constexpr int TILE = IN8 ? RJ_TILE8 : RJ_TILE;
+};
+
+__device__ __forceinline__ long long rj_key(const longlong2& t, unsigned long long) { return t.x; }
+__device__ __forceinline__ long long rj_key(unsigned long long w, unsigned long long kbase)
+{
+    return (long long)(kbase + (w & 0xFFFFFFFFULL));
+}
 
 struct RJTileRange {
     long long begin, end;
     int seg;
 };
 
+template <int TILE>
 __device__ RJTileRange rj_tile_range(const RJPass& a, long long tile)
 {
     int lo = 0, hi = a.nseg;  // seg_tile0[lo] <= tile < seg_tile0[hi]
@@ -140,20 +201,22 @@ __device__ RJTileRange rj_tile_range(const RJPass& a, long long tile)
     }
     RJTileRange r;
     r.seg = lo;
-    r.begin = (long long)a.seg_start[lo] + (tile - (long long)a.seg_tile0[lo]) * RJ_TILE;
+    r.begin = (long long)a.seg_start[lo] + (tile - (long long)a.seg_tile0[lo]) * TILE;
     const long long seg_end =
         a.seg_count ? (long long)a.seg_start[lo] + (long long)a.seg_count[lo] : (long long)a.seg_start[lo + 1];
-    r.end = min(r.begin + RJ_TILE, seg_end);
+    r.end = min(r.begin + TILE, seg_end);
     return r;
 }
 
 // Shared memory of one partition CTA: a ring of RJ_STAGES input tiles that
 // bulk copies fill ahead of use, the grouped (staged) tile, and per-bin
 // counters.
+template <bool IN8, bool OUT8>
 struct RJPartSmem {
-    longlong2 in[RJ_STAGES][RJ_TILE];
-    longlong2 stage[RJ_TILE];
-    unsigned short stage_bin[RJ_TILE];
+    using F = RJFmt<IN8, OUT8>;
+    typename F::In in[RJ_STAGES][F::TILE];
+    typename F::Out stage[F::TILE];
+    typename F::Bin stage_bin[F::TILE];
     unsigned hist[RJ_LMAX];
     unsigned loff[RJ_LMAX];
     unsigned long long gdelta[RJ_LMAX];  // output position of staged slot i = gdelta[bin] + i
@@ -163,7 +226,9 @@ struct RJPartSmem {
     long long split[2][RJ_SPLIT_MAX];  // range mode: the splitters of this tile and the next
     int ok;
 };
-static_assert(2 * (sizeof(RJPartSmem) + 1024) <= 233472, "two partition CTAs per SM");
+static_assert(2 * (sizeof(RJPartSmem<false, false>) + 1024) <= 233472, "two partition CTAs per SM");
+static_assert(2 * (sizeof(RJPartSmem<false, true>) + 1024) <= 233472, "two partition CTAs per SM");
+static_assert(2 * (sizeof(RJPartSmem<true, true>) + 1024) <= 233472, "two partition CTAs per SM");
 
 __device__ __forceinline__ unsigned rj_range_bin(const long long* sp, int n, long long k)
 {
@@ -216,23 +281,33 @@ __global__ void __launch_bounds__(1024) rj_hist_range_kernel(const longlong2* __
 }
 
 // Thread 0: starts the bulk copy of tile `tile` into ring slot `slot`.
-__device__ __forceinline__ void rj_issue_tile(const RJPass& a, RJPartSmem& sm, int slot, long long tile)
+// Packed tiles start at an even word (regions and tiles are even), and the
+// copy is rounded up to 16 bytes: at most one word past the tile, inside
+// the buffer's 16-byte tail, which is never used as data.
+template <bool IN8, bool OUT8>
+__device__ __forceinline__ void rj_issue_tile(const RJPass& a, RJPartSmem<IN8, OUT8>& sm, int slot, long long tile)
 {
-    const RJTileRange r = rj_tile_range(a, tile);
+    using F = RJFmt<IN8, OUT8>;
+    const RJTileRange r = rj_tile_range<F::TILE>(a, tile);
     sm.info[slot] = r;
-    const unsigned bytes = (unsigned)(r.end - r.begin) * 16u;
+    const unsigned bytes = ((unsigned)(r.end - r.begin) * (unsigned)sizeof(typename F::In) + 15u) & ~15u;
     mbar_arrive_expect_tx(&sm.bar[slot], bytes);
-    bulk_load(sm.in[slot], a.in + r.begin, bytes, &sm.bar[slot]);
+    bulk_load(sm.in[slot], reinterpret_cast<const typename F::In*>(a.in) + r.begin, bytes, &sm.bar[slot]);
 }
 
+template <bool IN8, bool OUT8>
 __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_kernel(RJPass a, long long ntiles)
 {
+    using F = RJFmt<IN8, OUT8>;
+    using Out = typename F::Out;
     if (a.ntiles_dev) ntiles = (long long)*a.ntiles_dev;
     extern __shared__ __align__(128) unsigned char rj_pt_raw[];
-    RJPartSmem& sm = *reinterpret_cast<RJPartSmem*>(rj_pt_raw);
-    constexpr int PER = RJ_TILE / RJ_PT_THREADS;
+    RJPartSmem<IN8, OUT8>& sm = *reinterpret_cast<RJPartSmem<IN8, OUT8>*>(rj_pt_raw);
+    constexpr int PER = F::TILE / RJ_PT_THREADS;
     const int L = 1 << a.lbits;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    Out* out = reinterpret_cast<Out*>(a.out);
+    bool miss = false;  // a 16-byte tuple outside the packed frame
     for (int b = tid; b < RJ_LMAX; b += RJ_PT_THREADS) sm.hist[b] = 0;
     if (tid == 0) {
         for (int s = 0; s < RJ_STAGES; ++s) mbar_init(&sm.bar[s], 1);
@@ -258,7 +333,7 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
         const RJTileRange cur = sm.info[slot];
         const unsigned n = (unsigned)(cur.end - cur.begin);
         // (1) Bin and rank every tuple; one shared atomic per (warp, bin).
-        longlong2 t[PER];
+        Out t[PER];
         unsigned bin[PER], rank[PER];
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
@@ -266,9 +341,19 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
             const bool valid = landed && i < n;
             bin[j] = 0xFFFFFFFFu;
             if (valid) {
-                t[j] = sm.in[slot][i];
-                bin[j] = a.nsplit ? rj_range_bin(sm.split[a.nseg > 1 ? (k & 1) : 0], a.nsplit, t[j].x)
-                                  : rj_bin(rj_hash((uint64_t)t[j].x), a.shift, a.mask);
+                const typename F::In e = sm.in[slot][i];
+                const long long key = rj_key(e, a.kbase);
+                if constexpr (IN8 || !OUT8) {
+                    t[j] = e;
+                } else {
+                    // Pack: (key - kbase) | (payload - pbase) << 32.
+                    const unsigned long long dk = (unsigned long long)e.x - a.kbase;
+                    const unsigned long long dp = (unsigned long long)e.y - a.pbase;
+                    miss |= ((dk | dp) >> 32) != 0;
+                    t[j] = (dk & 0xFFFFFFFFULL) | (dp << 32);
+                }
+                bin[j] = a.nsplit ? rj_range_bin(sm.split[a.nseg > 1 ? (k & 1) : 0], a.nsplit, key)
+                                  : rj_bin(rj_hash((uint64_t)key), a.shift, a.mask);
             }
             // Skewed keys put many lanes of a warp into one bin: when at
             // least 8 lanes share lane 0's bin, they take their ranks from
@@ -329,7 +414,7 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
             if (bin[j] != 0xFFFFFFFFu) {
                 const unsigned s = sm.loff[bin[j]] + rank[j];
                 sm.stage[s] = t[j];
-                sm.stage_bin[s] = (unsigned short)bin[j];
+                sm.stage_bin[s] = (typename F::Bin)bin[j];
             }
         // Range mode over several segments: the next tile's splitters
         // (its copy was issued a tile ago, so its segment is known).
@@ -355,28 +440,40 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
         // (4) Write each bin's run contiguously.
         for (unsigned i = tid; i < total; i += RJ_PT_THREADS) {
             const unsigned long long gd = sm.gdelta[sm.stage_bin[i]];
-            if (gd != kSkipRun) __stcs(&a.out[gd + i], sm.stage[i]);
+            if (gd != kSkipRun) __stcs(&out[gd + i], sm.stage[i]);
         }
     }
     __syncthreads();
     if (tid == 0 && !sm.ok) atomicOr(a.err, 1u);
+    if (miss) atomicOr(a.frame, 1u);
 }
 
 
 namespace {
 
-int launch_pass(pyg_ctx* ctx, const RJPass& p, long long ntiles)
+template <bool IN8, bool OUT8>
+int launch_pass_t(pyg_ctx* ctx, const RJPass& p, long long ntiles)
 {
-    if (ntiles <= 0) return PYG_OK;
-    const size_t smem = sizeof(RJPartSmem);
-    PYG_CUDA(cudaFuncSetAttribute(rj_partition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    auto fn = rj_partition_kernel<IN8, OUT8>;
+    const size_t smem = sizeof(RJPartSmem<IN8, OUT8>);
+    PYG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rj_partition_kernel, RJ_PT_THREADS, smem));
+    PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, RJ_PT_THREADS, smem));
     if (per_sm < 1) per_sm = 1;
     long long grid = std::min<long long>(ntiles, (long long)ctx->sm_count * per_sm);
-    rj_partition_kernel<<<(unsigned)grid, RJ_PT_THREADS, smem, ctx->stream>>>(p, ntiles);
+    fn<<<(unsigned)grid, RJ_PT_THREADS, smem, ctx->stream>>>(p, ntiles);
     PYG_LAUNCHED(ctx);
     return PYG_OK;
+}
+
+// One pass: 16-byte tuples in and out, 16-byte tuples in and packed words
+// out (the first pass of a packed layout), or packed words in and out.
+int launch_pass(pyg_ctx* ctx, const RJPass& p, long long ntiles, bool in8, bool out8)
+{
+    if (ntiles <= 0) return PYG_OK;
+    if (in8) return launch_pass_t<true, true>(ctx, p, ntiles);
+    if (out8) return launch_pass_t<false, true>(ctx, p, ntiles);
+    return launch_pass_t<false, false>(ctx, p, ntiles);
 }
 
 // Host-side layout of one relation's partitions.  Exact layouts come from a
@@ -385,21 +482,37 @@ int launch_pass(pyg_ctx* ctx, const RJPass& p, long long ntiles)
 
 }  // namespace
 
-void layout_exact(const std::vector<unsigned long long>& h, int C, int sub, RJLayout& L)
+void layout_exact(const std::vector<unsigned long long>& h, int C, int sub, RJLayout& L, bool pack)
 {
     const size_t F = h.size();
     L.sampled = false;
+    L.packed = pack;
+    // Packed regions are rounded up to an even number of words.
+    auto sz = [&](unsigned long long c) { return pack ? (c + 1) & ~1ULL : c; };
     L.fstart.assign(F + 1, 0);
-    for (size_t f = 0; f < F; ++f) L.fstart[f + 1] = L.fstart[f] + h[f];
+    for (size_t f = 0; f < F; ++f) L.fstart[f + 1] = L.fstart[f] + sz(h[f]);
     L.cstart.assign(C + 1, 0);
     for (int c = 0; c <= C; ++c) L.cstart[c] = L.fstart[(size_t)c << sub];
-    L.tiles2.assign(C + 1, 0);
-    for (int c = 0; c < C; ++c) L.tiles2[c + 1] = L.tiles2[c] + (L.cstart[c + 1] - L.cstart[c] + RJ_TILE - 1) / RJ_TILE;
     L.fcap.clear();
     L.ccap.clear();
+    L.tiles2.assign(C + 1, 0);
+    if (pack) {
+        // The second pass's tiles come from the first pass's cursors (the
+        // exact counts), formed on the device as for sampled layouts; the
+        // region sizes bound them.
+        L.ccap.assign(C, 0);
+        L.tiles2_max = 0;
+        for (int c = 0; c < C; ++c) {
+            L.ccap[c] = L.cstart[c + 1] - L.cstart[c];
+            L.tiles2_max += (L.ccap[c] + RJ_TILE8 - 1) / RJ_TILE8;
+        }
+    } else {
+        for (int c = 0; c < C; ++c)
+            L.tiles2[c + 1] = L.tiles2[c] + (L.cstart[c + 1] - L.cstart[c] + RJ_TILE - 1) / RJ_TILE;
+        L.tiles2_max = L.tiles2[C];
+    }
     L.count = h;
     L.p1 = L.p2 = L.fstart[F];
-    L.tiles2_max = L.tiles2[C];
 }
 
 unsigned long long sampled_cap(unsigned long long c, long long step, unsigned long long extra)
@@ -408,14 +521,18 @@ unsigned long long sampled_cap(unsigned long long c, long long step, unsigned lo
     return (unsigned long long)std::ceil((x + 6.0 * std::sqrt(x) + 8.0) * (double)step) + extra;
 }
 
-void layout_sampled(const std::vector<unsigned long long>& sc, long long step, int C, int sub, RJLayout& L)
+void layout_sampled(const std::vector<unsigned long long>& sc, long long step, int C, int sub, RJLayout& L,
+                    bool pack)
 {
     const size_t F = sc.size();
     L.sampled = true;
+    L.packed = pack;
+    auto sz = [&](unsigned long long c) { return pack ? (c + 1) & ~1ULL : c; };
+    const int tile2 = pack ? RJ_TILE8 : RJ_TILE;
     L.fcap.assign(F, 0);
     L.fstart.assign(F + 1, 0);
     for (size_t f = 0; f < F; ++f) {
-        L.fcap[f] = sampled_cap(sc[f], step, 64);
+        L.fcap[f] = sz(sampled_cap(sc[f], step, 64));
         L.fstart[f + 1] = L.fstart[f] + L.fcap[f];
     }
     L.ccap.assign(C, 0);
@@ -424,9 +541,9 @@ void layout_sampled(const std::vector<unsigned long long>& sc, long long step, i
     for (int c = 0; c < C; ++c) {
         unsigned long long cc = 0;
         for (size_t f = (size_t)c << sub; f < (size_t)(c + 1) << sub; ++f) cc += sc[f];
-        L.ccap[c] = sampled_cap(cc, step, 1024);
+        L.ccap[c] = sz(sampled_cap(cc, step, 1024));
         L.cstart[c + 1] = L.cstart[c] + L.ccap[c];
-        L.tiles2_max += (L.ccap[c] + RJ_TILE - 1) / RJ_TILE;
+        L.tiles2_max += (L.ccap[c] + tile2 - 1) / tile2;
     }
     L.tiles2.clear();
     L.count.clear();
@@ -434,16 +551,36 @@ void layout_sampled(const std::vector<unsigned long long>& sc, long long step, i
     L.p2 = L.fstart[F];
 }
 
+bool pack_frame(long long kmin, long long kmax, long long pmin, long long pmax, bool exact, RJLayout& L)
+{
+    // A window [base, base + 2^32) centred on [lo, hi]; a sampled range
+    // must leave at least 2^30 of margin on each side.
+    auto fit = [&](long long lo, long long hi, unsigned long long& base) {
+        if (hi < lo) {  // nothing was read
+            base = 0;
+            return true;
+        }
+        const unsigned long long span = (unsigned long long)hi - (unsigned long long)lo;
+        if (span > (exact ? 0xFFFFFFFFULL : (1ULL << 31))) return false;
+        base = (unsigned long long)lo - (0xFFFFFFFFULL - span) / 2;
+        return true;
+    };
+    unsigned long long kb = 0, pb = 0;
+    if (!fit(kmin, kmax, kb) || !fit(pmin, pmax, pb)) return false;
+    L.kbase = kb;
+    L.pbase = pb;
+    return true;
+}
+
 int upload_layout(pyg_ctx* ctx, const RJLayout& L, const RJSideDev& d, int F, int C, int64_t n)
 {
     PYG_CUDA(cudaMemcpyAsync(d.fstart, L.fstart.data(), (size_t)(F + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
     PYG_CUDA(cudaMemcpyAsync(d.cstart, L.cstart.data(), (size_t)(C + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
-    if (L.sampled) {
-        PYG_CUDA(cudaMemcpyAsync(d.fcap, L.fcap.data(), (size_t)F * 8, cudaMemcpyHostToDevice, ctx->stream));
+    if (L.sampled) PYG_CUDA(cudaMemcpyAsync(d.fcap, L.fcap.data(), (size_t)F * 8, cudaMemcpyHostToDevice, ctx->stream));
+    if (L.sampled || L.packed)
         PYG_CUDA(cudaMemcpyAsync(d.ccap, L.ccap.data(), (size_t)C * 8, cudaMemcpyHostToDevice, ctx->stream));
-    } else {
+    else
         PYG_CUDA(cudaMemcpyAsync(d.tiles2, L.tiles2.data(), (size_t)(C + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
-    }
     PYG_CUDA(cudaMemsetAsync(d.cur1, 0, (size_t)(C + F) * 8, ctx->stream));  // cur1 and cur2 are adjacent
     const unsigned long long w[4] = {0, (unsigned long long)n, 0, (unsigned long long)((n + RJ_TILE - 1) / RJ_TILE)};
     PYG_CUDA(cudaMemcpyAsync(d.whole, w, sizeof(w), cudaMemcpyHostToDevice, ctx->stream));
@@ -453,9 +590,13 @@ int upload_layout(pyg_ctx* ctx, const RJLayout& L, const RJSideDev& d, int F, in
 // Runs the partition pass(es) of one relation into P1 (and P2).
 int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, const RJSideDev& d, bool two, int FB,
                int CB, void* P1, void* P2, unsigned* err, unsigned* ovf, const long long* csplit,
-               const long long* fsplit)
+               const long long* fsplit, unsigned* frame, cudaEvent_t between)
 {
     const int C = 1 << CB, sub = FB - CB;
+    if (L.packed && (!frame || csplit || (two && sub > 8))) {
+        set_error("partition: packed layouts need a frame flag, hash bins and at most 2^8 second-pass bins");
+        return PYG_ERR_ARG;
+    }
     RJPass p;
     memset(&p, 0, sizeof(p));
     p.in = in;
@@ -471,17 +612,22 @@ int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, 
     p.cursor = two ? d.cur1 : d.cur2;
     p.err = err;
     p.ovf = ovf;
+    p.kbase = L.kbase;
+    p.pbase = L.pbase;
+    p.frame = frame;
     if (csplit) {
         p.split = csplit;
         p.nsplit = C - 1;
     }
-    int rc = launch_pass(ctx, p, (n + RJ_TILE - 1) / RJ_TILE);
+    int rc = launch_pass(ctx, p, (n + RJ_TILE - 1) / RJ_TILE, false, L.packed);
     if (rc || !two) return rc;
+    if (between) cudaEventRecord(between, ctx->stream);
     long long ntiles2;
-    if (L.sampled) {
+    if (L.sampled || L.packed) {
         // Second-pass segments are the first pass's regions, filled to the
         // counts its cursors reached; the tile prefix is formed on the device.
-        rj_tile_prefix_kernel<<<1, 32, 0, ctx->stream>>>(d.cur1, d.ccap, C, d.tiles2);
+        rj_tile_prefix_kernel<<<1, 32, 0, ctx->stream>>>(d.cur1, d.ccap, C, L.packed ? RJ_TILE8 : RJ_TILE,
+                                                          d.tiles2);
         PYG_LAUNCHED(ctx);
         p.seg_count = d.cur1;
         p.ntiles_dev = d.tiles2 + C;
@@ -504,10 +650,11 @@ int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, 
         p.split = fsplit;
         p.nsplit = (1 << sub) - 1;
     }
-    return launch_pass(ctx, p, ntiles2);
+    return launch_pass(ctx, p, ntiles2, L.packed, L.packed);
 }
 
-int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int FB, unsigned long long* hist)
+int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int FB, unsigned long long* hist,
+                long long* mm)
 {
     // At most 2^15 counters (128 KB) per launch: 2^16 bins take two.
     const int F = 1 << FB, span = F < (1 << 15) ? F : (1 << 15);
@@ -522,8 +669,13 @@ int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int 
     unsigned* part = nullptr;
     int rc;
     if ((rc = dalloc(ctx, (void**)&part, (size_t)grid * span * 4))) return rc;
+    if (mm) {
+        rj_mm_init_kernel<<<1, 32, 0, ctx->stream>>>(mm);
+        PYG_LAUNCHED(ctx);
+    }
     for (int base = 0; base < F; base += span) {
-        rj_hist_kernel<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, FB, base, span, part);
+        // The key and payload ranges are taken in the first launch only.
+        rj_hist_kernel<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, FB, base, span, part, base ? nullptr : mm);
         PYG_LAUNCHED(ctx);
         rj_hist_sum_kernel<<<(span + 255) / 256, 256, 0, ctx->stream>>>(part, grid, span, hist + base);
         PYG_LAUNCHED(ctx);
@@ -558,10 +710,16 @@ int hist_launch_range(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step
 int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsigned* flags, unsigned* hflags,
                        cudaEvent_t hist_done)
 {
-    const int CB = two ? (FB + 1) / 2 : FB;
-    const int F = 1 << FB, C = 1 << CB, sub = FB - CB;
-    const size_t side = RJSideDev::words(F, C);
-    if (ns < 1 || ns > 2 || (size_t)ns * F * 8 > ctx->pinned_bytes - kPinnedScalarBytes) {
+    // Coarse bits of the first of two passes.  Unpacked layouts split FB
+    // evenly (2048-tuple tiles); packed layouts keep the second pass at 2^8
+    // bins, so that its 4096-word tiles use one-byte bin indexes and both
+    // passes write runs of about 16 words.  The unpacked split has at least
+    // as many coarse partitions, so its metadata size covers both.
+    auto coarse_bits = [&](bool packed) { return !two ? FB : (packed ? std::max(1, FB - 8) : (FB + 1) / 2); };
+    const int F = 1 << FB;
+    const size_t side = RJSideDev::words(F, 1 << coarse_bits(false));
+    const size_t per = side + F + 4;  // metadata, histogram, {kmin, kmax, pmin, pmax}
+    if (ns < 1 || ns > 2 || (size_t)ns * (F + 4) * 8 > ctx->pinned_bytes - kPinnedScalarBytes) {
         set_error("partition: %d relations of 2^%d partitions exceed the staging area", ns, FB);
         return PYG_ERR_ARG;
     }
@@ -571,84 +729,103 @@ int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsig
     unsigned long long* hh = (unsigned long long*)((char*)ctx->pinned + kPinnedScalarBytes);
     unsigned long long* meta = nullptr;
     RJSideDev d[2];
+    int CBs[2] = {FB, FB};
     bool sample[2] = {false, false};
     int rc = PYG_OK;
     for (int s = 0; s < ns; ++s) sd[s].P1 = sd[s].P2 = nullptr;
-    auto hist_of = [&](int s, int64_t st, unsigned long long* hist) {
-        return sd[s].csplit ? hist_launch_range(ctx, sd[s].in, sd[s].n, st, CB, sub, sd[s].csplit, sd[s].fsplit, hist)
-                            : hist_launch(ctx, sd[s].in, sd[s].n, st, FB, hist);
+    auto hist_at = [&](int s) { return meta + (size_t)s * per + side; };
+    auto hh_at = [&](int s) { return hh + (size_t)s * (F + 4); };
+    auto hist_of = [&](int s, int64_t st) {
+        if (sd[s].csplit) {
+            const int cb = coarse_bits(false);
+            return hist_launch_range(ctx, sd[s].in, sd[s].n, st, cb, FB - cb, sd[s].csplit, sd[s].fsplit, hist_at(s));
+        }
+        return hist_launch(ctx, sd[s].in, sd[s].n, st, FB, hist_at(s),
+                           sd[s].allow_pack ? (long long*)(hist_at(s) + F) : nullptr);
     };
-    auto hist_at = [&](int s) { return meta + (size_t)s * (side + F) + side; };
+    // Layout of relation s from host counts h (F counts, then the key and
+    // payload ranges): packed when the caller allows it and a frame fits.
+    auto form = [&](int s, const unsigned long long* h, int64_t st, bool exact) {
+        RJLayout& L = sd[s].L;
+        const long long* mm = (const long long*)(h + F);
+        const bool pack = sd[s].allow_pack && !sd[s].csplit && pack_frame(mm[0], mm[1], mm[2], mm[3], exact, L);
+        CBs[s] = coarse_bits(pack);
+        const int C = 1 << CBs[s], sub = FB - CBs[s];
+        std::vector<unsigned long long> hv(h, h + F);
+        if (exact) layout_exact(hv, C, sub, L, pack);
+        else layout_sampled(hv, st, C, sub, L, pack);
+        d[s].carve(meta + (size_t)s * per, F, C);
+    };
     auto launch = [&](int s) {
+        const RJLayout& L = sd[s].L;
         int r;
-        if ((r = upload_layout(ctx, sd[s].L, d[s], F, C, sd[s].n))) return r;
+        if ((r = upload_layout(ctx, L, d[s], F, 1 << CBs[s], sd[s].n))) return r;
         dfree(ctx, sd[s].P1);
         dfree(ctx, sd[s].P2);
         sd[s].P1 = sd[s].P2 = nullptr;
-        if ((r = dalloc(ctx, &sd[s].P1, (size_t)sd[s].L.p1 * 16))) return r;
-        if (two && (r = dalloc(ctx, &sd[s].P2, (size_t)sd[s].L.p2 * 16))) return r;
-        if ((r = run_passes(ctx, sd[s].in, sd[s].n, sd[s].L, d[s], two, FB, CB, sd[s].P1, sd[s].P2, flags + 2 * s,
-                            flags + 2 * s + 1, sd[s].csplit, sd[s].fsplit)))
+        if ((r = dalloc(ctx, &sd[s].P1, pass_bytes(L, L.p1)))) return r;
+        if (two && (r = dalloc(ctx, &sd[s].P2, pass_bytes(L, L.p2)))) return r;
+        if (sd[s].begin) cudaEventRecord(sd[s].begin, ctx->stream);
+        if ((r = run_passes(ctx, sd[s].in, sd[s].n, L, d[s], two, FB, CBs[s], sd[s].P1, sd[s].P2, flags + 4 * s,
+                            flags + 4 * s + 1, sd[s].csplit, sd[s].fsplit, flags + 4 * s + 2, sd[s].mid)))
             return r;
         if (sd[s].done) cudaEventRecord(sd[s].done, ctx->stream);
         return PYG_OK;
     };
     do {
-        if ((rc = dalloc(ctx, (void**)&meta, (side + F) * 8 * ns))) break;
-        PYG_CUDA(cudaMemsetAsync(flags, 0, (size_t)8 * ns, ctx->stream));
+        if ((rc = dalloc(ctx, (void**)&meta, per * 8 * ns))) break;
+        PYG_CUDA(cudaMemsetAsync(flags, 0, (size_t)16 * ns, ctx->stream));
         int64_t step[2] = {1, 1};
         for (int s = 0; s < ns && !rc; ++s) {
-            d[s].carve(meta + (size_t)s * (side + F), F, C);
             sample[s] = sd[s].allow_sample && two && sd[s].n >= ((int64_t)1 << 25);
             step[s] = sample[s] ? std::max<int64_t>(1, sd[s].n >> RJ_SAMPLE_LOG2) : 1;
-            if ((rc = hist_of(s, step[s], hist_at(s)))) break;
+            if ((rc = hist_of(s, step[s]))) break;
             sd[s].hist_tuples = (sd[s].n + step[s] - 1) / step[s];
         }
         if (rc) break;
         if (hist_done) cudaEventRecord(hist_done, ctx->stream);
         for (int s = 0; s < ns; ++s)
-            PYG_CUDA(cudaMemcpyAsync(hh + (size_t)s * F, hist_at(s), (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaMemcpyAsync(hh_at(s), hist_at(s), (size_t)(F + 4) * 8, cudaMemcpyDeviceToHost, ctx->stream));
         PYG_CUDA(cudaStreamSynchronize(ctx->stream));
         // The second relation's layout is formed while the first one's
         // passes run.
         for (int s = 0; s < ns && !rc; ++s) {
-            std::vector<unsigned long long> h(hh + (size_t)s * F, hh + (size_t)(s + 1) * F);
-            if (sample[s]) layout_sampled(h, step[s], C, sub, sd[s].L);
-            else layout_exact(h, C, sub, sd[s].L);
+            form(s, hh_at(s), step[s], !sample[s]);
             rc = launch(s);
         }
         if (rc) break;
-        PYG_CUDA(cudaMemcpyAsync(hflags, flags, (size_t)8 * ns, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(hflags, flags, (size_t)16 * ns, cudaMemcpyDeviceToHost, ctx->stream));
         for (int s = 0; s < ns; ++s)
             if (sd[s].L.sampled)
-                PYG_CUDA(cudaMemcpyAsync(hh + (size_t)s * F, d[s].cur2, (size_t)F * 8, cudaMemcpyDeviceToHost,
-                                         ctx->stream));
+                PYG_CUDA(cudaMemcpyAsync(hh_at(s), d[s].cur2, (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
         PYG_CUDA(cudaStreamSynchronize(ctx->stream));
         for (int s = 0; s < ns && !rc; ++s) {
-            if (hflags[2 * s]) {
+            if (hflags[4 * s]) {
                 set_error("partition: a tile copy did not complete in time");
                 rc = PYG_ERR_TIMEOUT;
                 break;
             }
-            if (sd[s].L.sampled) sd[s].L.count.assign(hh + (size_t)s * F, hh + (size_t)(s + 1) * F);
-            if (!hflags[2 * s + 1]) continue;
-            // A sampled region overflowed: redo this relation from an exact
-            // histogram (exact regions cannot overflow).
+            if (sd[s].L.sampled) sd[s].L.count.assign(hh_at(s), hh_at(s) + F);
+            if (!hflags[4 * s + 1] && !hflags[4 * s + 2]) continue;
+            // A sampled region overflowed, or a tuple fell outside a frame
+            // taken from the sample: redo this relation from an exact
+            // histogram, whose key and payload ranges are exact too (exact
+            // regions cannot overflow, and an exact frame misses nothing).
             sd[s].overflowed = true;
-            sd[s].done = nullptr;  // the redo's time is not attributed to the relation
-            if ((rc = hist_of(s, 1, hist_at(s)))) break;
-            PYG_CUDA(cudaMemcpyAsync(hh, hist_at(s), (size_t)F * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            sd[s].done = sd[s].begin = sd[s].mid = nullptr;  // the redo's time is not attributed to the relation
+            if ((rc = hist_of(s, 1))) break;
+            PYG_CUDA(cudaMemcpyAsync(hh_at(s), hist_at(s), (size_t)(F + 4) * 8, cudaMemcpyDeviceToHost, ctx->stream));
             PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-            layout_exact(std::vector<unsigned long long>(hh, hh + F), C, sub, sd[s].L);
-            PYG_CUDA(cudaMemsetAsync(flags + 2 * s, 0, 8, ctx->stream));
+            form(s, hh_at(s), 1, true);
+            PYG_CUDA(cudaMemsetAsync(flags + 4 * s, 0, 16, ctx->stream));
             if ((rc = launch(s))) break;
-            PYG_CUDA(cudaMemcpyAsync(hflags + 2 * s, flags + 2 * s, 8, cudaMemcpyDeviceToHost, ctx->stream));
+            PYG_CUDA(cudaMemcpyAsync(hflags + 4 * s, flags + 4 * s, 16, cudaMemcpyDeviceToHost, ctx->stream));
             PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-            if (hflags[2 * s]) {
+            if (hflags[4 * s]) {
                 set_error("partition: a tile copy did not complete in time");
                 rc = PYG_ERR_TIMEOUT;
-            } else if (hflags[2 * s + 1]) {
-                set_error("partition: an exact region overflowed");
+            } else if (hflags[4 * s + 1] || hflags[4 * s + 2]) {
+                set_error("partition: an exact layout overflowed a region or missed its frame");
                 rc = PYG_ERR_CAPACITY;
             }
         }

@@ -13,6 +13,15 @@
 //               tiles by bulk copy into a two-deep shared-memory ring, groups
 //               a tile by bin in shared memory and writes each bin's run
 //               contiguously after one global reservation per (tile, bin).
+//   packing     (callers that opt in) when the histogram's reading of the
+//               relation shows that key - kbase and payload - pbase both
+//               fit in 32 bits for some frame (kbase, pbase), the passes
+//               write 8-byte words (key - kbase) | (payload - pbase) << 32
+//               instead of 16-byte tuples: frame-of-reference encoding,
+//               exact, and half the bytes of every intermediate write and
+//               re-read.  A tuple outside the frame (possible when the
+//               histogram read a sample) sets a flag and the relation is
+//               redone with 16-byte intermediates.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -30,6 +39,7 @@ namespace pyg {
 #define PYG_RJ_PT_THREADS 512
 #endif
 constexpr int RJ_TILE = PYG_RJ_TILE;            // tuples per partition tile
+constexpr int RJ_TILE8 = 4096;                  // packed words per partition tile (packed input)
 constexpr int RJ_PT_THREADS = PYG_RJ_PT_THREADS;  // partition CTA
 constexpr int RJ_MAX_LOCAL_BITS = 9;     // bins of one partition pass
 constexpr int RJ_LMAX = 1 << RJ_MAX_LOCAL_BITS;
@@ -49,6 +59,12 @@ constexpr int RJ_SAMPLE_LOG2 = PYG_RJ_SAMPLE_LOG2;
 // Host-side layout of one relation's partitions.
 struct RJLayout {
     bool sampled = false;
+    // Packed (8-byte) intermediates and their frame: key = kbase + low 32
+    // bits, payload = pbase + high 32 bits (64-bit wrap-around arithmetic).
+    // Packed layouts start every region at an even word, so that each
+    // region's tiles begin 16-byte aligned for bulk copies.
+    bool packed = false;
+    unsigned long long kbase = 0, pbase = 0;
     std::vector<unsigned long long> fstart;  // F + 1 fine region starts
     std::vector<unsigned long long> fcap;    // F fine region capacities (sampled)
     std::vector<unsigned long long> cstart;  // C + 1 coarse region starts
@@ -60,10 +76,19 @@ struct RJLayout {
 };
 
 // Exact layout from exact per-fine-partition counts h (F = h.size()).
-void layout_exact(const std::vector<unsigned long long>& h, int C, int sub, RJLayout& L);
+// pack: regions rounded up to an even number of words (packed layouts).
+void layout_exact(const std::vector<unsigned long long>& h, int C, int sub, RJLayout& L, bool pack = false);
 // Sampled layout from the counts sc of every step-th tuple: each region is
 // sized with six standard deviations of slack.
-void layout_sampled(const std::vector<unsigned long long>& sc, long long step, int C, int sub, RJLayout& L);
+void layout_sampled(const std::vector<unsigned long long>& sc, long long step, int C, int sub, RJLayout& L,
+                    bool pack = false);
+// Frame of a packed layout from the key and payload ranges seen by the
+// histogram ([kmin, kmax], [pmin, pmax], signed).  exact: the ranges cover
+// every tuple; else they come from a sample and must leave a margin of at
+// least 2^30 on each side.  Returns false when no frame fits.
+bool pack_frame(long long kmin, long long kmax, long long pmin, long long pmax, bool exact, RJLayout& L);
+// Bytes of one intermediate element of a layout.
+inline int elem_bytes(const RJLayout& L) { return L.packed ? 8 : 16; }
 
 // Device copy of one relation's partition metadata (u64 words).
 struct RJSideDev {
@@ -86,17 +111,27 @@ struct RJSideDev {
 // Copies a layout to the device and zeroes its cursors.
 int upload_layout(pyg_ctx* ctx, const RJLayout& L, const RJSideDev& d, int F, int C, int64_t n);
 // Histogram of the top FB hash bits of in[0], in[step], ... into hist
-// (2^FB device words, zeroed here).
-int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int FB, unsigned long long* hist);
+// (2^FB device words, zeroed here).  mm (optional, 4 words): receives the
+// minimum and maximum key and payload of the tuples read, as signed
+// {kmin, kmax, pmin, pmax}.
+int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int FB, unsigned long long* hist,
+                long long* mm = nullptr);
 // Partition pass(es) of one relation into P1 (and P2 when two): *err is set
-// if a tile's bulk copy never landed, *ovf if a sampled region overflowed.
-// Afterwards d.cur2 holds the tuples written per fine partition.
+// if a tile's bulk copy never landed, *ovf if a sampled region overflowed,
+// *frame if a tuple fell outside a packed layout's frame.  Afterwards
+// d.cur2 holds the tuples written per fine partition.
 // Range mode when csplit is set: pass 1 bins by the 2^CB - 1 coarse
 // splitters, pass 2 by the fine splitters (F - 1, ascending; coarse
 // splitter i = fine splitter (i + 1) * 2^(FB - CB) - 1).
 int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, const RJSideDev& d, bool two, int FB,
                int CB, void* P1, void* P2, unsigned* err, unsigned* ovf, const long long* csplit = nullptr,
-               const long long* fsplit = nullptr);
+               const long long* fsplit = nullptr, unsigned* frame = nullptr, cudaEvent_t between = nullptr);
+// Device bytes of a layout's pass buffers (packed buffers get 16 bytes of
+// tail so that the last tile's 16-byte-rounded copy stays inside).
+inline size_t pass_bytes(const RJLayout& L, unsigned long long words)
+{
+    return (size_t)words * elem_bytes(L) + (L.packed ? 16 : 0);
+}
 // Histogram of range bins (see run_passes) of in[0], in[step], ...
 int hist_launch_range(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int CB, int sub,
                       const long long* csplit, const long long* fsplit, unsigned long long* hist);
@@ -109,8 +144,11 @@ struct RPSide {
     const longlong2* in = nullptr;
     int64_t n = 0;
     bool allow_sample = true;
+    bool allow_pack = false;  // the caller reads packed intermediates (L.packed tells)
     const long long* csplit = nullptr;
     const long long* fsplit = nullptr;
+    cudaEvent_t begin = nullptr;  // recorded before the first pass (optional)
+    cudaEvent_t mid = nullptr;    // between the two passes (optional)
     cudaEvent_t done = nullptr;
     RJLayout L;
     void* P1 = nullptr;
@@ -123,9 +161,10 @@ struct RPSide {
 // host round trip, both relations' passes (the second relation's layout is
 // formed while the first one's passes run), one more round trip for the
 // counts and flags, and an exact redo of a relation whose sampled region
-// overflowed.  flags: 2 device words per relation (bulk copy never landed,
-// region overflow); hflags: as many pinned host words.  hist_done
-// (optional) is recorded after the histograms.
+// overflowed or whose packed frame missed a tuple (the redo is unpacked).
+// flags: 4 device words per relation (bulk copy never landed, region
+// overflow, frame miss, unused); hflags: as many pinned host words.
+// hist_done (optional) is recorded after the histograms.
 int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsigned* flags, unsigned* hflags,
                        cudaEvent_t hist_done);
 
@@ -135,8 +174,8 @@ int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsig
 // overflowed.  On success the partitions are in (two ? *P2 : *P1) at
 // L.fstart with L.count tuples each; the caller frees *P1 and *P2.  flags:
 // two device words (bulk copy never landed, region overflow); hflags: two
-// pinned host words.  hist_ms / hist_tuples (optional): the histogram's
-// time and the tuples it read.
+// pinned host words; both need 4 words (see rp_partition_sides).  hist_ms /
+// hist_tuples (optional): the histogram's time and the tuples it read.
 int rp_partition(pyg_ctx* ctx, const longlong2* in, int64_t n, int FB, bool two, bool allow_sample,
                  const long long* csplit, const long long* fsplit, RJLayout& L, void** P1, void** P2,
                  unsigned* flags, unsigned* hflags, float* hist_ms = nullptr, int64_t* hist_tuples = nullptr);

@@ -1,9 +1,16 @@
 // Operator shims for the join / aggregation hot path over the libpyg C ABI.
 #include "engine.h"
 
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <iostream>
 #include <sstream>
 
 #include "../../include/pyg_mpsm.h"
@@ -579,11 +586,215 @@ private:
     int32_t attr = 0;
 };
 
+// `sortlimit` (SortLimit, operators/sortlimit.cpp:32-262): the first
+// limit[0] tuples in the order of the `by` columns ("$i" strings, as
+// parseSortInput reads them, :18-30), ascending when asc[0] == 1 else
+// descending, ties in input order; pyg_sortlimit on the GPU.
+class SortLimitOp : public MaterializedOp {
+public:
+    Operator* nextOp = nullptr;
+    std::vector<Operator*> children() override { return {nextOp}; }
+    void init(const Setting& root, const Setting& node) override
+    {
+        Operator::init(root, node);
+        schema = nextOp->getOutSchema();
+        const Setting& by = node["by"];
+        for (size_t i = 0; i < by.size(); ++i) {
+            const std::string& s = by[i].asString();
+            const size_t d = s.find('$');
+            if (d == std::string::npos || d + 1 >= s.size())
+                throw EngineError("sortlimit: `by` entries name columns as \"$i\"");
+            const int c = std::stoi(s.substr(d + 1));
+            if (c < 0 || (size_t)c >= schema.columns()) throw EngineError("sortlimit: column out of range");
+            keys.push_back(c);
+        }
+        asc = node["asc"][0].asInt() == 1;
+        limit = node["limit"][0].asInt();
+    }
+    ResultCode scanStart(unsigned short tid) override
+    {
+        if (nextOp->scanStart(tid) == Error) return Error;
+        HostRel in;
+        drain(nextOp, tid, in);
+        nextOp->scanStop(tid);
+        pyg_rel r = schema.rel(in.data, in.ntuples, false);
+        const int64_t k = limit < in.ntuples ? limit : in.ntuples;
+        void* out = nullptr;
+        check(pyg_alloc(ctx, (size_t)(k > 0 ? k : 1) * schema.tuple_bytes, &out), "sortlimit");
+        int64_t n = 0;
+        int rc = pyg_sortlimit(ctx, &r, keys.data(), (int32_t)keys.size(), asc ? 1 : 0, limit, out, k, &n);
+        if (rc == PYG_OK) serve_from_device(out, n);
+        pyg_free(ctx, out);
+        check(rc, "sortlimit");
+        return Ready;
+    }
+
+private:
+    std::vector<int32_t> keys;
+    bool asc = true;
+    int64_t limit = 0;
+};
+
+// `shmwriter` (MemSegmentWriter, operators/memsegmentwriter.cpp): writes
+// its input's tuples into memory segments instead of returning them.  A
+// segment is the file paths[i] + counter (a "/dev/shm/..." path is opened
+// with shm_open, anything else as a file), created exclusively and mapped,
+// of at most `size` bytes of whole tuples; when one is full the next path
+// takes over round-robin, the seven-digit counter advancing after each
+// cycle (:239-265, :380-452).  The last segment is truncated to the bytes
+// it holds, and deleted when it holds none.  getNext returns Finished with
+// an empty page.  The NUMA `policy` / `numanodes` settings are accepted
+// and, as in a reference build without NUMA, only warned about.
+class ShmWriterOp : public Operator {
+public:
+    Operator* nextOp = nullptr;
+    std::vector<Operator*> children() override { return {nextOp}; }
+    void init(const Setting& root, const Setting& node) override
+    {
+        Operator::init(root, node);
+        schema = nextOp->getOutSchema();
+        seg_bytes = node["size"].asInt();
+        if (node.exists("policy"))
+            std::cerr << " ** NUMA POLICY WARNING: Memory policy is ignored by the GPU engine." << std::endl;
+        const Setting& p = node["paths"];
+        if (p.isAggregate())
+            for (size_t i = 0; i < p.size(); ++i) paths.push_back(p[i].asString());
+        else
+            paths.push_back(p.asString());
+        if (paths.empty()) throw EngineError("shmwriter: no paths");
+        if (seg_bytes < schema.tuple_bytes) throw EngineError("shmwriter: size below one tuple");
+    }
+    ResultCode scanStart(unsigned short tid) override { return nextOp->scanStart(tid); }
+    ResultCode scanStop(unsigned short tid) override { return nextOp->scanStop(tid); }
+    GetNextResultT getNext(unsigned short tid) override
+    {
+        const int64_t tb = schema.tuple_bytes;
+        const int64_t per = seg_bytes / tb;  // tuples per segment
+        std::string counter = "0000000";
+        size_t node = 0;
+        Segment seg;
+        seg.open(paths[node] + counter, (size_t)seg_bytes);
+        GetNextResultT r;
+        do {
+            r = nextOp->getNext(tid);
+            if (r.first == Error) {
+                seg.close(0);
+                return r;
+            }
+            const Page* in = r.second;
+            int64_t at = 0;
+            while (in && at < in->ntuples) {
+                const int64_t room = per - seg.used / tb;
+                const int64_t take = std::min(room, in->ntuples - at);
+                memcpy(seg.mem + seg.used, in->data + at * tb, (size_t)(take * tb));
+                seg.used += (size_t)(take * tb);
+                at += take;
+                if (at < in->ntuples) {  // full: the next path, the counter after a cycle
+                    seg.close(seg.used);
+                    node = (node + 1) % paths.size();
+                    if (node == 0) advance(counter);
+                    seg.open(paths[node] + counter, (size_t)seg_bytes);
+                }
+            }
+        } while (r.first == Ready);
+        seg.close(seg.used);
+        empty.ntuples = 0;
+        empty.tuple_bytes = schema.tuple_bytes;
+        return std::make_pair(Finished, &empty);
+    }
+
+private:
+    struct Segment {
+        std::string name;
+        uint8_t* mem = nullptr;
+        size_t cap = 0, used = 0;
+        void open(const std::string& path, size_t bytes)
+        {
+            name = path;
+            const bool shm = path.compare(0, 8, "/dev/shm") == 0;
+            const int fd = shm ? shm_open(path.c_str() + 8, O_RDWR | O_EXCL | O_CREAT, S_IRUSR | S_IWUSR)
+                               : ::open(path.c_str(), O_RDWR | O_EXCL | O_CREAT, S_IRUSR | S_IWUSR);
+            if (fd == -1) throw EngineError("shmwriter: cannot create segment " + path);
+            if (ftruncate(fd, (off_t)bytes) != 0) {
+                ::close(fd);
+                throw EngineError("shmwriter: cannot size segment " + path);
+            }
+            void* m = mmap(nullptr, bytes, PROT_READ | PROT_WRITE, MAP_SHARED | MAP_NORESERVE, fd, 0);
+            ::close(fd);
+            if (m == MAP_FAILED) throw EngineError("shmwriter: cannot map segment " + path);
+            mem = (uint8_t*)m;
+            cap = bytes;
+            used = 0;
+        }
+        // Unmaps, then truncates to the bytes written (unlinks when none).
+        void close(size_t bytes)
+        {
+            if (!mem) return;
+            munmap(mem, cap);
+            mem = nullptr;
+            const bool shm = name.compare(0, 8, "/dev/shm") == 0;
+            if (bytes == 0) {
+                if (shm) shm_unlink(name.c_str() + 8);
+                else unlink(name.c_str());
+                return;
+            }
+            if (truncate(name.c_str(), (off_t)bytes) != 0) throw EngineError("shmwriter: cannot truncate " + name);
+        }
+    };
+    static void advance(std::string& c)
+    {
+        for (int pos = (int)c.size() - 1; pos >= 0; --pos) {
+            if (c[pos] != '9') {
+                ++c[pos];
+                return;
+            }
+            c[pos] = '0';
+        }
+        throw EngineError("shmwriter: segment counter overflowed");
+    }
+    int64_t seg_bytes = 0;
+    std::vector<std::string> paths;
+    Page empty;
+};
+
+// Largest number of tuples of `in` that share one value of column `key`:
+// a GPU count per key (pyg_groupby), then the maximum on the host.
+static int64_t max_key_multiplicity(pyg_ctx* ctx, const pyg_rel& in, int32_t key)
+{
+    if (in.ntuples == 0) return 0;
+    const int kb = in.col_type[key] == PYG_INT32 ? 4 : 8;
+    const size_t tb = (size_t)kb + 8;  // key, count
+    void* out = nullptr;
+    check(pyg_alloc(ctx, (size_t)in.ntuples * tb, &out), "key multiplicity");
+    int64_t groups = 0;
+    int rc = pyg_groupby(ctx, &in, &key, 1, PYG_AGG_COUNT, 0, 0, 0, out, in.ntuples, &groups);
+    std::vector<uint8_t> h;
+    if (rc == PYG_OK) {
+        h.resize((size_t)groups * tb);
+        if (groups) rc = pyg_memcpy_d2h(ctx, h.data(), out, h.size());
+    }
+    pyg_free(ctx, out);
+    check(rc, "key multiplicity");
+    int64_t most = 0;
+    for (int64_t g = 0; g < groups; ++g) {
+        int64_t c;
+        memcpy(&c, h.data() + (size_t)g * tb + kb, 8);
+        most = c > most ? c : most;
+    }
+    return most;
+}
+
 // `sortmergejoin` / `mpsmjoin` / `newmpsmjoin` / `preprejoin`
 // (operators/join.cpp:905-2212): MPSM join on single keys.  The
 // buildprepartitioned range (if any) gives equal-width splitters as the
 // reference; an optional gpu { splitter = "sampled" | "learned" |
 // "exactrange"; fanout = N; } group picks the splitters.
+// `newmpsmjoin` and `preprejoin` merge through a buffer that holds at most
+// `mostfreqbuildkeyoccurances` build tuples of one key (newmpsmjoin adds
+// the setting as 1 when it is missing, operators/join.cpp:1628-1631;
+// preprejoin requires it, :1821, and sizes its buffer by it, :1857-1859).
+// The reference overruns that buffer when a build key repeats more often;
+// here such a build side is refused with an error naming both numbers.
 class MpsmJoinOp : public DualInputOp {
 public:
     void init(const Setting& root, const Setting& node) override
@@ -615,6 +826,12 @@ public:
                                  : k == "exactrange" ? PYG_MPSM_SPLIT_EXACTRANGE : PYG_MPSM_SPLIT_SAMPLED;
             opts.fanout = (int32_t)g.getInt("fanout", opts.fanout);
         }
+        if (type == "preprejoin" && !node.exists("mostfreqbuildkeyoccurances"))
+            throw EngineError("preprejoin: mostfreqbuildkeyoccurances is required");
+        if (type == "newmpsmjoin" || type == "preprejoin") {
+            mfbko = node.getInt("mostfreqbuildkeyoccurances", 1);
+            if (mfbko < 1) throw EngineError(type + ": mostfreqbuildkeyoccurances must be at least 1");
+        }
     }
     ResultCode scanStart(unsigned short tid) override
     {
@@ -626,6 +843,12 @@ public:
         probeOp->scanStop(tid);
         pyg_rel r = buildOp->getOutSchema().rel(R.data, R.ntuples, false);
         pyg_rel s = probeOp->getOutSchema().rel(S.data, S.ntuples, false);
+        if (mfbko > 0) {
+            const int64_t most = max_key_multiplicity(ctx, r, bkey);
+            if (most > mfbko)
+                throw EngineError(type + ": a build key occurs " + std::to_string(most) +
+                                  " times, more than mostfreqbuildkeyoccurances = " + std::to_string(mfbko));
+        }
         int64_t n = 0;
         int rc = pyg_mpsm_join_materialize(ctx, &r, bkey, &s, pkey, proj.data(), (int32_t)proj.size(), &opts, nullptr,
                                            0, &n);
@@ -666,6 +889,7 @@ public:
 private:
     std::vector<pyg_proj> proj;
     int32_t bkey = 0, pkey = 0;
+    int64_t mfbko = 0;  // 0: no bound (sortmergejoin, mpsmjoin)
     pyg_mpsm_opts opts;
     HostRel result;
     int64_t served = 0;
@@ -680,6 +904,8 @@ static void set_input(Operator* op, Operator* child)
     else if (auto* a = dynamic_cast<AggregateOp*>(op)) a->nextOp = child;
     else if (auto* p = dynamic_cast<PartitionOp*>(op)) p->nextOp = child;
     else if (auto* so = dynamic_cast<SortOp*>(op)) so->nextOp = child;
+    else if (auto* sl = dynamic_cast<SortLimitOp*>(op)) sl->nextOp = child;
+    else if (auto* sw = dynamic_cast<ShmWriterOp*>(op)) sw->nextOp = child;
     else throw EngineError("operator '" + op->name + "' takes no input");
 }
 
@@ -699,6 +925,8 @@ static Operator* construct(Query& q, const Setting& root, const Setting& node)
     else if (type == "printer_tuplecount") op.reset(new TupleCountPrinter());
     else if (type == "partition") op.reset(new PartitionOp());
     else if (type == "sort") op.reset(new SortOp());
+    else if (type == "sortlimit") op.reset(new SortLimitOp());
+    else if (type == "shmwriter") op.reset(new ShmWriterOp());
     else throw EngineError("plan node type '" + type + "' is not on the GPU join/aggregation path");
     op->type = type;
     op->name = name;

@@ -79,7 +79,9 @@ class pyg_join_opts(C.Structure):
 class pyg_join_stats(C.Structure):
     _fields_ = [("algorithm", C.c_int32), ("radix_bits", C.c_int32), ("build_partition_ms", C.c_double),
                 ("build_ms", C.c_double), ("probe_partition_ms", C.c_double), ("probe_ms", C.c_double), ("overflow_tuples", C.c_int64),
-                ("padded_tuples", C.c_int64), ("histogram_ms", C.c_double), ("histogram_tuples", C.c_int64)]
+                ("padded_tuples", C.c_int64), ("histogram_ms", C.c_double), ("histogram_tuples", C.c_int64),
+                ("build_pass_ms", C.c_double * 2), ("probe_pass_ms", C.c_double * 2), ("build_packed", C.c_int32),
+                ("probe_packed", C.c_int32)]
 
 
 class pyg_splitter(C.Structure):
@@ -149,6 +151,7 @@ SIGNATURES = [
     ("pyg_partition", C.c_int, [_P, C.POINTER(pyg_rel), _I32, C.POINTER(pyg_splitter), _P, _PI64]),
     ("pyg_sort", C.c_int, [_P, C.POINTER(pyg_rel), _I32, _P]),
     ("pyg_lower_bound", C.c_int, [_P, C.POINTER(pyg_rel), _I32, _P, _I64, _P]),
+    ("pyg_sortlimit", C.c_int, [_P, C.POINTER(pyg_rel), _PI32, _I32, _I32, _I64, _P, _I64, _PI64]),
     ("pyg_mpsm_join_agg", C.c_int, [_P, C.POINTER(pyg_rel), _I32, C.POINTER(pyg_rel), _I32, C.POINTER(pyg_proj), _I32,
                                     C.POINTER(pyg_mpsm_opts), C.POINTER(pyg_join_result), C.POINTER(pyg_mpsm_stats)]),
     ("pyg_mpsm_join_materialize", C.c_int, [_P, C.POINTER(pyg_rel), _I32, C.POINTER(pyg_rel), _I32,
@@ -409,6 +412,16 @@ class Ctx:
     def sort(self, rel, key_col, out):
         r = rel.c()
         check(lib().pyg_sort(self.h, C.byref(r), key_col, _ptr(out)))
+
+    def sortlimit(self, rel, key_cols, asc, limit, out, capacity):
+        k = (C.c_int32 * max(1, len(key_cols)))(*key_cols)
+        n = C.c_int64()
+        r = rel.c()
+        rc = lib().pyg_sortlimit(self.h, C.byref(r), k, len(key_cols), int(bool(asc)), limit, _ptr(out), capacity,
+                                 C.byref(n))
+        if rc not in (PYG_OK, PYG_ERR_CAPACITY):
+            check(rc)
+        return rc, n.value
 
     def lower_bound(self, rel, key_col, queries, nq, out):
         r = rel.c()

@@ -138,7 +138,33 @@ def main():
         rows, _, _ = refrun.run(d, refrun.plan_mpsm(T, rf, [I64, I64], sf, [I64, I64], [(0, 0), (0, 1), (1, 1)], 0,
                                                     n - 1, 2 * n, 2 * S.shape[0]))
     save("mpsm_pkfk", R=R, S=S, proj=np.array([(0, 0), (0, 1), (1, 1)]), out=rows_array(rows, [I64, I64, I64]))
+    sortlimit_cases()
+
+
+def sortlimit_cases():
+    """Top-k with ties (input order decides), ascending and descending, on
+    an int64 key and on an (int32, int32) pair; one input file so the
+    arrival order is the file order."""
+    rng = np.random.default_rng(20241201)
+    m = 20000
+    A = struct([rng.integers(-300, 300, m), np.arange(m, dtype=np.int64)], [I64, I64])
+    B = struct([rng.integers(-5, 5, m).astype(np.int32), rng.integers(-40, 40, m).astype(np.int32),
+                np.arange(m, dtype=np.int64)], [I32, I32, I64])
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        af = refrun.write_rel(d, "A", A, 1)
+        bf = refrun.write_rel(d, "B", B, 1)
+        for asc in (1, 0):
+            for limit in (1, 100, 5000):
+                rows, _, _ = refrun.run(d, refrun.plan_sortlimit(af, [I64, I64], [0], asc, limit))
+                out[f"a_{asc}_{limit}"] = rows_array(rows, [I64, I64])
+                rows, _, _ = refrun.run(d, refrun.plan_sortlimit(bf, [I32, I32, I64], [0, 1], asc, limit))
+                out[f"b_{asc}_{limit}"] = rows_array(rows, [I32, I32, I64])
+    save("sortlimit", A=A, B=B, **out)
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["sortlimit"]:
+        sortlimit_cases()
+    else:
+        main()

@@ -131,3 +131,16 @@ def test_oracle_sort_is_stable_and_ordered():
     assert np.all(np.diff(out["c0"]) >= 0)
     ref = A[np.argsort(A["c0"], kind="stable")]
     assert np.array_equal(out, ref)
+
+
+def test_oracle_sortlimit_matches_reference(golden):
+    """SortLimit top-k (operators/sortlimit.cpp), as the reference engine
+    printed it for int64 and (int32, int32) keys, both directions, with
+    ties decided by input order."""
+    g = golden("sortlimit")
+    for asc in (1, 0):
+        for limit in (1, 100, 5000):
+            got = O.sortlimit(g["A"], [2, 2], [0], asc, limit)
+            assert got.tolist() == g[f"a_{asc}_{limit}"].tolist()
+            got = O.sortlimit(g["B"], [1, 1, 2], [0, 1], asc, limit)
+            assert got.tolist() == g[f"b_{asc}_{limit}"].tolist()

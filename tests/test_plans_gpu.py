@@ -96,3 +96,120 @@ def test_partition_plan_orders_partitions(golden):
     keys = np.array([r[0] for r in out])
     assert np.all(np.diff(keys) >= 0)  # partitions in order, each sorted
     assert sorted(out) == sorted(rows(A))
+
+
+def _mpsm_family_plan(jtype, rf, sf, n, m, mfbko=None, presort=False):
+    """partition(build) [and partition(probe), each sorted] -> jtype ->
+    merge, over (int64, int64) relations with keys in [0, n)."""
+    extra = f"mostfreqbuildkeyoccurances = {mfbko}; " if mfbko is not None else ""
+    sort = '"yes"' if presort else '"no"'
+    part = (lambda name, maxt: f'{name}: {{ type = "partition"; attr = 0; range = [0, {n - 1}]; buckets = {T}; '
+            f'maxtuples = {maxt}; sort = {sort}; }};\n')
+    probe_leaf = '{ name: "partS"; input: { name: "scanS"; }; }' if presort else '{ name: "scanS"; }'
+    return (refrun.header() + refrun.scan_node("scanR", rf, [2, 2]) + refrun.scan_node("scanS", sf, [2, 2])
+            + part("partR", 2 * n) + (part("partS", 2 * m) if presort else "")
+            + f'join: {{ type = "{jtype}"; maxbuildtuples = {2 * n}; maxprobetuples = {2 * m}; '
+              f'threadgroups = ( [{refrun._list(range(T))}] ); buildjattr = 0; probejattr = 0; '
+              f'projection = ("B$1", "P$1"); {extra}'
+              f'buildprepartitioned: {{ range = [0, {n - 1}]; buckets = {T}; }}; }};\n'
+            + f'merge: {{ type = "merge"; threads = {T}; }};\n'
+            + "treeroot: " + refrun._tree("merge", leaf=(f'{{ name: "join"; build: {{ name: "partR"; input: '
+                                                         f'{{ name: "scanR"; }}; }}; probe: {probe_leaf}; }}'))
+            + ";\n")
+
+
+def _pkfk(n, m, seed, dup_every=0):
+    rng = np.random.default_rng(seed)
+    dt = np.dtype([("c0", np.int64), ("c1", np.int64)])
+    k = rng.permutation(n).astype(np.int64)
+    if dup_every:
+        k[::dup_every] = k[1]
+    R = np.zeros(n, dtype=dt)
+    R["c0"], R["c1"] = k, k * 7 + 3
+    S = np.zeros(m, dtype=dt)
+    S["c0"], S["c1"] = rng.integers(0, n, m), rng.integers(0, 1 << 20, m)
+    return R, S
+
+
+@pytest.mark.parametrize("jtype,mfbko,presort", [("newmpsmjoin", None, False), ("newmpsmjoin", 1, False),
+                                                 ("preprejoin", 1, True), ("preprejoin", 4, True)])
+def test_mpsm_family_plans_match_oracle(jtype, mfbko, presort):
+    """`newmpsmjoin` and `preprejoin` plans (operators/join.cpp:1619-2212;
+    preprejoin over sorted partitions of both sides) give the joined rows
+    of the oracle on PK-FK inputs, whose build keys occur once."""
+    import oracle as O
+    n, m = 5000, 40000
+    R, S = _pkfk(n, m, 11)
+    out, _, _ = run_plan(lambda rf, sf: _mpsm_family_plan(jtype, rf, sf, n, m, mfbko, presort), R, S)
+    want = O.hashjoin_materialize(R, [2, 2], [0], S, [2, 2], [0], [(0, 1), (1, 1)], buckets=n)
+    assert sorted(out) == sorted(rows(want))
+
+
+def test_mpsm_family_refuses_build_keys_above_mfbko():
+    """A build key that occurs more often than mostfreqbuildkeyoccurances is
+    refused with an error (the reference's merge buffer holds only that
+    many); a bound that covers the repeats joins normally."""
+    import oracle as O
+    n, m = 4000, 20000
+    R, S = _pkfk(n, m, 12, dup_every=100)  # key k[1] occurs about 41 times
+    most = int(np.unique(R["c0"], return_counts=True)[1].max())
+    with pytest.raises(RuntimeError, match="mostfreqbuildkeyoccurances"):
+        run_plan(lambda rf, sf: _mpsm_family_plan("preprejoin", rf, sf, n, m, most - 1, True), R, S)
+    out, _, _ = run_plan(lambda rf, sf: _mpsm_family_plan("preprejoin", rf, sf, n, m, most, True), R, S)
+    want = O.hashjoin_materialize(R, [2, 2], [0], S, [2, 2], [0], [(0, 1), (1, 1)], buckets=n)
+    assert sorted(out) == sorted(rows(want))
+
+
+def test_sort_plan():
+    """scan -> sort (attr 0) -> merge: every tuple once, keys in order
+    (operators/sort.cpp:87-311)."""
+    rng = np.random.default_rng(13)
+    dt = np.dtype([("c0", np.int64), ("c1", np.int64)])
+    A = np.zeros(30000, dtype=dt)
+    A["c0"], A["c1"] = rng.integers(-(1 << 40), 1 << 40, A.shape[0]), rng.integers(0, 1000, A.shape[0])
+    A["c0"][::7] = 12345  # ties
+    plan = (lambda f: refrun.header() + refrun.scan_node("scan", f, [2, 2])
+            + f'srt: {{ type = "sort"; attr = 0; maxtuples = ( {", ".join(chr(34) + "1 M" + chr(34) for _ in range(T))} ); }};\n'
+            + f'merge: {{ type = "merge"; threads = {T}; }};\n'
+            + "treeroot: " + refrun._tree("merge", "srt", leaf='{ name: "scan"; }') + ";\n")
+    out, _, _ = run_plan(plan, A)
+    keys = [r[0] for r in out]
+    assert keys == sorted(keys)
+    assert sorted(out) == sorted(rows(A))
+
+
+def test_sortlimit_plan(golden):
+    """scan -> sortlimit gives the reference engine's own top-k rows
+    (golden fixture made by the reference from the same plan text)."""
+    g = golden("sortlimit")
+    for asc in (1, 0):
+        for limit in (1, 100, 5000):
+            out, _, _ = run_plan(lambda f: refrun.plan_sortlimit(f, [2, 2], [0], asc, limit), g["A"])
+            assert out == rows(g[f"a_{asc}_{limit}"])
+    out, _, _ = run_plan(lambda f: refrun.plan_sortlimit(f, [1, 1, 2], [0, 1], 0, 100), g["B"])
+    assert out == rows(g["b_0_100"])
+
+
+def test_shmwriter_plan(tmp_path):
+    """scan -> shmwriter: the input's tuples land, in order, in segments of
+    at most `size` bytes named path + counter, alternating between the two
+    paths and advancing the counter after each cycle; the last segment is
+    truncated to what it holds (operators/memsegmentwriter.cpp)."""
+    rng = np.random.default_rng(17)
+    dt = np.dtype([("c0", np.int64), ("c1", np.int64)])
+    A = np.zeros(2500, dtype=dt)
+    A["c0"], A["c1"] = rng.integers(-(1 << 50), 1 << 50, A.shape[0]), np.arange(A.shape[0])
+    pa, pb = str(tmp_path / "segA"), str(tmp_path / "segB")
+    size = 1000 * 16 + 8  # 1000 whole tuples per segment
+    plan = (lambda f: refrun.header(1 << 12) + refrun.scan_node("scan", f, [2, 2])
+            + f'w: {{ type = "shmwriter"; size = {size}; paths = ("{pa}", "{pb}"); }};\n'
+            + 'treeroot: { name: "w"; input: { name: "scan"; }; };\n')
+    with tempfile.TemporaryDirectory() as d:
+        files = [refrun.write_rel(d, "r0", A, 1)]
+        out, _, _ = refrun.run(d, plan(files[0]), exe=EXE)
+    assert out == []
+    names = [pa + "0000000", pb + "0000000", pa + "0000001"]
+    segs = [np.fromfile(n, dtype=dt) for n in names]
+    assert [s.shape[0] for s in segs] == [1000, 1000, 500]
+    assert np.array_equal(np.concatenate(segs), A)
+    assert not os.path.exists(pb + "0000001")

@@ -77,6 +77,36 @@ def test_radix_sentinel_keys_and_duplicates(ctx, torch_cuda):
     assert ctx.hashjoin_agg(Rd, [0], Sd, [0], PROJ, pyg.JOIN_RADIX) == want
 
 
+@pytest.mark.parametrize("case", ["unique", "repeated", "many_sentinels", "empty_probe", "empty_build"])
+def test_direct_one_shot_join(ctx, torch_cuda, case):
+    """The one-shot direct join (clear, build, probe; the probe reads the
+    build's flags on the device) against the oracle, for every projection
+    over {B$1, P$1}.  Repeated build keys and more empty-marker build keys
+    than its side list holds make the probe stand down and the general path
+    answer; the result is the same."""
+    rng = np.random.default_rng(len(case))
+    mn = np.iinfo(np.int64).min
+    n, m = 1 << 16, 1 << 20
+    k = rng.permutation(n).astype(np.int64) * 11 - 5000
+    if case == "repeated":
+        k[: n // 3] = k[n // 3: 2 * (n // 3)]
+    if case == "many_sentinels":
+        k[:2000] = mn
+    R = struct([k, rng.integers(-(1 << 62), 1 << 62, n)], [I64, I64])
+    fk = rng.choice(k, m) + (rng.random(m) < 0.1)
+    fk[::777] = mn
+    S = struct([fk, rng.integers(-(1 << 62), 1 << 62, m)], [I64, I64])
+    if case == "empty_probe":
+        S = S[:0]
+    if case == "empty_build":
+        R = R[:0]
+    Rd, Sd = dev_rel(torch_cuda, R, [I64, I64]), dev_rel(torch_cuda, S, [I64, I64])
+    for proj in (PROJ, [(1, 1), (0, 1)], [(1, 1)], [(0, 1)], []):
+        want = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], proj, buckets=n)
+        for _ in range(2):  # a second call reuses the context's table
+            assert ctx.hashjoin_agg(Rd, [0], Sd, [0], proj, pyg.JOIN_DIRECT) == want
+
+
 @pytest.mark.parametrize("bits", [4, 9, 11])
 def test_radix_duplicate_build_keys(ctx, torch_cuda, bits):
     """Repeated build keys switch the join to its counted slot layout (and
@@ -141,6 +171,54 @@ def test_radix_sample_misjudged_redoes_exactly(ctx, torch_cuda):
     got, st = ctx.hashjoin_agg(dev_rel(torch_cuda, R, [I64, I64]), [0], dev_rel(torch_cuda, S, [I64, I64]), [0], PROJ,
                                pyg.JOIN_RADIX, 10, stats=True)
     assert got == want and st.overflow_tuples == 1
+
+
+@pytest.mark.parametrize("bits", [0, 6, 12, 16])
+@pytest.mark.parametrize("case", ["both", "build_only", "probe_only", "near_min"])
+def test_radix_packed_intermediates(ctx, torch_cuda, bits, case):
+    """Partition passes write 8-byte frame-of-reference words when a
+    relation's key and payload ranges each fit in 32 bits, and 16-byte
+    tuples otherwise, per relation.  Every combination, at one pass (6
+    bits), two passes (12, 16 bits) and the automatic choice, must equal the
+    oracle bit for bit.  near_min puts the keys just above INT64_MIN (the
+    table's empty marker among them), so the frame arithmetic wraps."""
+    rng = np.random.default_rng(bits * 7 + len(case))
+    n, m = 1 << 17, 1 << 21
+    mn = np.iinfo(np.int64).min
+    base = mn if case == "near_min" else -(1 << 35)
+    k = rng.permutation(n).astype(np.int64) * 3 + base
+    small = lambda c: rng.integers(-(1 << 31), 1 << 31, c)  # noqa: E731
+    large = lambda c: rng.integers(-(1 << 62), 1 << 62, c)  # noqa: E731
+    R = struct([k, large(n) if case == "probe_only" else small(n)], [I64, I64])
+    fk = zipf_keys(rng, m, k, 0.8) + (rng.random(m) < 0.05)  # some misses (keys are 3 apart)
+    S = struct([fk, large(m) if case == "build_only" else small(m)], [I64, I64])
+    want = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ, buckets=n)
+    got, st = ctx.hashjoin_agg(dev_rel(torch_cuda, R, [I64, I64]), [0], dev_rel(torch_cuda, S, [I64, I64]), [0], PROJ,
+                               pyg.JOIN_RADIX, bits, stats=True)
+    assert got == want
+    assert st.build_packed == (case != "probe_only")
+    assert st.probe_packed == (case != "build_only")
+
+
+def test_radix_packed_frame_missed_redoes(ctx, torch_cuda):
+    """A probe side of 2^25 tuples is laid out from a strided sample, which
+    also gives the frame of its packed words.  One payload that no sampled
+    tuple shows lies far outside that frame: the first pass flags it, and
+    the probe side is redone from an exact histogram (whose exact ranges no
+    longer fit 32 bits, so the redo is unpacked).  Same result as the
+    oracle."""
+    rng = np.random.default_rng(23)
+    n, m = 1 << 16, 1 << 25
+    k = rng.permutation(n).astype(np.int64) + 1
+    R = struct([k, k * 7], [I64, I64])
+    pay = rng.integers(0, 1 << 20, m)
+    pay[1] = 1 << 45  # index 1: between two sampled tuples
+    S = struct([k[rng.integers(0, n, m)], pay], [I64, I64])
+    want = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ, buckets=n)
+    got, st = ctx.hashjoin_agg(dev_rel(torch_cuda, R, [I64, I64]), [0], dev_rel(torch_cuda, S, [I64, I64]), [0], PROJ,
+                               pyg.JOIN_RADIX, 12, stats=True)
+    assert got == want
+    assert st.overflow_tuples == 1 and st.build_packed == 1 and st.probe_packed == 0
 
 
 def test_empty_sides(ctx, torch_cuda):
