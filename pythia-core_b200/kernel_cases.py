@@ -54,7 +54,7 @@ def case_join(torch, ctx, a, algo, nR, nS):
     Rr, Sr = pyg.Rel(R, nR, [I64, I64]), pyg.Rel(S, nS, [I64, I64])
     want = expect_pkfk(S, nS)
     for _ in range(a.reps):
-        cnt, (sb, sp) = ctx.hashjoin_agg(Rr, [0], Sr, [0], [(0, 1), (1, 1)], algo)
+        cnt, (sb, sp) = ctx.hashjoin_agg(Rr, [0], Sr, [0], [(0, 1), (1, 1)], algo, a.bits)
         assert cnt == nS and (sb + sp) & 0xFFFFFFFFFFFFFFFF == want
 
 
@@ -161,6 +161,7 @@ def main():
     ap.add_argument("--shift", type=int, default=0, help="shrink the inputs by 2^shift")
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--theta", type=float, default=0.0)
+    ap.add_argument("--bits", type=int, default=0, help="radix: log2 partition fan-out (0 = automatic)")
     a = ap.parse_args()
     import torch
 
