@@ -138,12 +138,16 @@ int pyg_hashjoin_probe_materialize(pyg_ctx* ctx, const pyg_hashtable* ht, const 
 /* One-shot join + aggregate (build and probe in one call), the plan
  * hashjoin -> aggregate_sum of the reference (HashJoinOp::scanStart +
  * getNext, operators/join.cpp:548-757, feeding GenericAggregate).
- * PYG_JOIN_DIRECT: one table in HBM, probed in input order.
+ * PYG_JOIN_DIRECT: one table in HBM, probed in input order; for 16-byte
+ * device relations a three-launch call with one host synchronisation whose
+ * table lives in a buffer the context keeps between calls.
  * PYG_JOIN_RADIX: both sides partitioned by the top radix_bits bits of the
- * key hash first, so each partition's probes hit one L2-sized slice of the
- * table (16-byte (int64, int64) device relations, projection over
+ * key hash first, then joined partition by partition with shared-memory
+ * tables (16-byte (int64, int64) device relations, projection over
  * {B$1, P$1}; other shapes use DIRECT).  PYG_JOIN_AUTO picks RADIX for
- * large eligible inputs.  stats (optional) receives phase timings. */
+ * eligible inputs whose direct table would exceed 64 MB (so not stay in
+ * L2) and whose probe side has at least 2^22 tuples.  stats (optional)
+ * receives phase timings. */
 #define PYG_JOIN_AUTO   0
 #define PYG_JOIN_DIRECT 1
 #define PYG_JOIN_RADIX  2

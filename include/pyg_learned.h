@@ -26,12 +26,16 @@ typedef struct pyg_cdf pyg_cdf;
 
 typedef struct pyg_cdf_train_opts {
     int32_t leaves;              /* second-level linear leaves (e.g. 1024) */
-    int32_t epochs;              /* full-batch gradient steps             */
+    int32_t epochs;              /* full-batch gradient steps (leaves)    */
     float lr;                    /* Adam step size                        */
     uint64_t seed;
 } pyg_cdf_train_opts;
 
-/* Trains the model on n device int64 sample keys (any order). */
+/* Trains the model on n device int64 sample keys (any order): the root and
+ * every leaf start from their least-squares lines (one pass of sums each),
+ * then the leaves take `epochs` projected-Adam steps through the forward /
+ * backward kernels.  A few epochs at a small step size fine-tune; the
+ * least-squares start already holds most of the fit. */
 int pyg_cdf_train(pyg_ctx* ctx, const int64_t* sample_keys, int64_t n, const pyg_cdf_train_opts* opts,
                   pyg_cdf** out);
 int pyg_cdf_free(pyg_ctx* ctx, pyg_cdf* model);

@@ -429,9 +429,17 @@ int64_t orc_sortlimit(const orc_rel* in, const int* by, int nby, int asc, int64_
     int64_t* list = (int64_t*)malloc(sizeof(int64_t) * (size_t)(limit + 1));
     int64_t size = 0;
     for (int64_t i = 0; i < in->ntuples; ++i) {
-        int64_t pos = 0;
-        while (pos < size && !orc_ahead(in, i, list[pos], by, nby, asc)) ++pos;
-        if (pos == size && size == limit) continue;  /* ahead of none while full */
+        /* The list is ordered, so the walk's stopping point (the first
+         * tuple this one is ahead of) is found by binary search, and a full
+         * list whose tail this tuple is not ahead of rejects it at once. */
+        if (size == limit && !orc_ahead(in, i, list[size - 1], by, nby, asc)) continue;
+        int64_t lo = 0, hi = size;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) / 2;
+            if (orc_ahead(in, i, list[mid], by, nby, asc)) hi = mid;
+            else lo = mid + 1;
+        }
+        const int64_t pos = lo;
         memmove(list + pos + 1, list + pos, sizeof(int64_t) * (size_t)(size - pos));
         list[pos] = i;
         if (size < limit) ++size;                   /* else the tail dropped off */

@@ -17,12 +17,17 @@
 
 namespace pyg {
 
+// A fragment's table: cap 16-byte slots {key, payload sum} (one 128-bit CAS
+// stores a fresh key with its payload) and cap 32-bit counters of extra
+// copies of a key, touched only by repeated build keys.  At the default
+// load factor the largest fragment's slots stay inside L2.
 struct FragDesc {
     const longlong2* build;
     int64_t nb;
     const longlong2* probe;
     int64_t np;
-    ulonglong4* table;  // {key, payload sum, count, -}
+    ulonglong2* table;
+    unsigned* extra;
     uint64_t cap;
     int32_t n_init, n_build, n_probe, pad;
 };
@@ -54,7 +59,15 @@ struct BatchDev {
     unsigned int* probe_done;
     unsigned long long* res;     // RES_WORDS per fragment
     unsigned long long* t_done;  // per fragment completion time
+    unsigned int* dup;           // per fragment: a build key repeated
 };
+
+constexpr int BATCH_U = 4;  // probe / build tuples in flight per thread
+
+__device__ __forceinline__ unsigned __int128 bslot(uint64_t key, uint64_t pay)
+{
+    return ((unsigned __int128)pay << 64) | (unsigned __int128)key;
+}
 
 __device__ __forceinline__ unsigned long long gtimer()
 {
@@ -81,9 +94,10 @@ __device__ bool wait_count(const unsigned int* ctr, unsigned int target, BatchSt
 __global__ void __launch_bounds__(1024) batch_kernel(BatchDev d)
 {
     __shared__ long long item;
-    __shared__ int ok;
+    __shared__ int ok, dupf;
     __shared__ unsigned long long red[RES_WORDS];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(&d.st->t0, 0ULL, gtimer());
+    const unsigned __int128 empty = bslot(kEmptyKey, 0);
     for (;;) {
         if (threadIdx.x == 0) item = (long long)atomicAdd(&d.st->next, 1ULL);
         __syncthreads();
@@ -96,57 +110,106 @@ __global__ void __launch_bounds__(1024) batch_kernel(BatchDev d)
             if (w.kind == 1) ok = wait_count(&d.init_done[w.frag], (unsigned)f.n_init, d.st);
             if (w.kind == 2) ok = wait_count(&d.build_done[w.frag], (unsigned)f.n_build, d.st);
             __threadfence();
+            dupf = w.kind == 2 ? (int)*(volatile unsigned*)&d.dup[w.frag] : 0;
         }
         __syncthreads();
+        const int64_t stride = blockDim.x;
         if (w.kind == 0) {
-            for (int64_t s = w.begin + threadIdx.x; s < w.end; s += blockDim.x)
-                f.table[s] = make_ulonglong4(kEmptyKey, 0, 0, 0);
+            for (int64_t s = w.begin + threadIdx.x; s < w.end; s += stride) {
+                f.table[s] = make_ulonglong2(kEmptyKey, 0);
+                f.extra[s] = 0;
+            }
         } else if (w.kind == 1 && ok) {
+            // BATCH_U inserts in flight per thread: loads, the first 128-bit
+            // CAS of each, then the chains.  A repeated key adds its payload
+            // and one to the slot's extra-copies counter.
             uint64_t ec = 0, es = 0;
-            for (int64_t i = w.begin + threadIdx.x; i < w.end; i += blockDim.x) {
-                longlong2 t = f.build[i];
-                uint64_t k = (uint64_t)t.x;
-                if (k == kEmptyKey) {
-                    ++ec;
-                    es += (uint64_t)t.y;
-                    continue;
+            bool dup = false;
+            for (int64_t i0 = w.begin + threadIdx.x; i0 < w.end; i0 += stride * BATCH_U) {
+                longlong2 t[BATCH_U];
+                uint64_t s[BATCH_U];
+                unsigned long long pv[BATCH_U];
+#pragma unroll
+                for (int u = 0; u < BATCH_U; ++u) {
+                    const int64_t i = i0 + u * stride;
+                    t[u] = i < w.end ? __ldcs(&f.build[i]) : make_longlong2((long long)kEmptyKey, 0);
                 }
-                uint64_t s = reduce_range(mix64(k), f.cap);
-                for (uint64_t steps = 0; steps < f.cap; ++steps) {
-                    unsigned long long* slot = (unsigned long long*)&f.table[s];
-                    unsigned long long prev = atomicCAS(slot, kEmptyKey, k);
-                    if (prev == kEmptyKey || prev == k) {
-                        atomicAdd(slot + 1, (unsigned long long)t.y);
-                        atomicAdd(slot + 2, 1ULL);
-                        break;
+#pragma unroll
+                for (int u = 0; u < BATCH_U; ++u) {
+                    const uint64_t k = (uint64_t)t[u].x;
+                    s[u] = reduce_range(mix64(k), f.cap);
+                    pv[u] = k == kEmptyKey ? ~0ULL
+                                           : (unsigned long long)atomicCAS((unsigned __int128*)&f.table[s[u]], empty,
+                                                                           bslot(k, (uint64_t)t[u].y));
+                }
+#pragma unroll
+                for (int u = 0; u < BATCH_U; ++u) {
+                    if (i0 + u * stride >= w.end) continue;
+                    const uint64_t k = (uint64_t)t[u].x;
+                    if (k == kEmptyKey) {
+                        ++ec;
+                        es += (uint64_t)t[u].y;
+                        continue;
                     }
-                    s = (s + 1 == f.cap) ? 0 : s + 1;
+                    uint64_t ss = s[u];
+                    unsigned long long p = pv[u];
+                    // cap > build tuples, so the chain ends at a free slot or the key.
+                    for (uint64_t steps = 1; p != kEmptyKey && p != k && steps < f.cap; ++steps) {
+                        ss = (ss + 1 == f.cap) ? 0 : ss + 1;
+                        p = (unsigned long long)atomicCAS((unsigned __int128*)&f.table[ss], empty,
+                                                          bslot(k, (uint64_t)t[u].y));
+                    }
+                    if (p == k) {
+                        dup = true;
+                        atomicAdd(&f.table[ss].y, (unsigned long long)t[u].y);
+                        atomicAdd(&f.extra[ss], 1u);
+                    }
                 }
             }
             if (ec) {
                 atomicAdd(&red[2], (unsigned long long)ec);
                 atomicAdd(&red[3], (unsigned long long)es);
             }
+            if (__any_sync(0xffffffffu, dup) && (threadIdx.x & 31) == 0) atomicOr(&d.dup[w.frag], 1u);
         } else if (w.kind == 2 && ok) {
+            // BATCH_U independent lookups in flight per thread; the table
+            // of the fragment being probed is L2-resident.
             uint64_t cnt = 0, sum = 0, ec = 0, es = 0;
-            for (int64_t i = w.begin + threadIdx.x; i < w.end; i += blockDim.x) {
-                longlong2 t = __ldcs(&f.probe[i]);
-                uint64_t k = (uint64_t)t.x;
-                if (k == kEmptyKey) {
-                    ++ec;
-                    es += (uint64_t)t.y;
-                    continue;
+            const bool dup = dupf != 0;
+            for (int64_t i0 = w.begin + threadIdx.x; i0 < w.end; i0 += stride * BATCH_U) {
+                longlong2 t[BATCH_U];
+                uint64_t s[BATCH_U];
+                ulonglong2 e[BATCH_U];
+#pragma unroll
+                for (int u = 0; u < BATCH_U; ++u) {
+                    const int64_t i = i0 + u * stride;
+                    t[u] = i < w.end ? __ldcs(&f.probe[i]) : make_longlong2((long long)kEmptyKey, 0);
                 }
-                uint64_t s = reduce_range(mix64(k), f.cap);
-                for (uint64_t steps = 0; steps < f.cap; ++steps) {
-                    ulonglong4 e = f.table[s];
-                    if (e.x == k) {
-                        cnt += e.z;
-                        sum += e.y + e.z * (uint64_t)t.y;
-                        break;
+#pragma unroll
+                for (int u = 0; u < BATCH_U; ++u) {
+                    s[u] = reduce_range(mix64((uint64_t)t[u].x), f.cap);
+                    e[u] = f.table[s[u]];
+                }
+#pragma unroll
+                for (int u = 0; u < BATCH_U; ++u) {
+                    if (i0 + u * stride >= w.end) continue;
+                    const uint64_t k = (uint64_t)t[u].x;
+                    if (k == kEmptyKey) {
+                        ++ec;
+                        es += (uint64_t)t[u].y;
+                        continue;
                     }
-                    if (e.x == kEmptyKey) break;
-                    s = (s + 1 == f.cap) ? 0 : s + 1;
+                    uint64_t ss = s[u];
+                    ulonglong2 ee = e[u];
+                    for (uint64_t steps = 1; ee.x != k && ee.x != kEmptyKey && steps < f.cap; ++steps) {
+                        ss = (ss + 1 == f.cap) ? 0 : ss + 1;
+                        ee = f.table[ss];
+                    }
+                    if (ee.x == k) {
+                        const uint64_t c = dup ? 1ULL + f.extra[ss] : 1ULL;
+                        cnt += c;
+                        sum += ee.y + c * (uint64_t)t[u].y;
+                    }
                 }
             }
             cnt = warp_sum_u64(cnt);
@@ -205,7 +268,7 @@ static pyg_tuning default_tuning()
     pyg_tuning t;
     t.block_threads = 512;
     t.blocks_per_sm = 2;
-    t.load_factor = 0.5f;
+    t.load_factor = 0.7f;  // 16-byte slots: a 2^22-tuple build's table (96 MB) stays in L2
     t.chunk_tuples = 16384;
     t.fanout = 0;
     return t;
@@ -281,7 +344,8 @@ int pyg_batch_create(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const p
     pyg_batch* b = new pyg_batch();
     b->n = n;
     b->tuning = t;
-    // Tables: one arena, per-fragment capacity nbuild / load factor.
+    // Tables: one arena of 16-byte slots and one of extra-copy counters,
+    // per-fragment capacity nbuild / load factor.
     std::vector<FragDesc> fd(n);
     uint64_t total_slots = 0;
     for (int i = 0; i < n; ++i) {
@@ -289,8 +353,10 @@ int pyg_batch_create(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const p
         fd[i].cap = cap;
         total_slots += cap;
     }
-    ulonglong4* arena;
-    if ((rc = batch_alloc(ctx, b, (void**)&arena, total_slots * sizeof(ulonglong4)))) {
+    ulonglong2* arena;
+    unsigned* extra;
+    if ((rc = batch_alloc(ctx, b, (void**)&arena, total_slots * sizeof(ulonglong2))) ||
+        (rc = batch_alloc(ctx, b, (void**)&extra, total_slots * sizeof(unsigned)))) {
         pyg_batch_free(ctx, b);
         return rc;
     }
@@ -316,6 +382,7 @@ int pyg_batch_create(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const p
         f.probe = (const longlong2*)frags[i].probe;
         f.np = frags[i].nprobe;
         f.table = arena + toff[i];
+        f.extra = extra + toff[i];
         f.n_init = f.n_build = f.n_probe = 0;
         for (uint64_t s = 0; s < f.cap; s += (uint64_t)grain * 2, ++f.n_init)
             items.push_back({i, 0, (int64_t)s, (int64_t)std::min<uint64_t>(f.cap, s + grain * 2)});
@@ -328,7 +395,7 @@ int pyg_batch_create(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const p
     for (int i = 0; i < n; ++i) b->empty_frag[i] = (fd[i].n_build == 0 && fd[i].n_probe == 0);
     FragDesc* dfd;
     WorkItem* ditems;
-    b->state_bytes = sizeof(BatchState) + (size_t)n * (3 * sizeof(unsigned) + (RES_WORDS + 1) * 8) + 64;
+    b->state_bytes = sizeof(BatchState) + (size_t)n * (4 * sizeof(unsigned) + (RES_WORDS + 1) * 8) + 64;
     if ((rc = batch_alloc(ctx, b, (void**)&dfd, n * sizeof(FragDesc))) ||
         (rc = batch_alloc(ctx, b, (void**)&ditems, items.size() * sizeof(WorkItem))) ||
         (rc = batch_alloc(ctx, b, &b->state, b->state_bytes))) {
@@ -352,6 +419,7 @@ int pyg_batch_create(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const p
     b->dev.init_done = (unsigned*)sp;
     b->dev.build_done = b->dev.init_done + n;
     b->dev.probe_done = b->dev.build_done + n;
+    b->dev.dup = b->dev.probe_done + n;
 
     // Capture: reset the state, run the persistent kernel.
     int grid = ctx->sm_count * t.blocks_per_sm;
@@ -432,7 +500,7 @@ int pyg_batch_run_plain(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, int6
         S.ntuples = frags[i].nprobe;
         int32_t k = 0;
         pyg_proj proj[2] = {{0, 1}, {1, 1}};
-        pyg_join_opts o = {PYG_JOIN_DIRECT, 0, 0.5f, 0};
+        pyg_join_opts o = {PYG_JOIN_AUTO, 0, 0.5f, 0};  // the best single-call algorithm per fragment
         pyg_join_result r;
         rc = pyg_hashjoin_agg(ctx, &R, &k, &S, &k, 1, proj, 2, &o, &r, nullptr);
         cudaEventRecord(ev[i + 1], ctx->stream);
@@ -501,7 +569,7 @@ int pyg_autotune(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const char*
     // Candidate grid: block shape x occupancy x load factor x grain.
     const int bts[] = {256, 512, 1024};
     const int bps[] = {1, 2, 4};
-    const float lfs[] = {0.5f, 0.7f};
+    const float lfs[] = {0.5f, 0.7f, 0.8f};
     const int chunks[] = {4096, 16384, 65536};
     float best = 1e30f;
     pyg_tuning best_t = default_tuning();

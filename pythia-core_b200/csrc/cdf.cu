@@ -8,10 +8,13 @@
 //   u = clamp(L * r - l, 0, 1)                  leaf-local coordinate
 //   cdf = ylo_l + (yhi_l - ylo_l) * clamp(a_l * u + b_l, 0, 1)
 // The root is fitted to y_i = i / n of the sorted sample, then each leaf to
-// its samples' targets normalised to the leaf's y range.  Training is full
-// batch, projected Adam (slopes kept >= 0 so the model stays monotone),
-// with the step size decayed to 1% over the epochs.  Residual arithmetic
-// is fp64; parameters are fp32.
+// its samples' targets normalised to the leaf's y range.  The root is the
+// least-squares line (one pass of sums; it minimises the root's loss, so no
+// steps follow), and so is each leaf to start with; the leaves then take
+// `epochs` full-batch steps of projected Adam (slopes kept >= 0 so the
+// model stays monotone) with the step size decayed to 1% over the epochs,
+// through the forward and backward kernels.  Residual arithmetic is fp64;
+// parameters are fp32.
 #include <math.h>
 #include <string.h>
 
@@ -189,6 +192,101 @@ __global__ void __launch_bounds__(CDF_THREADS) leaf_backward_kernel(int64_t n, c
     }
 }
 
+// Closed-form start (the linear models of a recursive model index, Kraska
+// et al., SIGMOD 2018, each fitted by least squares): root sums over the
+// sorted sample, acc = {sum x, sum x^2, sum y, sum x y} with y = i / n.
+__global__ void __launch_bounds__(CDF_THREADS) root_ls_kernel(const int64_t* __restrict__ keys, int64_t n, double lo,
+                                                              double scale, double* __restrict__ acc)
+{
+    double sx = 0, sxx = 0, sy = 0, sxy = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double x = norm_key(keys[i], lo, scale), y = (double)i / (double)n;
+        sx += x;
+        sxx += x * x;
+        sy += y;
+        sxy += x * y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sxx += __shfl_xor_sync(0xffffffffu, sxx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        sxy += __shfl_xor_sync(0xffffffffu, sxy, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&acc[0], sx);
+        atomicAdd(&acc[1], sxx);
+        atomicAdd(&acc[2], sy);
+        atomicAdd(&acc[3], sxy);
+    }
+}
+
+// Least-squares line through c points from their sums; the slope is kept
+// >= 0 (a monotone model), the intercept refitted when it is clamped.
+__device__ __forceinline__ void ls_line(double c, double sx, double sxx, double sy, double sxy, float* a, float* b)
+{
+    if (c < 1) {
+        *a = 1.f;
+        *b = 0.f;
+        return;
+    }
+    const double den = c * sxx - sx * sx;
+    double s = den > 1e-12 * c * c ? (c * sxy - sx * sy) / den : 0.0;
+    if (s < 0) s = 0;
+    *a = (float)s;
+    *b = (float)((sy - s * sx) / c);
+}
+
+__global__ void root_solve_kernel(const double* __restrict__ acc, int64_t n, float* __restrict__ params)
+{
+    ls_line((double)n, acc[0], acc[1], acc[2], acc[3], &params[0], &params[1]);
+}
+
+// Per-leaf least-squares sums of the leaf-local target t against u:
+// s[5l .. 5l+4] = {count, sum u, sum u^2, sum t, sum u t}.
+__global__ void __launch_bounds__(CDF_THREADS) leaf_ls_kernel(int64_t n, const int* __restrict__ leaf,
+                                                              const double* __restrict__ u,
+                                                              const double* __restrict__ yr, double* __restrict__ s)
+{
+    const unsigned lane = threadIdx.x & 31;
+    for (int64_t wb = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u); wb < n;
+         wb += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = wb + lane;
+        const bool valid = i < n;
+        const int l = valid ? leaf[i] : -1;
+        double v[5] = {0, 0, 0, 0, 0};
+        if (valid) {
+            const double ylo = yr[2 * l], yhi = yr[2 * l + 1];
+            const double t = yhi > ylo ? ((double)i / (double)n - ylo) / (yhi - ylo) : 0.0;
+            const double uu = u[i];
+            v[0] = 1;
+            v[1] = uu;
+            v[2] = uu * uu;
+            v[3] = t;
+            v[4] = uu * t;
+        }
+        const int l0 = __shfl_sync(0xffffffffu, l, 0);
+        if (__all_sync(0xffffffffu, !valid || l == l0)) {
+#pragma unroll
+            for (int k = 0; k < 5; ++k)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+            if (lane == 0)
+                for (int k = 0; k < 5; ++k) atomicAdd(&s[5 * l0 + k], v[k]);
+        } else if (valid) {
+            for (int k = 0; k < 5; ++k) atomicAdd(&s[5 * l + k], v[k]);
+        }
+    }
+}
+
+__global__ void leaf_solve_kernel(const double* __restrict__ s, int L, float* __restrict__ params)
+{
+    for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < L; l += gridDim.x * blockDim.x) {
+        const double* q = s + 5 * l;
+        ls_line(q[0], q[1], q[2], q[3], q[4], &params[2 + 2 * l], &params[3 + 2 * l]);
+    }
+}
+
 __global__ void root_to_raw_kernel(const double* __restrict__ acc, double* __restrict__ raw)
 {
     raw[0] = acc[1];
@@ -301,10 +399,11 @@ struct CdfWork {
     double* gscale = nullptr;  // 1 + L gradient scales (root, leaves)
     double* acc = nullptr;     // root: e^2, e x, e ; then per-leaf loss sums (L)
     LeafStat* st = nullptr;
+    double* ls = nullptr;      // least-squares sums: 4 (root), then 5 per leaf
     void release(pyg_ctx* ctx)
     {
         dfree(ctx, leaf); dfree(ctx, u); dfree(ctx, g); dfree(ctx, raw); dfree(ctx, gscale); dfree(ctx, acc);
-        dfree(ctx, st);
+        dfree(ctx, st); dfree(ctx, ls);
     }
     int alloc(pyg_ctx* ctx, int64_t n, int L)
     {
@@ -316,7 +415,9 @@ struct CdfWork {
         if ((rc = dalloc(ctx, (void**)&gscale, (size_t)(1 + L) * 8))) return rc;
         if ((rc = dalloc(ctx, (void**)&acc, (size_t)(3 + L) * 8))) return rc;
         if ((rc = dalloc(ctx, (void**)&st, (size_t)L * sizeof(LeafStat)))) return rc;
+        if ((rc = dalloc(ctx, (void**)&ls, (size_t)(4 + 5 * L) * 8))) return rc;
         PYG_CUDA(cudaMemsetAsync(raw, 0, (size_t)(2 + 2 * L) * 8, ctx->stream));
+        PYG_CUDA(cudaMemsetAsync(ls, 0, (size_t)(4 + 5 * L) * 8, ctx->stream));
         return PYG_OK;
     }
 };
@@ -340,9 +441,44 @@ static int cdf_assign(pyg_ctx* ctx, CdfWork& w, const int64_t* keys, int64_t n, 
     return PYG_OK;
 }
 
+// Packed key words of every step-th tuple (m of them).
+__global__ void key_sample_kernel(const uint8_t* __restrict__ base, int64_t m, int64_t step, int32_t tb, KeySpec ks,
+                                  int64_t* __restrict__ out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (int64_t)load_key(base + i * step * tb, ks);
+}
+
 }  // namespace pyg
 
 using namespace pyg;
+
+namespace pyg {
+
+int estimate_distinct_keys(pyg_ctx* ctx, const uint8_t* base, int64_t n, int32_t tb, const KeySpec& ks,
+                           int64_t* out)
+{
+    const int64_t m = n < CDF_ESTIMATE_SAMPLE ? n : CDF_ESTIMATE_SAMPLE;
+    const int64_t step = n / m;
+    int64_t* sample = nullptr;
+    int rc = dalloc(ctx, (void**)&sample, (size_t)m * 8);
+    if (rc) return rc;
+    key_sample_kernel<<<grid_for(ctx, m, 256, 4, 4), 256, 0, ctx->stream>>>(base, m, step, tb, ks, sample);
+    PYG_LAUNCHED(ctx);
+    pyg_cdf_train_opts o;
+    o.leaves = 64;
+    o.epochs = 1;
+    o.lr = 0.001f;
+    o.seed = 1;
+    pyg_cdf* model = nullptr;
+    rc = pyg_cdf_train(ctx, sample, m, &o, &model);
+    if (!rc) rc = pyg_cdf_estimate_distinct(ctx, model, n, out);
+    pyg_cdf_free(ctx, model);
+    dfree(ctx, sample);
+    return rc;
+}
+
+}  // namespace pyg
 
 extern "C" {
 
@@ -431,19 +567,20 @@ int pyg_cdf_train(pyg_ctx* ctx, const int64_t* sample_keys, int64_t n, const pyg
         PYG_CUDA(cudaMemcpyAsync(w.gscale, &root_scale, 8, cudaMemcpyHostToDevice, ctx->stream));
         int gr = grid_for(ctx, n, CDF_THREADS, 4, 8);
         const int E = opts->epochs;
-        // Root: forward+backward, then Adam on (a0, b0).
-        for (int e = 1; e <= E; ++e) {
-            float lr = opts->lr * powf(0.01f, (float)(e - 1) / (float)E);
-            PYG_CUDA(cudaMemsetAsync(w.acc, 0, 24, ctx->stream));
-            root_fwd_bwd_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(sorted, n, m->key_lo, m->key_scale, m->d_params, w.acc);
-            root_to_raw_kernel<<<1, 1, 0, ctx->stream>>>(w.acc, w.raw);
-            adam_kernel<<<1, 32, 0, ctx->stream>>>(m->d_params, w.raw, w.gscale, adam, adam + 2 + 2 * L, 2, lr, e);
-            ctx->launches += 3;
-        }
+        // Root: the least-squares line in one pass (the exact minimiser of
+        // the root's squared loss, so no gradient steps follow).
+        root_ls_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(sorted, n, m->key_lo, m->key_scale, w.ls);
+        root_solve_kernel<<<1, 1, 0, ctx->stream>>>(w.ls, n, m->d_params);
+        ctx->launches += 2;
         PYG_CUDA(cudaGetLastError());
-        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
         if ((rc = cdf_assign(ctx, w, sorted, n, L, m->key_lo, m->key_scale, m->d_params, m->d_yr))) break;
-        // Leaves: forward (residuals), backward (per-leaf gradient sums), Adam.
+        // Leaves: least-squares lines from one pass of per-leaf sums, then
+        // E epochs of forward (residuals), backward (per-leaf gradient
+        // sums) and projected Adam, which keep the slopes >= 0.
+        leaf_ls_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(n, w.leaf, w.u, m->d_yr, w.ls + 4);
+        leaf_solve_kernel<<<grid_for(ctx, L, 256, 1, 4), 256, 0, ctx->stream>>>(w.ls + 4, L, m->d_params);
+        ctx->launches += 2;
+        PYG_CUDA(cudaGetLastError());
         int ga = grid_for(ctx, 2 + 2 * L, 256, 1, 4);
         for (int e = 1; e <= E; ++e) {
             float lr = opts->lr * powf(0.01f, (float)(e - 1) / (float)E);

@@ -310,6 +310,19 @@ extern "C" int pyg_groupby(pyg_ctx* ctx, const pyg_rel* in, const int32_t* key_c
         return PYG_OK;
     }
 
+    // No group estimate from the caller (the plan's hash.buckets): on large
+    // inputs the learned CDF model's distinct-key estimate from a key
+    // sample stands in, so that tables are sized for the keys at hand and
+    // 16-byte tuples take the shared-memory paths.  A wrong estimate costs
+    // time only.
+    if (expected_groups <= 0 && in->ntuples >= ((int64_t)1 << 20)) {
+        int64_t est = 0;
+        if ((rc = estimate_distinct_keys(ctx, (const uint8_t*)R.rel.base, in->ntuples, in->tuple_bytes, ks, &est))) {
+            R.release(ctx);
+            return rc;
+        }
+        expected_groups = est > 0 ? est : 0;
+    }
     GroupArgs a;
     memset(&a, 0, sizeof(a));
     a.base = (const uint8_t*)R.rel.base;

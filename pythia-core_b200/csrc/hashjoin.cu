@@ -979,8 +979,12 @@ int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_ke
     bool eligible = nkeys == 1 && is16(build, build_keys) && is16(probe, probe_keys) && nproj <= 2 && npay <= 1;
     for (int p = 0; eligible && p < nproj; ++p) eligible = proj[p].col == 1;
     if (eligible && nproj == 2) eligible = proj[0].side != proj[1].side;
+    // AUTO: the direct join while its table (16 bytes per slot at load
+    // factor lf) fits well inside the 126 MB L2, the radix join beyond.
+    const double table_bytes = 16.0 * (double)build->ntuples / (double)lf;
     bool radix = eligible && (algorithm == PYG_JOIN_RADIX ||
-                              (algorithm == PYG_JOIN_AUTO && probe->ntuples >= ((int64_t)1 << 24)));
+                              (algorithm == PYG_JOIN_AUTO && table_bytes > 64.0 * 1024 * 1024 &&
+                               probe->ntuples >= ((int64_t)1 << 22)));
     PhaseTimer tm;
     if (!radix && eligible) {
         // 16-byte device relations: the one-shot direct join (falls back

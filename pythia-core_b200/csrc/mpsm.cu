@@ -508,8 +508,9 @@ static int mpsm_run(pyg_ctx* ctx, const pyg_rel* build, int32_t bkey, const pyg_
             } else {
                 pyg_cdf_train_opts to;
                 to.leaves = o->cdf_leaves > 0 ? o->cdf_leaves : 1024;
-                to.epochs = 200;
-                to.lr = 0.05f;
+                // Least-squares start, then a short fine-tuning of the leaves.
+                to.epochs = 4;
+                to.lr = 0.002f;
                 to.seed = o->seed;
                 pyg_cdf* model = nullptr;
                 if ((rc = pyg_cdf_train(ctx, sample, ns, &to, &model))) return fail(rc);

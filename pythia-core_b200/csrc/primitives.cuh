@@ -37,6 +37,14 @@ __host__ __device__ __forceinline__ uint64_t packed_to_sortable(uint64_t k, int 
     return nkeys == 2 ? (k ^ 0x8000000080000000ULL) : (k ^ 0x8000000000000000ULL);
 }
 
+// Distinct-key estimate for n tuples (device, tb bytes each) from the
+// packed keys of a strided sample of CDF_ESTIMATE_SAMPLE tuples: the GEE
+// estimate carried by the learned CDF model trained on that sample
+// (cdf.cu).  Sizes hash tables when a caller gives no group estimate.
+constexpr int64_t CDF_ESTIMATE_SAMPLE = (int64_t)1 << 18;
+int estimate_distinct_keys(pyg_ctx* ctx, const uint8_t* base, int64_t n, int32_t tb, const KeySpec& ks,
+                           int64_t* out);
+
 // Gather rows: out[i] = in[idx[i]] for tuples of tb bytes.
 int gather_rows(pyg_ctx* ctx, const uint8_t* in, const uint64_t* idx, int64_t n, int32_t tb, uint8_t* out);
 

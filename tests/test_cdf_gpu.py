@@ -135,3 +135,29 @@ def test_sampled_splitters_are_quantiles(ctx, torch_cuda):
     srt = np.sort(keys)
     want = srt[np.ceil(np.arange(1, fan) * len(keys) / fan).astype(np.int64)]
     assert np.array_equal(out, want)
+
+
+@pytest.mark.parametrize("theta", [1.0, 1.5])
+def test_learned_vs_sampled_splitters_on_mpsm_join(ctx, torch_cuda, theta):
+    """What the trained model gains over the method without it, on the
+    skewed MPSM join: the same join result; a max-partition imbalance no
+    worse than sample quantiles (heavy keys get ranges of their own); and a
+    splitter cost (sample, sort, least-squares start, fine-tuning epochs)
+    of a few milliseconds, not the tens a long gradient training took."""
+    torch = torch_cuda
+    nR, nS = 1 << 22, 1 << 24
+    R = torch.empty(nR * 2, dtype=torch.int64, device="cuda")
+    S = torch.empty(nS * 2, dtype=torch.int64, device="cuda")
+    ctx.gen_pk(R, nR, 7, 31)
+    ctx.gen_fk(S, nS, nR, theta, 31, 1 << 20, 32)
+    Rr, Sr = pyg.Rel(R, nR, [pyg.INT64, pyg.INT64]), pyg.Rel(S, nS, [pyg.INT64, pyg.INT64])
+    res = {}
+    for kind in (pyg.MPSM_SAMPLED, pyg.MPSM_LEARNED):
+        opts = ctx.mpsm_opts(kind, 4096, 0.01, 1024)
+        ctx.mpsm_join_agg(Rr, 0, Sr, 0, [(0, 1), (1, 1)], opts)  # warm
+        cnt, sums, st = ctx.mpsm_join_agg(Rr, 0, Sr, 0, [(0, 1), (1, 1)], opts)
+        res[kind] = (cnt, sums, st.max_partition_imbalance, st.splitter_ms)
+    assert res[pyg.MPSM_LEARNED][:2] == res[pyg.MPSM_SAMPLED][:2]
+    assert res[pyg.MPSM_LEARNED][0] == nS
+    assert res[pyg.MPSM_LEARNED][2] <= 1.05 * res[pyg.MPSM_SAMPLED][2] + 0.1
+    assert res[pyg.MPSM_LEARNED][3] < 5.0, res
