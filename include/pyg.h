@@ -260,6 +260,15 @@ int pyg_sort(pyg_ctx* ctx, const pyg_rel* in, int32_t key_col, void* out);
 int pyg_sortlimit(pyg_ctx* ctx, const pyg_rel* in, const int32_t* key_cols, int32_t nkeys, int32_t asc,
                   int64_t limit, void* out, int64_t out_capacity, int64_t* out_n);
 
+/* Replaces TupleBuffer::bitonicsort (util/buffer.cpp:97-110) and its SIMD
+ * merge sort (util/bitonicsort.cpp:59-74, 371-443): sorts n 8-byte records
+ * {int32 rid; int32 key} of device buffer `records` in place by the signed
+ * key.  4096-record pages are bitonic-sorted in shared memory (each page
+ * brought in by one bulk copy), then merged.  Equal keys end in rid order
+ * (the reference leaves it open).  The reference requires n = 2^k > 4096;
+ * any n works here.  records must be 16-byte aligned. */
+int pyg_bitonic_sort(pyg_ctx* ctx, void* records, int64_t n);
+
 /* Replaces TupleBuffer::findsmallest<KeyT> (util/buffer.inl:~300-452):
  * for each of nq query keys (device array), the index of the first tuple
  * of the sorted relation whose key is >= the query. */

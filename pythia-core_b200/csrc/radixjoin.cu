@@ -254,6 +254,121 @@ __global__ void __launch_bounds__(RJ_JOIN_THREADS, RJ_JOIN_BLOCKS) rj_join_kerne
 }
 
 // ---------------------------------------------------------------------------
+// Join of packed partitions that share one key frame.  The low halves of
+// both relations' words are then comparable 32-bit key offsets, so a table
+// slot is the build word itself (key offset, payload offset): 8 bytes, one
+// 64-bit CAS to insert, one 64-bit shared load per probe, no key decoding,
+// and a 32-bit slot hash.  Offsets never reach 2^32 - 1, so the all-ones
+// word marks an empty slot.  Two 512-thread CTAs per SM, 96 KB tables of
+// 12288 slots (a build chunk fills at most half).  Sums are kept over the
+// payload offsets and rebased at the end: sum = count x base + sum of
+// offsets, modulo 2^64.
+
+constexpr int RJ32_THREADS = 512;
+constexpr int RJ32_TABLE_BYTES = 96 * 1024;
+constexpr unsigned RJ32_SLOTS = RJ32_TABLE_BYTES / 8;
+constexpr unsigned RJ32_RCAP = RJ32_SLOTS / 2;
+constexpr int RJ32_U = 8;  // probe words in flight per thread
+constexpr unsigned long long kEmptyWord = ~0ULL;
+
+// Slot of a key offset: the MurmurHash3 32-bit finaliser, then
+// multiply-high into the table.
+__device__ __forceinline__ unsigned rj32_slot(unsigned off)
+{
+    off ^= off >> 16;
+    off *= 0x85ebca6bu;
+    off ^= off >> 13;
+    off *= 0xc2b2ae35u;
+    off ^= off >> 16;
+    return __umulhi(off, RJ32_SLOTS);
+}
+
+__global__ void __launch_bounds__(RJ32_THREADS, 2) rj_join32_kernel(RJJoinArgs a)
+{
+    extern __shared__ __align__(16) unsigned long long rj32_table[];
+    __shared__ long long item_cur, item_next;
+    const unsigned long long* Rw = reinterpret_cast<const unsigned long long*>(a.R);
+    const unsigned long long* Sw = reinterpret_cast<const unsigned long long*>(a.S);
+    uint64_t cnt = 0, bsum = 0, psum = 0;  // matches, build and probe payload offsets
+    bool dup = false;
+    if (threadIdx.x == 0) item_next = (long long)atomicAdd(a.next, 1u);
+    for (;;) {
+        __syncthreads();  // previous item done with the table and item slots
+        if (threadIdx.x == 0) {
+            item_cur = item_next;
+            if (item_cur < a.nitems) {
+                item_next = (long long)atomicAdd(a.next, 1u);
+                if (item_next < a.nitems) {
+                    const RJItem nx = a.items[item_next];
+                    rj_prefetch_l2(Rw + nx.r0, (unsigned long long)nx.rn * 8);
+                    rj_prefetch_l2(Sw + nx.s0, (unsigned long long)min(nx.sn, 8192u) * 8);
+                }
+            }
+        }
+        ulonglong2* T2 = reinterpret_cast<ulonglong2*>(rj32_table);
+        for (unsigned i = threadIdx.x; i < RJ32_SLOTS / 2; i += RJ32_THREADS)
+            T2[i] = make_ulonglong2(kEmptyWord, kEmptyWord);
+        __syncthreads();
+        const long long it = item_cur;
+        if (it >= a.nitems) break;
+        const RJItem item = a.items[it];
+        // Build: one 64-bit CAS per word; a chunk fills at most half the
+        // table, so a free slot always exists.
+        for (unsigned i = threadIdx.x; i < item.rn; i += RJ32_THREADS) {
+            const unsigned long long w = Rw[item.r0 + i];
+            const unsigned off = (unsigned)w;
+            unsigned pos = rj32_slot(off);
+            for (unsigned steps = 0; steps < RJ32_SLOTS; ++steps) {
+                const unsigned long long prev = atomicCAS(&rj32_table[pos], kEmptyWord, w);
+                if (prev == kEmptyWord) break;
+                if ((unsigned)prev == off) {  // a repeated build key: the counted join takes over
+                    dup = true;
+                    break;
+                }
+                pos = pos + 1 == RJ32_SLOTS ? 0 : pos + 1;
+            }
+        }
+        __syncthreads();
+        auto probe = [&](const unsigned long long w) {
+            const unsigned off = (unsigned)w;
+            unsigned pos = rj32_slot(off);
+            for (unsigned steps = 0; steps < RJ32_SLOTS; ++steps) {
+                const unsigned long long e = rj32_table[pos];
+                if ((unsigned)e == off) {
+                    cnt += 1;
+                    bsum += e >> 32;
+                    psum += w >> 32;
+                    return;
+                }
+                if (e == kEmptyWord) return;
+                pos = pos + 1 == RJ32_SLOTS ? 0 : pos + 1;
+            }
+        };
+        const unsigned long long* S = Sw + item.s0;
+        const unsigned sn = item.sn;
+        unsigned i = threadIdx.x;
+        for (; i + (RJ32_U - 1) * RJ32_THREADS < sn; i += RJ32_U * RJ32_THREADS) {
+            unsigned long long w[RJ32_U];
+#pragma unroll
+            for (int u = 0; u < RJ32_U; ++u) w[u] = __ldcs(&S[i + u * RJ32_THREADS]);
+#pragma unroll
+            for (int u = 0; u < RJ32_U; ++u) probe(w[u]);
+        }
+        for (; i < sn; i += RJ32_THREADS) probe(__ldcs(&S[i]));
+    }
+    uint64_t b = cnt * a.rp + bsum, p = cnt * a.sp + psum;
+    cnt = warp_sum_u64(cnt);
+    b = warp_sum_u64(b);
+    p = warp_sum_u64(p);
+    if ((threadIdx.x & 31) == 0 && (cnt | b | p)) {
+        atomicAdd(&a.acc[0], (unsigned long long)cnt);
+        atomicAdd(&a.acc[1], (unsigned long long)b);
+        atomicAdd(&a.acc[2], (unsigned long long)p);
+    }
+    if (__any_sync(0xffffffffu, dup) && (threadIdx.x & 31) == 0) atomicOr(a.dup, 1u);
+}
+
+// ---------------------------------------------------------------------------
 // Host driver.
 
 namespace {
@@ -369,7 +484,7 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
             side[s].mid = tm.on ? tm.ev[6 + 2 * s] : nullptr;
             side[s].done = tm.on ? tm.ev[2 + s] : nullptr;
         }
-        rc = rp_partition_sides(ctx, side, 2, FB, two, flags, hflags, tm.on ? tm.ev[1] : nullptr);
+        rc = rp_partition_sides(ctx, side, 2, FB, two, flags, hflags, tm.on ? tm.ev[1] : nullptr, true);
         R1 = side[0].P1;
         R2 = side[0].P2;
         S1 = side[1].P1;
@@ -386,17 +501,27 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
         std::vector<unsigned long long> rstart(LR.fstart.begin(), LR.fstart.begin() + F);
         std::vector<unsigned long long> sstart(LS.fstart.begin(), LS.fstart.begin() + F);
         std::vector<RJItem> items;
+        // Both relations packed in one key frame: the 32-bit-offset join
+        // (distinct build keys; a repeated key falls back to the counted
+        // join below, which decodes the words).
+        const bool same_frame = LR.packed && LS.packed && LR.kbase == LS.kbase;
         for (int pass = 0; pass < 2; ++pass) {
             const bool unique = pass == 0;
-            make_items(LR.count, LS.count, rstart, sstart, unique ? RJ_RCAP_UNIQUE : RJ_RCAP_COUNTED, items);
+            const bool j32 = unique && same_frame;
+            make_items(LR.count, LS.count, rstart, sstart,
+                       j32 ? RJ32_RCAP : (unique ? RJ_RCAP_UNIQUE : RJ_RCAP_COUNTED), items);
             if (items.empty()) break;
             dfree(ctx, ditems);
             ditems = nullptr;
             if ((rc = dalloc(ctx, (void**)&ditems, items.size() * sizeof(RJItem)))) break;
             PYG_CUDA(cudaMemcpyAsync(ditems, items.data(), items.size() * sizeof(RJItem), cudaMemcpyHostToDevice,
                                      ctx->stream));
-            void* fn = unique ? join_fn<true>(LR.packed, LS.packed) : join_fn<false>(LR.packed, LS.packed);
-            PYG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, RJ_TABLE_BYTES));
+            void* fn = j32 ? (void*)rj_join32_kernel
+                           : (unique ? join_fn<true>(LR.packed, LS.packed) : join_fn<false>(LR.packed, LS.packed));
+            const int smem = j32 ? RJ32_TABLE_BYTES : RJ_TABLE_BYTES;
+            const int threads = j32 ? RJ32_THREADS : RJ_JOIN_THREADS;
+            const int per_sm = j32 ? 2 : RJ_JOIN_BLOCKS;
+            PYG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
             PYG_CUDA(cudaMemsetAsync(acc, 0, 3 * 8, ctx->stream));
             PYG_CUDA(cudaMemsetAsync(next, 0, 16, ctx->stream));
             RJJoinArgs ja;
@@ -412,9 +537,9 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
             ja.rp = LR.pbase;
             ja.sk = LS.kbase;
             ja.sp = LS.pbase;
-            const unsigned grid = (unsigned)std::min<long long>((long long)ctx->sm_count * RJ_JOIN_BLOCKS, ja.nitems);
+            const unsigned grid = (unsigned)std::min<long long>((long long)ctx->sm_count * per_sm, ja.nitems);
             void* args[] = {&ja};
-            PYG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(RJ_JOIN_THREADS), args, RJ_TABLE_BYTES, ctx->stream));
+            PYG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, smem, ctx->stream));
             PYG_LAUNCHED(ctx);
             PYG_CUDA(cudaMemcpyAsync(h, acc, 3 * 8, cudaMemcpyDeviceToHost, ctx->stream));
             PYG_CUDA(cudaMemcpyAsync(h + 3, next, 16, cudaMemcpyDeviceToHost, ctx->stream));

@@ -551,25 +551,41 @@ void layout_sampled(const std::vector<unsigned long long>& sc, long long step, i
     L.p2 = L.fstart[F];
 }
 
-bool pack_frame(long long kmin, long long kmax, long long pmin, long long pmax, bool exact, RJLayout& L)
+// A window [base, base + 2^32 - 1) centred on [lo, hi] (offset 2^32 - 1 is
+// never used, so a join can take it as its empty-slot marker); a sampled
+// range must leave at least 2^30 of margin on each side.
+static bool frame_fit(long long lo, long long hi, bool exact, unsigned long long& base)
 {
-    // A window [base, base + 2^32) centred on [lo, hi]; a sampled range
-    // must leave at least 2^30 of margin on each side.
-    auto fit = [&](long long lo, long long hi, unsigned long long& base) {
-        if (hi < lo) {  // nothing was read
-            base = 0;
-            return true;
-        }
-        const unsigned long long span = (unsigned long long)hi - (unsigned long long)lo;
-        if (span > (exact ? 0xFFFFFFFFULL : (1ULL << 31))) return false;
-        base = (unsigned long long)lo - (0xFFFFFFFFULL - span) / 2;
+    if (hi < lo) {  // nothing was read
+        base = 0;
         return true;
-    };
+    }
+    const unsigned long long span = (unsigned long long)hi - (unsigned long long)lo;
+    if (span > (exact ? 0xFFFFFFFEULL : (1ULL << 31))) return false;
+    base = (unsigned long long)lo - (0xFFFFFFFEULL - span) / 2;
+    return true;
+}
+
+bool pack_frame(long long kmin, long long kmax, long long pmin, long long pmax, bool exact, RJLayout& L,
+                const unsigned long long* key_base)
+{
     unsigned long long kb = 0, pb = 0;
-    if (!fit(kmin, kmax, kb) || !fit(pmin, pmax, pb)) return false;
+    if (key_base) {
+        kb = *key_base;  // a frame shared with another relation, fitted to both ranges
+    } else if (!frame_fit(kmin, kmax, exact, kb)) {
+        return false;
+    }
+    if (!frame_fit(pmin, pmax, exact, pb)) return false;
     L.kbase = kb;
     L.pbase = pb;
     return true;
+}
+
+bool common_key_frame(const long long* mm0, bool exact0, const long long* mm1, bool exact1, unsigned long long* base)
+{
+    if (mm0[1] < mm0[0] || mm1[1] < mm1[0]) return false;
+    const long long lo = std::min(mm0[0], mm1[0]), hi = std::max(mm0[1], mm1[1]);
+    return frame_fit(lo, hi, exact0 && exact1, *base);
 }
 
 int upload_layout(pyg_ctx* ctx, const RJLayout& L, const RJSideDev& d, int F, int C, int64_t n)
@@ -708,7 +724,7 @@ int hist_launch_range(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step
 }
 
 int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsigned* flags, unsigned* hflags,
-                       cudaEvent_t hist_done)
+                       cudaEvent_t hist_done, bool share_key_frame)
 {
     // Coarse bits of the first of two passes.  Unpacked layouts split FB
     // evenly (2048-tuple tiles); packed layouts keep the second pass at 2^8
@@ -745,10 +761,11 @@ int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsig
     };
     // Layout of relation s from host counts h (F counts, then the key and
     // payload ranges): packed when the caller allows it and a frame fits.
-    auto form = [&](int s, const unsigned long long* h, int64_t st, bool exact) {
+    auto form = [&](int s, const unsigned long long* h, int64_t st, bool exact, const unsigned long long* kb) {
         RJLayout& L = sd[s].L;
         const long long* mm = (const long long*)(h + F);
-        const bool pack = sd[s].allow_pack && !sd[s].csplit && pack_frame(mm[0], mm[1], mm[2], mm[3], exact, L);
+        const bool pack =
+            sd[s].allow_pack && !sd[s].csplit && pack_frame(mm[0], mm[1], mm[2], mm[3], exact, L, kb);
         CBs[s] = coarse_bits(pack);
         const int C = 1 << CBs[s], sub = FB - CBs[s];
         std::vector<unsigned long long> hv(h, h + F);
@@ -787,10 +804,17 @@ int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsig
         for (int s = 0; s < ns; ++s)
             PYG_CUDA(cudaMemcpyAsync(hh_at(s), hist_at(s), (size_t)(F + 4) * 8, cudaMemcpyDeviceToHost, ctx->stream));
         PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        // One key frame for both relations when asked and both ranges fit
+        // in it, so that their packed words compare by key offset.
+        unsigned long long ckb = 0;
+        const bool common = share_key_frame && ns == 2 && sd[0].allow_pack && sd[1].allow_pack && !sd[0].csplit &&
+                            !sd[1].csplit &&
+                            common_key_frame((const long long*)(hh_at(0) + F), !sample[0],
+                                             (const long long*)(hh_at(1) + F), !sample[1], &ckb);
         // The second relation's layout is formed while the first one's
         // passes run.
         for (int s = 0; s < ns && !rc; ++s) {
-            form(s, hh_at(s), step[s], !sample[s]);
+            form(s, hh_at(s), step[s], !sample[s], common ? &ckb : nullptr);
             rc = launch(s);
         }
         if (rc) break;
@@ -816,7 +840,7 @@ int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsig
             if ((rc = hist_of(s, 1))) break;
             PYG_CUDA(cudaMemcpyAsync(hh_at(s), hist_at(s), (size_t)(F + 4) * 8, cudaMemcpyDeviceToHost, ctx->stream));
             PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-            form(s, hh_at(s), 1, true);
+            form(s, hh_at(s), 1, true, nullptr);
             PYG_CUDA(cudaMemsetAsync(flags + 4 * s, 0, 16, ctx->stream));
             if ((rc = launch(s))) break;
             PYG_CUDA(cudaMemcpyAsync(hflags + 4 * s, flags + 4 * s, 16, cudaMemcpyDeviceToHost, ctx->stream));

@@ -85,8 +85,14 @@ void layout_sampled(const std::vector<unsigned long long>& sc, long long step, i
 // Frame of a packed layout from the key and payload ranges seen by the
 // histogram ([kmin, kmax], [pmin, pmax], signed).  exact: the ranges cover
 // every tuple; else they come from a sample and must leave a margin of at
-// least 2^30 on each side.  Returns false when no frame fits.
-bool pack_frame(long long kmin, long long kmax, long long pmin, long long pmax, bool exact, RJLayout& L);
+// least 2^30 on each side.  Offsets stay below 2^32 - 1.  key_base (when
+// given) is a key frame shared with another relation (common_key_frame).
+// Returns false when no frame fits.
+bool pack_frame(long long kmin, long long kmax, long long pmin, long long pmax, bool exact, RJLayout& L,
+                const unsigned long long* key_base = nullptr);
+// One key frame covering two relations' key ranges mm = {kmin, kmax, ...},
+// so that their packed words carry comparable 32-bit key offsets.
+bool common_key_frame(const long long* mm0, bool exact0, const long long* mm1, bool exact1, unsigned long long* base);
 // Bytes of one intermediate element of a layout.
 inline int elem_bytes(const RJLayout& L) { return L.packed ? 8 : 16; }
 
@@ -165,8 +171,10 @@ struct RPSide {
 // flags: 4 device words per relation (bulk copy never landed, region
 // overflow, frame miss, unused); hflags: as many pinned host words.
 // hist_done (optional) is recorded after the histograms.
+// share_key_frame: pack both relations with one key frame when their key
+// ranges fit one (a redone relation gets its own frame).
 int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsigned* flags, unsigned* hflags,
-                       cudaEvent_t hist_done);
+                       cudaEvent_t hist_done, bool share_key_frame = false);
 
 // Partitions one relation into 2^FB partitions (hash bits, or ranges when
 // csplit is set; two passes when `two`): histogram (sampled when allowed

@@ -152,6 +152,7 @@ SIGNATURES = [
     ("pyg_sort", C.c_int, [_P, C.POINTER(pyg_rel), _I32, _P]),
     ("pyg_lower_bound", C.c_int, [_P, C.POINTER(pyg_rel), _I32, _P, _I64, _P]),
     ("pyg_sortlimit", C.c_int, [_P, C.POINTER(pyg_rel), _PI32, _I32, _I32, _I64, _P, _I64, _PI64]),
+    ("pyg_bitonic_sort", C.c_int, [_P, _P, _I64]),
     ("pyg_mpsm_join_agg", C.c_int, [_P, C.POINTER(pyg_rel), _I32, C.POINTER(pyg_rel), _I32, C.POINTER(pyg_proj), _I32,
                                     C.POINTER(pyg_mpsm_opts), C.POINTER(pyg_join_result), C.POINTER(pyg_mpsm_stats)]),
     ("pyg_mpsm_join_materialize", C.c_int, [_P, C.POINTER(pyg_rel), _I32, C.POINTER(pyg_rel), _I32,

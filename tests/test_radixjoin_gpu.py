@@ -200,6 +200,22 @@ def test_radix_packed_intermediates(ctx, torch_cuda, bits, case):
     assert st.probe_packed == (case != "build_only")
 
 
+@pytest.mark.parametrize("bits", [6, 12])
+def test_radix_shared_frame_with_repeated_build_keys(ctx, torch_cuda, bits):
+    """Both relations packed in one key frame take the 32-bit-offset join;
+    a repeated build key there hands the join to the counted kernel, which
+    decodes the packed words.  Same result as the oracle."""
+    rng = np.random.default_rng(50 + bits)
+    n, m = 1 << 17, 1 << 21
+    k = rng.integers(1000, 1000 + (1 << 15), n)  # about 4 copies per key
+    R = struct([k, rng.integers(0, 1 << 30, n)], [I64, I64])
+    S = struct([rng.integers(900, 1100 + (1 << 15), m), rng.integers(0, 1 << 30, m)], [I64, I64])
+    want = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ, buckets=n)
+    got, st = ctx.hashjoin_agg(dev_rel(torch_cuda, R, [I64, I64]), [0], dev_rel(torch_cuda, S, [I64, I64]), [0], PROJ,
+                               pyg.JOIN_RADIX, bits, stats=True)
+    assert got == want and st.build_packed == 1 and st.probe_packed == 1
+
+
 def test_radix_packed_frame_missed_redoes(ctx, torch_cuda):
     """A probe side of 2^25 tuples is laid out from a strided sample, which
     also gives the frame of its packed words.  One payload that no sampled
