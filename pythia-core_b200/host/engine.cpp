@@ -127,33 +127,79 @@ void Operator::init(const Setting& root, const Setting& node)
     if (buffsize < 1) throw EngineError("buffsize must be positive");
 }
 
-Operator::GetNextResultT MaterializedOp::getNext(unsigned short tid)
+pyg_rel input_rel(Operator* op, unsigned short tid, HostRel& host)
 {
-    int64_t per = buffsize / (schema.tuple_bytes ? schema.tuple_bytes : 1);
-    if (per < 1) per = 1;
-    int64_t left = result.ntuples - served;
-    int64_t n = left < per ? left : per;
-    page.data = result.data ? result.data + served * schema.tuple_bytes : nullptr;
-    page.ntuples = n;
-    page.tuple_bytes = schema.tuple_bytes;
-    served += n;
-    return std::make_pair(served >= result.ntuples ? Finished : Ready, &page);
+    const void* d = nullptr;
+    int64_t n = 0;
+    if (op->device_result(&d, &n)) return op->getOutSchema().rel(d, n, true);
+    drain(op, tid, host);
+    return op->getOutSchema().rel(host.data, host.ntuples, false);
 }
+
+int64_t ResultBuffer::d2h_bytes = 0;
+
+ResultBuffer::~ResultBuffer()
+{
+    if (dev && Operator::ctx) pyg_free(Operator::ctx, dev);
+}
+
+void ResultBuffer::keep_device(void* d, int64_t cnt, int32_t tuple_bytes)
+{
+    if (dev) pyg_free(Operator::ctx, dev);
+    dev = d;
+    n = cnt;
+    host.tuple_bytes = tuple_bytes;
+    host.ntuples = 0;
+    host_valid = false;
+    served = 0;
+}
+
+void ResultBuffer::keep_host()
+{
+    if (dev) pyg_free(Operator::ctx, dev);
+    dev = nullptr;
+    n = host.ntuples;
+    host_valid = true;
+    served = 0;
+}
+
+bool ResultBuffer::device(const void** d, int64_t* cnt) const
+{
+    if (!dev) return false;
+    *d = dev;
+    *cnt = n;
+    return true;
+}
+
+Operator::GetNextResultT ResultBuffer::next(int64_t buffsize, int32_t tuple_bytes)
+{
+    if (!host_valid) {
+        // First page pulled by a host consumer: one copy of the result.
+        host.tuple_bytes = tuple_bytes;
+        host.ntuples = 0;
+        host.reserve(n * tuple_bytes);
+        if (n) check(pyg_memcpy_d2h(Operator::ctx, host.data, dev, (size_t)n * tuple_bytes), "copy result");
+        host.ntuples = n;
+        d2h_bytes += n * tuple_bytes;
+        host_valid = true;
+    }
+    int64_t per = buffsize / (tuple_bytes ? tuple_bytes : 1);
+    if (per < 1) per = 1;
+    const int64_t left = host.ntuples - served;
+    const int64_t k = left < per ? left : per;
+    page.data = host.data ? host.data + served * tuple_bytes : nullptr;
+    page.ntuples = k;
+    page.tuple_bytes = tuple_bytes;
+    served += k;
+    return std::make_pair(served >= host.ntuples ? Operator::Finished : Operator::Ready, &page);
+}
+
+Operator::GetNextResultT MaterializedOp::getNext(unsigned short tid) { return out.next(buffsize, schema.tuple_bytes); }
 
 Operator::ResultCode MaterializedOp::scanStop(unsigned short tid)
 {
-    served = 0;
+    out.rewind();
     return Ready;
-}
-
-void MaterializedOp::serve_from_device(const void* dev, int64_t n)
-{
-    result.tuple_bytes = schema.tuple_bytes;
-    result.ntuples = 0;
-    result.reserve(n * schema.tuple_bytes);
-    if (n) check(pyg_memcpy_d2h(ctx, result.data, dev, (size_t)n * schema.tuple_bytes), "copy result");
-    result.ntuples = n;
-    served = 0;
 }
 
 // ------------------------------------------------------------------ scans
@@ -182,13 +228,14 @@ public:
     ResultCode scanStart(unsigned short tid) override
     {
         if (!loaded) load();
-        served = 0;
+        out.rewind();
         return Ready;
     }
 
 private:
     void load()
     {
+        HostRel& result = out.host;
         result.tuple_bytes = schema.tuple_bytes;
         for (auto& fn : files) {
             std::ifstream in(fn, std::ios::binary);
@@ -224,6 +271,7 @@ private:
                 }
             }
         }
+        out.keep_host();
         loaded = true;
     }
 
@@ -244,6 +292,7 @@ public:
     ResultCode scanStart(unsigned short tid) override { return nextOp->scanStart(tid); }
     GetNextResultT getNext(unsigned short tid) override { return nextOp->getNext(tid); }
     ResultCode scanStop(unsigned short tid) override { return nextOp->scanStop(tid); }
+    bool device_result(const void** dev, int64_t* n) override { return nextOp->device_result(dev, n); }
 };
 
 // `printer_tuplecount` (operators/printer_tuplecount.cpp): counts tuples.
@@ -262,6 +311,13 @@ public:
         return r;
     }
     ResultCode scanStop(unsigned short tid) override { return nextOp->scanStop(tid); }
+    // A GPU parent reading the child's device buffer passes every tuple.
+    bool device_result(const void** dev, int64_t* n) override
+    {
+        if (!nextOp->device_result(dev, n)) return false;
+        total += *n;
+        return true;
+    }
     int64_t total = 0;
 };
 
@@ -322,18 +378,16 @@ public:
     {
         if (buildOp->scanStart(tid) == Error || probeOp->scanStart(tid) == Error) return Error;
         HostRel R, S;
-        drain(buildOp, tid, R);
-        drain(probeOp, tid, S);
+        pyg_rel r = input_rel(buildOp, tid, R);
+        pyg_rel s = input_rel(probeOp, tid, S);
         buildOp->scanStop(tid);
-        pyg_rel r = buildOp->getOutSchema().rel(R.data, R.ntuples, false);
-        pyg_rel s = probeOp->getOutSchema().rel(S.data, S.ntuples, false);
         if (fuse) {
             pyg_join_opts o = {PYG_JOIN_AUTO, 0, load_factor, 0};
             check(pyg_hashjoin_agg(ctx, &r, bkeys.data(), &s, pkeys.data(), (int32_t)bkeys.size(), proj.data(),
                                    (int32_t)proj.size(), &o, &fused, nullptr),
                   "hashjoin (fused aggregate)");
-            result.ntuples = 0;
-            served = 0;
+            out.host.ntuples = 0;
+            out.keep_host();
             return Ready;
         }
         std::vector<int32_t> pay;
@@ -347,32 +401,22 @@ public:
         int rc = pyg_hashjoin_probe_materialize(ctx, ht, &s, pkeys.data(), proj.data(), (int32_t)proj.size(), nullptr,
                                                 0, &n);
         if (rc != PYG_OK && rc != PYG_ERR_CAPACITY) check(rc, "hashjoin probe");
-        void* out = nullptr;
-        check(pyg_alloc(ctx, (size_t)(n > 0 ? n : 1) * schema.tuple_bytes, &out), "hashjoin output");
-        rc = pyg_hashjoin_probe_materialize(ctx, ht, &s, pkeys.data(), proj.data(), (int32_t)proj.size(), out, n, &n);
+        void* dev = nullptr;
+        check(pyg_alloc(ctx, (size_t)(n > 0 ? n : 1) * schema.tuple_bytes, &dev), "hashjoin output");
+        rc = pyg_hashjoin_probe_materialize(ctx, ht, &s, pkeys.data(), proj.data(), (int32_t)proj.size(), dev, n, &n);
         pyg_hashtable_free(ctx, ht);
-        if (rc == PYG_OK) serve_from_device(out, n);
-        pyg_free(ctx, out);
+        if (rc != PYG_OK) pyg_free(ctx, dev);
         check(rc, "hashjoin probe");
+        out.keep_device(dev, n, schema.tuple_bytes);
         return Ready;
     }
 
-    GetNextResultT getNext(unsigned short tid) override
-    {
-        int64_t per = buffsize / schema.tuple_bytes;
-        if (per < 1) per = 1;
-        int64_t left = result.ntuples - served;
-        int64_t n = left < per ? left : per;
-        page.data = result.data ? result.data + served * schema.tuple_bytes : nullptr;
-        page.ntuples = n;
-        page.tuple_bytes = schema.tuple_bytes;
-        served += n;
-        return std::make_pair(served >= result.ntuples ? Finished : Ready, &page);
-    }
+    GetNextResultT getNext(unsigned short tid) override { return out.next(buffsize, schema.tuple_bytes); }
+    bool device_result(const void** dev, int64_t* n) override { return out.device(dev, n); }
 
     ResultCode scanStop(unsigned short tid) override
     {
-        served = 0;
+        out.rewind();
         return probeOp->scanStop(tid);
     }
 
@@ -380,19 +424,8 @@ public:
     std::vector<int32_t> bkeys, pkeys;
 
 private:
-    void serve_from_device(const void* dev, int64_t n)
-    {
-        result.tuple_bytes = schema.tuple_bytes;
-        result.ntuples = 0;
-        result.reserve(n * schema.tuple_bytes);
-        if (n) check(pyg_memcpy_d2h(ctx, result.data, dev, (size_t)n * schema.tuple_bytes), "copy result");
-        result.ntuples = n;
-        served = 0;
-    }
     float load_factor = 0.5f;
-    HostRel result;
-    int64_t served = 0;
-    Page page;
+    ResultBuffer out;
 };
 
 // ------------------------------------------------------------ aggregates
@@ -433,7 +466,7 @@ public:
 
     ResultCode scanStart(unsigned short tid) override
     {
-        served = 0;
+        out.rewind();
         // No GROUP BY straight over a hash join (possibly through
         // printer_tuplecount / merge): fuse the aggregate into the probe.
         if (keys.empty()) {
@@ -456,6 +489,7 @@ public:
                 nextOp->scanStop(tid);
                 for (auto* c : counters) c->total += hj->fused.count;
                 uint64_t v = is_sum ? (uint64_t)hj->fused.sums[sumfield] : (uint64_t)hj->fused.count;
+                HostRel& result = out.host;
                 result.tuple_bytes = schema.tuple_bytes;
                 result.ntuples = 0;
                 if (hj->fused.count > 0) {
@@ -468,23 +502,23 @@ public:
                     }
                     result.append(row, 1);
                 }
+                out.keep_host();
                 return Ready;
             }
         }
         if (nextOp->scanStart(tid) == Error) return Error;
         HostRel in;
-        drain(nextOp, tid, in);
-        nextOp->scanStop(tid);
-        pyg_rel r = nextOp->getOutSchema().rel(in.data, in.ntuples, false);
-        int64_t cap = in.ntuples > 0 ? in.ntuples : 1;
-        void* out = nullptr;
-        check(pyg_alloc(ctx, (size_t)cap * schema.tuple_bytes, &out), name.c_str());
+        pyg_rel r = input_rel(nextOp, tid, in);
+        int64_t cap = r.ntuples > 0 ? r.ntuples : 1;
+        void* dev = nullptr;
+        check(pyg_alloc(ctx, (size_t)cap * schema.tuple_bytes, &dev), name.c_str());
         int64_t g = 0;
         int rc = pyg_groupby(ctx, &r, keys.data(), (int32_t)keys.size(), is_sum ? PYG_AGG_SUM : PYG_AGG_COUNT,
-                             is_sum ? sumfield : 0, 1, expected, out, cap, &g);
-        if (rc == PYG_OK) serve_from_device(out, g);
-        pyg_free(ctx, out);
+                             is_sum ? sumfield : 0, 1, expected, dev, cap, &g);
+        nextOp->scanStop(tid);
+        if (rc != PYG_OK) pyg_free(ctx, dev);
         check(rc, name.c_str());
+        out.keep_device(dev, g, schema.tuple_bytes);
         return Ready;
     }
 
@@ -519,32 +553,32 @@ public:
     {
         if (nextOp->scanStart(tid) == Error) return Error;
         HostRel in;
-        drain(nextOp, tid, in);
-        nextOp->scanStop(tid);
-        pyg_rel r = schema.rel(in.data, in.ntuples, false);
-        void* out = nullptr;
-        check(pyg_alloc(ctx, (size_t)(in.ntuples > 0 ? in.ntuples : 1) * schema.tuple_bytes, &out), "partition");
+        pyg_rel r = input_rel(nextOp, tid, in);
+        const int64_t n_in = r.ntuples;
+        void* dev = nullptr;
+        check(pyg_alloc(ctx, (size_t)(n_in > 0 ? n_in : 1) * schema.tuple_bytes, &dev), "partition");
         pyg_splitter s = {PYG_SPLIT_EXACTRANGE, buckets, mn, mx, nullptr};
         offsets.assign(buckets + 1, 0);
-        int rc = pyg_partition(ctx, &r, attr, &s, out, offsets.data());
+        int rc = pyg_partition(ctx, &r, attr, &s, dev, offsets.data());
         if (rc == PYG_OK && sortout) {
             // Sort each partition on sortattr (PartitionOp with sort = yes).
             void* tmp = nullptr;
-            rc = pyg_alloc(ctx, (size_t)(in.ntuples > 0 ? in.ntuples : 1) * schema.tuple_bytes, &tmp);
+            rc = pyg_alloc(ctx, (size_t)(n_in > 0 ? n_in : 1) * schema.tuple_bytes, &tmp);
             for (int b = 0; rc == PYG_OK && b < buckets; ++b) {
                 int64_t n = offsets[b + 1] - offsets[b];
                 if (n < 2) continue;
-                pyg_rel pr = schema.rel((uint8_t*)out + offsets[b] * schema.tuple_bytes, n, true);
+                pyg_rel pr = schema.rel((uint8_t*)dev + offsets[b] * schema.tuple_bytes, n, true);
                 rc = pyg_sort(ctx, &pr, sortattr, (uint8_t*)tmp + offsets[b] * schema.tuple_bytes);
                 if (rc == PYG_OK)
-                    rc = pyg_memcpy_d2d(ctx, (uint8_t*)out + offsets[b] * schema.tuple_bytes,
+                    rc = pyg_memcpy_d2d(ctx, (uint8_t*)dev + offsets[b] * schema.tuple_bytes,
                                         (uint8_t*)tmp + offsets[b] * schema.tuple_bytes, (size_t)n * schema.tuple_bytes);
             }
             pyg_free(ctx, tmp);
         }
-        if (rc == PYG_OK) serve_from_device(out, in.ntuples);
-        pyg_free(ctx, out);
+        nextOp->scanStop(tid);
+        if (rc != PYG_OK) pyg_free(ctx, dev);
         check(rc, "partition");
+        out.keep_device(dev, n_in, schema.tuple_bytes);
         return Ready;
     }
     std::vector<int64_t> offsets;
@@ -570,15 +604,14 @@ public:
     {
         if (nextOp->scanStart(tid) == Error) return Error;
         HostRel in;
-        drain(nextOp, tid, in);
+        pyg_rel r = input_rel(nextOp, tid, in);
+        void* dev = nullptr;
+        check(pyg_alloc(ctx, (size_t)(r.ntuples > 0 ? r.ntuples : 1) * schema.tuple_bytes, &dev), "sort");
+        int rc = pyg_sort(ctx, &r, attr, dev);
         nextOp->scanStop(tid);
-        pyg_rel r = schema.rel(in.data, in.ntuples, false);
-        void* out = nullptr;
-        check(pyg_alloc(ctx, (size_t)(in.ntuples > 0 ? in.ntuples : 1) * schema.tuple_bytes, &out), "sort");
-        int rc = pyg_sort(ctx, &r, attr, out);
-        if (rc == PYG_OK) serve_from_device(out, in.ntuples);
-        pyg_free(ctx, out);
+        if (rc != PYG_OK) pyg_free(ctx, dev);
         check(rc, "sort");
+        out.keep_device(dev, r.ntuples, schema.tuple_bytes);
         return Ready;
     }
 
@@ -615,17 +648,16 @@ public:
     {
         if (nextOp->scanStart(tid) == Error) return Error;
         HostRel in;
-        drain(nextOp, tid, in);
-        nextOp->scanStop(tid);
-        pyg_rel r = schema.rel(in.data, in.ntuples, false);
-        const int64_t k = limit < in.ntuples ? limit : in.ntuples;
-        void* out = nullptr;
-        check(pyg_alloc(ctx, (size_t)(k > 0 ? k : 1) * schema.tuple_bytes, &out), "sortlimit");
+        pyg_rel r = input_rel(nextOp, tid, in);
+        const int64_t k = limit < r.ntuples ? limit : r.ntuples;
+        void* dev = nullptr;
+        check(pyg_alloc(ctx, (size_t)(k > 0 ? k : 1) * schema.tuple_bytes, &dev), "sortlimit");
         int64_t n = 0;
-        int rc = pyg_sortlimit(ctx, &r, keys.data(), (int32_t)keys.size(), asc ? 1 : 0, limit, out, k, &n);
-        if (rc == PYG_OK) serve_from_device(out, n);
-        pyg_free(ctx, out);
+        int rc = pyg_sortlimit(ctx, &r, keys.data(), (int32_t)keys.size(), asc ? 1 : 0, limit, dev, k, &n);
+        nextOp->scanStop(tid);
+        if (rc != PYG_OK) pyg_free(ctx, dev);
         check(rc, "sortlimit");
+        out.keep_device(dev, n, schema.tuple_bytes);
         return Ready;
     }
 
@@ -837,12 +869,8 @@ public:
     {
         if (buildOp->scanStart(tid) == Error || probeOp->scanStart(tid) == Error) return Error;
         HostRel R, S;
-        drain(buildOp, tid, R);
-        drain(probeOp, tid, S);
-        buildOp->scanStop(tid);
-        probeOp->scanStop(tid);
-        pyg_rel r = buildOp->getOutSchema().rel(R.data, R.ntuples, false);
-        pyg_rel s = probeOp->getOutSchema().rel(S.data, S.ntuples, false);
+        pyg_rel r = input_rel(buildOp, tid, R);
+        pyg_rel s = input_rel(probeOp, tid, S);
         if (mfbko > 0) {
             const int64_t most = max_key_multiplicity(ctx, r, bkey);
             if (most > mfbko)
@@ -853,36 +881,21 @@ public:
         int rc = pyg_mpsm_join_materialize(ctx, &r, bkey, &s, pkey, proj.data(), (int32_t)proj.size(), &opts, nullptr,
                                            0, &n);
         if (rc != PYG_OK && rc != PYG_ERR_CAPACITY) check(rc, "mpsm join");
-        void* out = nullptr;
-        check(pyg_alloc(ctx, (size_t)(n > 0 ? n : 1) * schema.tuple_bytes, &out), "mpsm output");
-        rc = pyg_mpsm_join_materialize(ctx, &r, bkey, &s, pkey, proj.data(), (int32_t)proj.size(), &opts, out, n, &n);
-        if (rc == PYG_OK) {
-            result.tuple_bytes = schema.tuple_bytes;
-            result.ntuples = 0;
-            result.reserve(n * schema.tuple_bytes);
-            if (n) rc = pyg_memcpy_d2h(ctx, result.data, out, (size_t)n * schema.tuple_bytes);
-            result.ntuples = n;
-        }
-        pyg_free(ctx, out);
+        void* dev = nullptr;
+        check(pyg_alloc(ctx, (size_t)(n > 0 ? n : 1) * schema.tuple_bytes, &dev), "mpsm output");
+        rc = pyg_mpsm_join_materialize(ctx, &r, bkey, &s, pkey, proj.data(), (int32_t)proj.size(), &opts, dev, n, &n);
+        buildOp->scanStop(tid);
+        probeOp->scanStop(tid);
+        if (rc != PYG_OK) pyg_free(ctx, dev);
         check(rc, "mpsm join");
-        served = 0;
+        out.keep_device(dev, n, schema.tuple_bytes);
         return Ready;
     }
-    GetNextResultT getNext(unsigned short tid) override
-    {
-        int64_t per = buffsize / schema.tuple_bytes;
-        if (per < 1) per = 1;
-        int64_t left = result.ntuples - served;
-        int64_t n = left < per ? left : per;
-        page.data = result.data ? result.data + served * schema.tuple_bytes : nullptr;
-        page.ntuples = n;
-        page.tuple_bytes = schema.tuple_bytes;
-        served += n;
-        return std::make_pair(served >= result.ntuples ? Finished : Ready, &page);
-    }
+    GetNextResultT getNext(unsigned short tid) override { return out.next(buffsize, schema.tuple_bytes); }
+    bool device_result(const void** dev, int64_t* n) override { return out.device(dev, n); }
     ResultCode scanStop(unsigned short tid) override
     {
-        served = 0;
+        out.rewind();
         return Ready;
     }
 
@@ -891,9 +904,7 @@ private:
     int32_t bkey = 0, pkey = 0;
     int64_t mfbko = 0;  // 0: no bound (sortmergejoin, mpsmjoin)
     pyg_mpsm_opts opts;
-    HostRel result;
-    int64_t served = 0;
-    Page page;
+    ResultBuffer out;
 };
 
 // ------------------------------------------------------------------ Query

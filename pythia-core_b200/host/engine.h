@@ -71,6 +71,11 @@ public:
     virtual ResultCode scanStop(unsigned short tid) = 0;
     virtual void threadClose(unsigned short tid) {}
     virtual std::vector<Operator*> children() { return {}; }
+    // After scanStart: the whole output as a device buffer of n tuples,
+    // when the operator produced it on the GPU.  A GPU parent reads it in
+    // place instead of pulling pages through host memory.  The buffer stays
+    // valid until the operator's next scanStart or its destruction.
+    virtual bool device_result(const void** dev, int64_t* n) { return false; }
     Schema& getOutSchema() { return schema; }
 
     std::string type, name;
@@ -81,17 +86,42 @@ protected:
     int64_t buffsize = 1 << 20;
 };
 
+// An operator's materialised output: either a device buffer, kept on the
+// device for GPU parents and copied to host only when pages are pulled, or
+// host pages filled directly.
+struct ResultBuffer {
+    HostRel host;
+    void* dev = nullptr;
+    int64_t n = 0;
+    bool host_valid = true;
+    int64_t served = 0;
+    Page page;
+    // Bytes copied device -> host to serve pages, over all operators of
+    // the process (the driver prints it).
+    static int64_t d2h_bytes;
+
+    ResultBuffer() = default;
+    ResultBuffer(const ResultBuffer&) = delete;
+    ResultBuffer& operator=(const ResultBuffer&) = delete;
+    ~ResultBuffer();
+    // Takes ownership of device buffer d (pyg_alloc) holding cnt tuples.
+    void keep_device(void* d, int64_t cnt, int32_t tuple_bytes);
+    // The host relation was filled directly.
+    void keep_host();
+    Operator::GetNextResultT next(int64_t buffsize, int32_t tuple_bytes);
+    bool device(const void** d, int64_t* cnt) const;
+    void rewind() { served = 0; }
+};
+
 // Serves a materialised relation as pages of buffsize bytes.
 class MaterializedOp : public Operator {
 public:
     GetNextResultT getNext(unsigned short tid) override;
     ResultCode scanStop(unsigned short tid) override;
+    bool device_result(const void** dev, int64_t* n) override { return out.device(dev, n); }
 
 protected:
-    void serve_from_device(const void* dev, int64_t n);  // copies to host
-    HostRel result;
-    int64_t served = 0;
-    Page page;
+    ResultBuffer out;
 };
 
 class SingleInputOp : public Operator {
@@ -109,6 +139,9 @@ public:
 
 // Reads a whole child into a pinned host relation.
 void drain(Operator* op, unsigned short tid, HostRel& out);
+// A child's output as a relation: its device buffer when it has one (no
+// host round trip), else its pages drained into `host`.
+pyg_rel input_rel(Operator* op, unsigned short tid, HostRel& host);
 
 // Builds the operator tree of a plan (reference Query::create, query.cpp:56-326).
 struct Query {

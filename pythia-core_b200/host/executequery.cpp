@@ -60,6 +60,7 @@ int main(int argc, char** argv)
         std::cout << "ResponseTimeInSec: " << sec << std::endl;
         for (auto& line : q.counter_report()) std::cout << line << std::endl;
         std::cout << "GpuKernelLaunches: " << pyg_ctx_kernel_launches(Operator::ctx) << std::endl;
+        std::cout << "DeviceToHostResultBytes: " << ResultBuffer::d2h_bytes << std::endl;
         q.threadClose();
         pyg_ctx_destroy(Operator::ctx);
     } catch (const std::exception& e) {

@@ -84,6 +84,25 @@ def test_mpsm_plan(golden):
     assert canon_rows(as_struct(out, g["out"].dtype)) == canon_rows(g["out"])
 
 
+def test_operator_results_stay_on_the_device(golden):
+    """partition -> mpsmjoin -> merge: the partition's output is read by
+    the join in device memory; the only device-to-host copy of results is
+    the join's rows pulled by the driver (DeviceToHostResultBytes)."""
+    import subprocess
+    g = golden("mpsm_pkfk")
+    proj = [tuple(int(v) for v in p) for p in g["proj"]]
+    n = g["R"].shape[0]
+    with tempfile.TemporaryDirectory() as d:
+        rf = refrun.write_rel(d, "R", g["R"], T)
+        sf = refrun.write_rel(d, "S", g["S"], T)
+        with open(os.path.join(d, "plan.conf"), "w") as f:
+            f.write(refrun.plan_mpsm(T, rf, [2, 2], sf, [2, 2], proj, 0, n - 1, 2 * n, 2 * g["S"].shape[0]))
+        r = subprocess.run([EXE, "plan.conf"], cwd=d, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    line = [x for x in r.stdout.splitlines() if x.startswith("DeviceToHostResultBytes:")]
+    assert line and int(line[0].split(":")[1]) == g["out"].shape[0] * g["out"].dtype.itemsize
+
+
 def test_partition_plan_orders_partitions(golden):
     g = golden("partition_exactrange")
     A = g["A"]
