@@ -385,6 +385,27 @@ class Ctx:
         res = (out.count, [out.sums[i] for i in range(len(proj))])
         return (res, st) if stats else res
 
+    def hashjoin_agg_prepared(self, R, rkeys, S, skeys, proj, algorithm=JOIN_AUTO, radix_bits=0, load_factor=0.5):
+        """The same call with its ctypes arguments built once: returns a
+        function that runs the join and returns (count, [sums]) (for timing
+        loops where Python argument marshalling would dominate)."""
+        rk = (C.c_int32 * len(rkeys))(*rkeys)
+        sk = (C.c_int32 * len(skeys))(*skeys)
+        pj = (pyg_proj * max(1, len(proj)))(*[pyg_proj(s, c) for s, c in proj])
+        o = pyg_join_opts(algorithm, radix_bits, load_factor, 0)
+        out = pyg_join_result()
+        r, s = R.c(), S.c()
+        f = lib().pyg_hashjoin_agg
+        args = (self.h, C.byref(r), rk, C.byref(s), sk, len(rkeys), pj, len(proj), C.byref(o), C.byref(out), None)
+        keep = (R, S)
+
+        def call():
+            check(f(*args))
+            assert keep
+            return out.count, [out.sums[i] for i in range(len(proj))]
+
+        return call
+
     # -- group-by -----------------------------------------------------
     def groupby(self, rel, key_cols, flags, sum_col, sort_by_key, expected_groups, out, capacity):
         k = (C.c_int32 * max(1, len(key_cols)))(*key_cols)
