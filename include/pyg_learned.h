@@ -3,10 +3,15 @@
  *
  * A two-level piecewise-linear model of a key sample's CDF: a root linear
  * model picks one of `leaves` linear leaves, each fitted to the keys routed
- * to it.  It is trained on the GPU by the library's own forward / backward
- * kernels (projected Adam on the squared CDF error) and used to pick range
- * partition splitters (the MPSM join) and to size hash tables for skewed
- * keys.  It only moves partition boundaries: results stay exact.
+ * to it.  Keys that fill at least 1/4096 of the sample (heavy keys) are
+ * exact point masses of the model; the root and leaves fit the rest, so
+ *   F(k) = (1 - W) C(k) + (mass of the heavy keys below k),
+ * with W the heavy keys' share of the sample.  It is trained on the GPU by
+ * the library's own kernels (least-squares start, then projected Adam on
+ * the squared CDF error through the forward / backward kernels) and used
+ * to pick range partition splitters (the MPSM join) and to size hash
+ * tables (its distinct-key estimate, for group-by without a group count).
+ * It only moves partition boundaries: results stay exact.
  *
  * No reference counterpart: it replaces the equal-width range split of
  * ExactRangeValueHasher (hash.h:452-487, used by PartitionOp,

@@ -35,9 +35,16 @@ struct pyg_cdf {
     double* d_yr = nullptr;         // device: (ylo, yhi) per leaf
     int64_t n_sample = 0, distinct = 0, f1 = 0;
     // Heavy keys: sample runs of at least n/4096 equal keys, kept as exact
-    // point masses [lo, hi) of the sample CDF next to the linear leaves.
+    // point masses beside the linear leaves, which are fitted to the rest
+    // of the sample (the continuous part C).  The model's CDF is
+    //   F(k) = (1 - W) C(k) + sum of w_h over heavy keys h < k,
+    // with w_h the share of the sample holding key h and W their total.
     std::vector<int64_t> heavy_key;
-    std::vector<double> heavy_lo, heavy_hi;
+    std::vector<double> heavy_w, heavy_before;  // mass, mass of the heavy keys below it
+    double wheavy = 0;
+    int64_t* d_hkeys = nullptr;    // device copies for predict
+    double* d_hbefore = nullptr;
+    double* d_hw = nullptr;
 };
 
 namespace pyg {
@@ -293,13 +300,17 @@ __global__ void root_to_raw_kernel(const double* __restrict__ acc, double* __res
     raw[1] = acc[2];
 }
 
+// F(k) = (1 - W) C(k) + (mass of the heavy keys below k): C from the root
+// and leaf of k, the heavy part by binary search over the nh heavy keys.
 __global__ void predict_kernel(const int64_t* __restrict__ keys, int64_t n, double lo, double scale,
                                const float* __restrict__ params, const double* __restrict__ yr, int L,
-                               float* __restrict__ out)
+                               const int64_t* __restrict__ hkeys, const double* __restrict__ hbefore,
+                               const double* __restrict__ hw, int nh, double W, float* __restrict__ out)
 {
     const double a0 = params[0], b0 = params[1];
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double x = norm_key(keys[i], lo, scale);
+        const int64_t k = keys[i];
+        double x = norm_key(k, lo, scale);
         double r = a0 * x + b0;
         double fl = floor(L * r);
         int l = fl < 0 ? 0 : (fl > L - 1 ? L - 1 : (int)fl);
@@ -307,7 +318,34 @@ __global__ void predict_kernel(const int64_t* __restrict__ keys, int64_t n, doub
         uu = uu < 0 ? 0 : (uu > 1 ? 1 : uu);
         double f = (double)params[2 + 2 * l] * uu + (double)params[3 + 2 * l];
         f = f < 0 ? 0 : (f > 1 ? 1 : f);
-        out[i] = (float)(yr[2 * l] + (yr[2 * l + 1] - yr[2 * l]) * f);
+        const double c = yr[2 * l] + (yr[2 * l + 1] - yr[2 * l]) * f;
+        int a = 0, b = nh;  // heavy keys < k: the first index with hkeys >= k
+        while (a < b) {
+            const int mid = (a + b) >> 1;
+            if (hkeys[mid] < k) a = mid + 1;
+            else b = mid;
+        }
+        const double below = a > 0 ? hbefore[a - 1] + hw[a - 1] : 0.0;
+        out[i] = (float)((1.0 - W) * c + below);
+    }
+}
+
+// Copies the sorted sample without its heavy runs [starts[r], ends[r]),
+// r < nr, ascending: out[i - cum[j]] = k[i] for i outside every run, where
+// j counts the runs starting at or before i and cum[j] is their length.
+__global__ void drop_runs_kernel(const int64_t* __restrict__ k, int64_t n, const long long* __restrict__ starts,
+                                 const long long* __restrict__ ends, const long long* __restrict__ cum, int nr,
+                                 int64_t* __restrict__ out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int a = 0, b = nr;
+        while (a < b) {
+            const int mid = (a + b) >> 1;
+            if (starts[mid] <= i) a = mid + 1;
+            else b = mid;
+        }
+        if (a > 0 && i < ends[a - 1]) continue;
+        out[i - cum[a]] = k[i];
     }
 }
 
@@ -501,6 +539,10 @@ int pyg_cdf_train(pyg_ctx* ctx, const int64_t* sample_keys, int64_t n, const pyg
     float* adam = nullptr;  // m and v for 2 + 2L params
     int64_t ends[2];
     unsigned long long* hs = (unsigned long long*)ctx->pinned + 128;
+    std::vector<long long> run_start, run_end;  // heavy runs in the sorted sample
+    int64_t* cont = nullptr;                    // the sample without its heavy runs
+    const int64_t* fit = sorted;                // what the root and leaves are fitted to
+    int64_t nfit = n;
     do {
         if ((rc = w.alloc(ctx, n, L))) break;
         if ((rc = dalloc(ctx, (void**)&m->d_params, (size_t)(2 + 2 * L) * 4))) break;
@@ -544,11 +586,56 @@ int pyg_cdf_train(pyg_ctx* ctx, const int64_t* sample_keys, int64_t n, const pyg
             std::vector<int> ord(nh);
             for (int i = 0; i < nh; ++i) ord[i] = i;
             std::sort(ord.begin(), ord.end(), [&](int a, int b) { return hr[a].x < hr[b].x; });
+            double before = 0;
             for (int i : ord) {
+                const double w = (double)(he[i] - hr[i].y) / (double)n;
                 m->heavy_key.push_back(hr[i].x);
-                m->heavy_lo.push_back((double)hr[i].y / (double)n);
-                m->heavy_hi.push_back((double)he[i] / (double)n);
+                m->heavy_w.push_back(w);
+                m->heavy_before.push_back(before);
+                run_start.push_back(hr[i].y);
+                run_end.push_back(he[i]);
+                before += w;
             }
+            m->wheavy = before;
+        }
+        // The leaves are fitted to the sample without its heavy runs (they
+        // are point masses of the model); the runs are ordered by key, so
+        // also by position in the sorted sample.
+        const int nh = (int)run_start.size();
+        int64_t heavy_n = 0;
+        for (int i = 0; i < nh; ++i) heavy_n += run_end[i] - run_start[i];
+        if (nh > 0 && n - heavy_n >= 2) {
+            std::vector<long long> cum(nh + 1, 0);
+            for (int i = 0; i < nh; ++i) cum[i + 1] = cum[i] + (run_end[i] - run_start[i]);
+            long long* runs = nullptr;
+            if ((rc = dalloc(ctx, (void**)&runs, (size_t)(3 * nh + 1) * 8))) break;
+            if ((rc = dalloc(ctx, (void**)&cont, (size_t)(n - heavy_n) * 8))) {
+                dfree(ctx, runs);
+                break;
+            }
+            PYG_CUDA(cudaMemcpyAsync(runs, run_start.data(), (size_t)nh * 8, cudaMemcpyHostToDevice, ctx->stream));
+            PYG_CUDA(cudaMemcpyAsync(runs + nh, run_end.data(), (size_t)nh * 8, cudaMemcpyHostToDevice, ctx->stream));
+            PYG_CUDA(cudaMemcpyAsync(runs + 2 * nh, cum.data(), (size_t)(nh + 1) * 8, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+            drop_runs_kernel<<<grid_for(ctx, n, 256, 4, 8), 256, 0, ctx->stream>>>(sorted, n, runs, runs + nh,
+                                                                                   runs + 2 * nh, nh, cont);
+            PYG_LAUNCHED(ctx);
+            PYG_CUDA(cudaStreamSynchronize(ctx->stream));  // keeps the host vectors alive until the copies ran
+            dfree(ctx, runs);
+            fit = cont;
+            nfit = n - heavy_n;
+        }
+        if (nh > 0) {
+            if ((rc = dalloc(ctx, (void**)&m->d_hkeys, (size_t)nh * 8)) ||
+                (rc = dalloc(ctx, (void**)&m->d_hbefore, (size_t)nh * 8)) ||
+                (rc = dalloc(ctx, (void**)&m->d_hw, (size_t)nh * 8)))
+                break;
+            PYG_CUDA(cudaMemcpyAsync(m->d_hkeys, m->heavy_key.data(), (size_t)nh * 8, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+            PYG_CUDA(cudaMemcpyAsync(m->d_hbefore, m->heavy_before.data(), (size_t)nh * 8, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+            PYG_CUDA(cudaMemcpyAsync(m->d_hw, m->heavy_w.data(), (size_t)nh * 8, cudaMemcpyHostToDevice,
+                                     ctx->stream));
         }
         m->key_lo = (double)m->kmin;
         m->key_scale = m->kmax > m->kmin ? 1.0 / ((double)m->kmax - (double)m->kmin) : 0.0;
@@ -563,29 +650,30 @@ int pyg_cdf_train(pyg_ctx* ctx, const int64_t* sample_keys, int64_t n, const pyg
         }
         PYG_CUDA(cudaMemcpyAsync(m->d_params, p.data(), p.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
         PYG_CUDA(cudaMemsetAsync(adam, 0, (size_t)2 * (2 + 2 * L) * 4, ctx->stream));
-        double root_scale = 2.0 / (double)n;
+        double root_scale = 2.0 / (double)nfit;
         PYG_CUDA(cudaMemcpyAsync(w.gscale, &root_scale, 8, cudaMemcpyHostToDevice, ctx->stream));
-        int gr = grid_for(ctx, n, CDF_THREADS, 4, 8);
+        int gr = grid_for(ctx, nfit, CDF_THREADS, 4, 8);
         const int E = opts->epochs;
         // Root: the least-squares line in one pass (the exact minimiser of
         // the root's squared loss, so no gradient steps follow).
-        root_ls_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(sorted, n, m->key_lo, m->key_scale, w.ls);
-        root_solve_kernel<<<1, 1, 0, ctx->stream>>>(w.ls, n, m->d_params);
+        root_ls_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(fit, nfit, m->key_lo, m->key_scale, w.ls);
+        root_solve_kernel<<<1, 1, 0, ctx->stream>>>(w.ls, nfit, m->d_params);
         ctx->launches += 2;
         PYG_CUDA(cudaGetLastError());
-        if ((rc = cdf_assign(ctx, w, sorted, n, L, m->key_lo, m->key_scale, m->d_params, m->d_yr))) break;
+        if ((rc = cdf_assign(ctx, w, fit, nfit, L, m->key_lo, m->key_scale, m->d_params, m->d_yr))) break;
         // Leaves: least-squares lines from one pass of per-leaf sums, then
         // E epochs of forward (residuals), backward (per-leaf gradient
         // sums) and projected Adam, which keep the slopes >= 0.
-        leaf_ls_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(n, w.leaf, w.u, m->d_yr, w.ls + 4);
+        leaf_ls_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(nfit, w.leaf, w.u, m->d_yr, w.ls + 4);
         leaf_solve_kernel<<<grid_for(ctx, L, 256, 1, 4), 256, 0, ctx->stream>>>(w.ls + 4, L, m->d_params);
         ctx->launches += 2;
         PYG_CUDA(cudaGetLastError());
         int ga = grid_for(ctx, 2 + 2 * L, 256, 1, 4);
         for (int e = 1; e <= E; ++e) {
             float lr = opts->lr * powf(0.01f, (float)(e - 1) / (float)E);
-            leaf_forward_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(n, w.leaf, w.u, m->d_yr, m->d_params, w.g, nullptr);
-            leaf_backward_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(n, w.leaf, w.u, w.g, w.raw);
+            leaf_forward_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(nfit, w.leaf, w.u, m->d_yr, m->d_params, w.g,
+                                                                      nullptr);
+            leaf_backward_kernel<<<gr, CDF_THREADS, 0, ctx->stream>>>(nfit, w.leaf, w.u, w.g, w.raw);
             // Root gradient entries are zero here; Adam skips scale-0 params.
             adam_kernel<<<ga, 256, 0, ctx->stream>>>(m->d_params + 2, w.raw + 2, w.gscale + 1, adam + 2,
                                                      adam + 2 + 2 * L + 2, 2 * L, lr, e);
@@ -614,6 +702,7 @@ int pyg_cdf_train(pyg_ctx* ctx, const int64_t* sample_keys, int64_t n, const pyg
     w.release(ctx);
     dfree(ctx, adam);
     dfree(ctx, sorted);
+    dfree(ctx, cont);
     if (rc) {
         pyg_cdf_free(ctx, m);
         return rc;
@@ -628,10 +717,62 @@ int pyg_cdf_free(pyg_ctx* ctx, pyg_cdf* m)
     if (ctx) {
         dfree(ctx, m->d_params);
         dfree(ctx, m->d_yr);
+        dfree(ctx, m->d_hkeys);
+        dfree(ctx, m->d_hbefore);
+        dfree(ctx, m->d_hw);
     }
     delete m;
     return PYG_OK;
 }
+
+}  // extern "C"
+
+namespace pyg {
+
+// C(k), the continuous part of the model, on the host (the predict
+// kernel's formula).
+static double cdf_continuous(const pyg_cdf* m, int64_t k)
+{
+    const double x = (double)(float)(((double)k - m->key_lo) * m->key_scale);
+    const double r = (double)m->a0 * x + (double)m->b0;
+    const int L = m->L;
+    const double fl = floor(L * r);
+    const int l = fl < 0 ? 0 : (fl > L - 1 ? L - 1 : (int)fl);
+    double uu = L * r - l;
+    uu = uu < 0 ? 0 : (uu > 1 ? 1 : uu);
+    double f = (double)m->la[l] * uu + (double)m->lb[l];
+    f = f < 0 ? 0 : (f > 1 ? 1 : f);
+    return m->ylo[l] + (m->yhi[l] - m->ylo[l]) * f;
+}
+
+// The key at which C reaches c: the leaf whose target range holds c, its
+// line inverted to a leaf coordinate, the root line inverted to a key;
+// `past` (one past the largest sample key) when c is beyond the model.
+static int64_t cdf_invert(const pyg_cdf* m, const std::vector<int>& ne, double c, int64_t past)
+{
+    if (ne.empty() || m->key_scale == 0) return past;
+    size_t lo = 0, hi = ne.size();
+    while (lo + 1 < hi) {
+        const size_t mid = (lo + hi) / 2;
+        if (m->ylo[ne[mid]] <= c) lo = mid;
+        else hi = mid;
+    }
+    const int l = ne[lo];
+    const double t = (c - m->ylo[l]) / (m->yhi[l] - m->ylo[l]);
+    const double a = m->la[l], b = m->lb[l];
+    double uu = a > 0 ? (t - b) / a : 0.0;
+    uu = std::min(1.0, std::max(0.0, uu));
+    const double r = ((double)l + uu) / (double)m->L;
+    const double x = m->a0 > 0 ? (r - (double)m->b0) / (double)m->a0 : 0.0;
+    const double kf = m->key_lo + x / m->key_scale;
+    if (!(kf > (double)m->kmin)) return m->kmin;
+    if (kf >= (double)m->kmax) return past;
+    return (int64_t)ceil(kf);
+}
+
+}  // namespace pyg
+
+extern "C" {
 
 int pyg_cdf_splitters(pyg_ctx* ctx, const pyg_cdf* m, int32_t fanout, int64_t* out)
 {
@@ -640,59 +781,60 @@ int pyg_cdf_splitters(pyg_ctx* ctx, const pyg_cdf* m, int32_t fanout, int64_t* o
         set_error("pyg_cdf_splitters: bad arguments");
         return PYG_ERR_ARG;
     }
-    const int L = m->L;
-    // Non-empty leaves in order (their y ranges are ordered and disjoint).
+    // Non-empty leaves in order (their target ranges are ordered, disjoint).
     std::vector<int> ne;
-    for (int l = 0; l < L; ++l)
+    for (int l = 0; l < m->L; ++l)
         if (m->yhi[l] > m->ylo[l]) ne.push_back(l);
     const int64_t past = m->kmax == INT64_MAX ? INT64_MAX : m->kmax + 1;  // past the largest sample key
+    // Heavy key h covers [Fb[h], Fb[h] + w_h) of F = (1 - W) C + heavy masses.
+    const int H = (int)m->heavy_key.size();
+    const double W = m->wheavy, cont = 1.0 - W;
+    std::vector<double> Fb(H), Fe(H);
+    for (int h = 0; h < H; ++h) {
+        Fb[h] = cont * cdf_continuous(m, m->heavy_key[h]) + m->heavy_before[h];
+        Fe[h] = Fb[h] + m->heavy_w[h];
+        if (h > 0) {  // keep the spans ordered when the fit is off
+            Fb[h] = std::max(Fb[h], Fe[h - 1]);
+            Fe[h] = Fb[h] + m->heavy_w[h];
+        }
+    }
+    std::vector<int> inside(fanout, -1);  // splitter j (1-based) falls in heavy key h's span
     int64_t prev = m->kmin;
     for (int j = 1; j < fanout; ++j) {
-        double q = (double)j / (double)fanout;
+        const double q = (double)j / (double)fanout;
+        // First heavy key whose span ends after q.
+        int a = 0, b = H;
+        while (a < b) {
+            const int mid = (a + b) >> 1;
+            if (Fe[mid] <= q) a = mid + 1;
+            else b = mid;
+        }
         int64_t key;
-        if (ne.empty() || m->key_scale == 0) {
-            key = past;
+        if (a < H && q >= Fb[a]) {
+            key = m->heavy_key[a];
+            inside[j] = a;
         } else {
-            // Leaf whose y range contains q.
-            size_t lo = 0, hi = ne.size();
-            while (lo + 1 < hi) {
-                size_t mid = (lo + hi) / 2;
-                if (m->ylo[ne[mid]] <= q) lo = mid;
-                else hi = mid;
-            }
-            int l = ne[lo];
-            double t = (q - m->ylo[l]) / (m->yhi[l] - m->ylo[l]);
-            double a = m->la[l], b = m->lb[l];
-            double uu = a > 0 ? (t - b) / a : 0.0;
-            uu = std::min(1.0, std::max(0.0, uu));
-            double r = ((double)l + uu) / (double)L;
-            double x = m->a0 > 0 ? (r - (double)m->b0) / (double)m->a0 : 0.0;
-            double kf = m->key_lo + x / m->key_scale;
-            if (!(kf > (double)m->kmin)) key = m->kmin;
-            else if (kf >= (double)m->kmax) key = past;
-            else key = (int64_t)ceil(kf);
+            // In the continuous part between heavy keys a - 1 and a.
+            const double below = a < H ? m->heavy_before[a] : W;
+            const double c = cont > 1e-12 ? (q - below) / cont : 0.0;
+            key = cdf_invert(m, ne, c, past);
+            if (a > 0) key = std::max(key, m->heavy_key[a - 1] == INT64_MAX ? INT64_MAX : m->heavy_key[a - 1] + 1);
+            if (a < H) key = std::min(key, m->heavy_key[a]);
         }
         if (key < prev) key = prev;
         out[j - 1] = key;
         prev = key;
     }
-    // Point masses: every splitter whose target quantile falls inside a
-    // heavy key's CDF step becomes that key, the last of them key + 1, so
-    // the heavy key gets a partition of its own (as exact quantiles do);
-    // neighbours are clamped to keep the splitters non-decreasing.
-    for (size_t h = 0; h < m->heavy_key.size(); ++h) {
-        const int64_t k = m->heavy_key[h];
-        int j0 = (int)floor(m->heavy_lo[h] * fanout) + 1;  // first j with j/F > lo
-        int j1 = (int)floor(m->heavy_hi[h] * fanout);      // last j with j/F <= hi
-        if (j1 > fanout - 1) j1 = fanout - 1;
-        if (j0 < 1) j0 = 1;
-        if (j0 > j1) continue;
-        for (int j = j0; j <= j1; ++j) out[j - 1] = k;
-        const int64_t k1 = k == INT64_MAX ? k : k + 1;
-        if (j1 > j0) out[j1 - 1] = k1;
-        for (int j = j0 - 1; j >= 1 && out[j - 1] > k; --j) out[j - 1] = k;
-        const int64_t after = j1 > j0 ? k1 : k;
-        for (int j = j1 + 1; j <= fanout - 1 && out[j - 1] < after; ++j) out[j - 1] = after;
+    // A heavy key that takes two or more splitters gets a range of its own:
+    // the last of them becomes key + 1 (exact quantiles do the same).
+    for (int j = fanout - 1; j >= 1; --j) {
+        const int h = inside[j];
+        if (h < 0 || (j + 1 < fanout && inside[j + 1] == h)) continue;  // not the last of its span
+        if (j - 1 >= 1 && inside[j - 1] == h) {
+            const int64_t k = m->heavy_key[h];
+            out[j - 1] = k == INT64_MAX ? k : k + 1;
+            for (int t = j + 1; t < fanout && out[t - 1] < out[j - 1]; ++t) out[t - 1] = out[j - 1];
+        }
     }
     return PYG_OK;
 }
@@ -706,8 +848,9 @@ int pyg_cdf_predict(pyg_ctx* ctx, const pyg_cdf* m, const int64_t* keys, int64_t
         return PYG_ERR_ARG;
     }
     if (n == 0) return PYG_OK;
-    predict_kernel<<<grid_for(ctx, n, 256, 4, 8), 256, 0, ctx->stream>>>(keys, n, m->key_lo, m->key_scale,
-                                                                        m->d_params, m->d_yr, m->L, out);
+    predict_kernel<<<grid_for(ctx, n, 256, 4, 8), 256, 0, ctx->stream>>>(
+        keys, n, m->key_lo, m->key_scale, m->d_params, m->d_yr, m->L, m->d_hkeys, m->d_hbefore, m->d_hw,
+        (int)m->heavy_key.size(), m->wheavy, out);
     PYG_LAUNCHED(ctx);
     return PYG_OK;
 }
