@@ -87,6 +87,30 @@ int pyg_memcpy_h2d(pyg_ctx* ctx, void* dst, const void* src, size_t bytes);
 int pyg_memcpy_d2h(pyg_ctx* ctx, void* dst, const void* src, size_t bytes);
 int pyg_memcpy_d2d(pyg_ctx* ctx, void* dst, const void* src, size_t bytes);
 
+/* ---- overlapped ingest ---------------------------------------------- */
+/* A host byte stream uploaded into one device buffer through a ring of
+ * pinned staging slots: while slot i's copy runs on the context's copy
+ * stream, the caller fills slot i+1 (reads a file chunk, parses text).
+ * Replaces the scan's whole-file load into memory followed by a separate
+ * copy (ParallelScanOp::scanStart / MemMappedTable::load,
+ * operators/parallelscan.cpp:176-190, operators/loaders/table.cpp:198-348).
+ *
+ *   pyg_upload_open   device buffer of `capacity` bytes (grown on demand),
+ *                     `slots` staging buffers of `slot_bytes` each.
+ *   pyg_upload_slot   the next staging buffer (waits for its last copy).
+ *   pyg_upload_commit queues the copy of its first `bytes` to the end of
+ *                     the uploaded data (`bytes` <= slot_bytes).
+ *   pyg_upload_finish waits for every copy; hands over the device buffer
+ *                     (owned by the caller, pyg_free) and the byte count,
+ *                     and frees the staging slots.
+ *   pyg_upload_abort  frees everything (after an error). */
+typedef struct pyg_upload pyg_upload;
+int pyg_upload_open(pyg_ctx* ctx, size_t capacity, size_t slot_bytes, int32_t slots, pyg_upload** out);
+int pyg_upload_slot(pyg_ctx* ctx, pyg_upload* up, void** buf, size_t* bytes);
+int pyg_upload_commit(pyg_ctx* ctx, pyg_upload* up, size_t bytes);
+int pyg_upload_finish(pyg_ctx* ctx, pyg_upload* up, void** device_buffer, size_t* total_bytes);
+int pyg_upload_abort(pyg_ctx* ctx, pyg_upload* up);
+
 /* ---- hash join ------------------------------------------------------ */
 /* Table modes.  AGGREGATE keeps one entry per distinct key with the
  * duplicate count and the wrapped sums of the stored build columns (all a

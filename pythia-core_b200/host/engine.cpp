@@ -204,9 +204,23 @@ Operator::ResultCode MaterializedOp::scanStop(unsigned short tid)
 
 // ------------------------------------------------------------------ scans
 
+int64_t ScanIngest::bytes = 0;
+double ScanIngest::seconds = 0;
+
+static double now_seconds()
+{
+    timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return t.tv_sec + t.tv_nsec * 1e-9;
+}
+
 // `scan` / `parallelscan` / `partitionedscan` (operators/scan.cpp,
 // parallelscan.cpp:41-190): all listed files, binary (raw packed tuples,
-// operators/loaders/table.cpp:198-348) or '|'-separated text.
+// operators/loaders/table.cpp:198-348) or '|'-separated text.  Loading is
+// lazy: a GPU parent (device_result) streams the files straight into HBM
+// through the overlapped upload ring (pyg_upload_*: the next chunk is read
+// or parsed while the previous one crosses PCIe); a host consumer
+// (getNext) loads them into pinned host pages.
 class ScanOp : public MaterializedOp {
 public:
     void init(const Setting& root, const Setting& node) override
@@ -227,56 +241,156 @@ public:
 
     ResultCode scanStart(unsigned short tid) override
     {
-        if (!loaded) load();
         out.rewind();
         return Ready;
     }
 
+    GetNextResultT getNext(unsigned short tid) override
+    {
+        if (!host_loaded && !dev_loaded) load_host();
+        return out.next(buffsize, schema.tuple_bytes);
+    }
+
+    bool device_result(const void** dev, int64_t* n) override
+    {
+        if (!dev_loaded) load_device();
+        return out.device(dev, n);
+    }
+
 private:
-    void load()
+    static int64_t file_bytes(const std::string& fn)
+    {
+        struct stat st;
+        if (stat(fn.c_str(), &st) != 0) throw EngineError("cannot open input file " + fn);
+        return (int64_t)st.st_size;
+    }
+
+    // Parses one '|'-separated text line into a packed tuple.
+    void parse_line(const std::string& line, uint8_t* tup) const
+    {
+        size_t pos = 0;
+        for (size_t c = 0; c < schema.columns(); ++c) {
+            size_t e = line.find_first_of(sep, pos);
+            std::string field = line.substr(pos, e == std::string::npos ? std::string::npos : e - pos);
+            int64_t v = strtoll(field.c_str(), nullptr, 10);
+            if (schema.types[c] == PYG_INT32) {
+                int32_t w = (int32_t)v;
+                memcpy(tup + schema.offs[c], &w, 4);
+            } else {
+                memcpy(tup + schema.offs[c], &v, 8);
+            }
+            pos = e == std::string::npos ? line.size() : e + 1;
+        }
+    }
+
+    // Calls sink(ptr, bytes) with runs of packed tuples read from every
+    // file; `want` asks the sink for its next buffer of at most `cap` bytes.
+    template <class Want, class Sink>
+    void read_files(Want want, Sink sink)
+    {
+        const int32_t tb = schema.tuple_bytes;
+        for (auto& fn : files) {
+            if (binary) {
+                int64_t left = file_bytes(fn);
+                if (left % tb) throw EngineError(fn + ": size is not a multiple of the tuple size");
+                FILE* f = fopen(fn.c_str(), "rb");
+                if (!f) throw EngineError("cannot open input file " + fn);
+                while (left > 0) {
+                    size_t cap = 0;
+                    uint8_t* buf = want(&cap);
+                    int64_t k = std::min<int64_t>(left, (int64_t)(cap / tb) * tb);
+                    if (k <= 0 || fread(buf, 1, (size_t)k, f) != (size_t)k) {
+                        fclose(f);
+                        throw EngineError(fn + ": short read");
+                    }
+                    sink(buf, k);
+                    left -= k;
+                }
+                fclose(f);
+            } else {
+                std::ifstream in(fn, std::ios::binary);
+                if (!in) throw EngineError("cannot open input file " + fn);
+                std::string line;
+                size_t cap = 0, used = 0;
+                uint8_t* buf = nullptr;
+                while (std::getline(in, line)) {
+                    if (line.empty()) continue;
+                    if (!buf || used + tb > cap) {
+                        if (buf && used) sink(buf, (int64_t)used);
+                        buf = want(&cap);
+                        used = 0;
+                        if (cap < (size_t)tb) throw EngineError("staging buffer smaller than a tuple");
+                    }
+                    parse_line(line, buf + used);
+                    used += tb;
+                }
+                if (buf && used) sink(buf, (int64_t)used);
+            }
+        }
+    }
+
+    void load_host()
     {
         HostRel& result = out.host;
         result.tuple_bytes = schema.tuple_bytes;
-        for (auto& fn : files) {
-            std::ifstream in(fn, std::ios::binary);
-            if (!in) throw EngineError("cannot open input file " + fn);
-            if (binary) {
-                in.seekg(0, std::ios::end);
-                int64_t bytes = (int64_t)in.tellg();
-                in.seekg(0);
-                if (bytes % schema.tuple_bytes)
-                    throw EngineError(fn + ": size is not a multiple of the tuple size");
-                result.reserve(result.ntuples * schema.tuple_bytes + bytes);
-                in.read((char*)result.data + result.ntuples * schema.tuple_bytes, bytes);
-                result.ntuples += bytes / schema.tuple_bytes;
-            } else {
-                std::string line;
-                std::vector<uint8_t> tup(schema.tuple_bytes);
-                while (std::getline(in, line)) {
-                    if (line.empty()) continue;
-                    size_t pos = 0;
-                    for (size_t c = 0; c < schema.columns(); ++c) {
-                        size_t e = line.find_first_of(sep, pos);
-                        std::string field = line.substr(pos, e == std::string::npos ? std::string::npos : e - pos);
-                        int64_t v = strtoll(field.c_str(), nullptr, 10);
-                        if (schema.types[c] == PYG_INT32) {
-                            int32_t w = (int32_t)v;
-                            memcpy(tup.data() + schema.offs[c], &w, 4);
-                        } else {
-                            memcpy(tup.data() + schema.offs[c], &v, 8);
-                        }
-                        pos = e == std::string::npos ? line.size() : e + 1;
-                    }
-                    result.append(tup.data(), 1);
+        result.ntuples = 0;
+        std::vector<uint8_t> text(1 << 20);
+        read_files(
+            [&](size_t* cap) -> uint8_t* {
+                if (binary) {
+                    // Binary files are read straight into the pinned pages.
+                    result.reserve(result.ntuples * schema.tuple_bytes + (1 << 24));
+                    *cap = (size_t)(result.cap_bytes - result.ntuples * schema.tuple_bytes);
+                    return result.data + result.ntuples * schema.tuple_bytes;
                 }
-            }
-        }
+                *cap = text.size();
+                return text.data();
+            },
+            [&](uint8_t* buf, int64_t bytes) {
+                if (binary)
+                    result.ntuples += bytes / schema.tuple_bytes;
+                else
+                    result.append(buf, bytes / schema.tuple_bytes);
+            });
         out.keep_host();
-        loaded = true;
+        host_loaded = true;
+        dev_loaded = false;
     }
 
+    void load_device()
+    {
+        int64_t total = 0;
+        for (auto& fn : files) total += file_bytes(fn);
+        const double t0 = now_seconds();
+        pyg_upload* up = nullptr;
+        check(pyg_upload_open(ctx, (size_t)std::max<int64_t>(total, schema.tuple_bytes), kSlotBytes, kSlots, &up),
+              "ingest open");
+        try {
+            read_files(
+                [&](size_t* cap) -> uint8_t* {
+                    void* b = nullptr;
+                    check(pyg_upload_slot(ctx, up, &b, cap), "ingest slot");
+                    return (uint8_t*)b;
+                },
+                [&](uint8_t* buf, int64_t bytes) { check(pyg_upload_commit(ctx, up, (size_t)bytes), "ingest copy"); });
+        } catch (...) {
+            pyg_upload_abort(ctx, up);
+            throw;
+        }
+        void* d = nullptr;
+        size_t bytes = 0;
+        check(pyg_upload_finish(ctx, up, &d, &bytes), "ingest finish");
+        out.keep_device(d, (int64_t)bytes / schema.tuple_bytes, schema.tuple_bytes);
+        ScanIngest::bytes += (int64_t)bytes;
+        ScanIngest::seconds += now_seconds() - t0;
+        dev_loaded = true;
+        host_loaded = false;
+    }
+
+    static constexpr size_t kSlotBytes = size_t(32) << 20;
+    static constexpr int kSlots = 3;
     std::vector<std::string> files;
-    bool binary = false, loaded = false;
+    bool binary = false, host_loaded = false, dev_loaded = false;
     std::string sep;
 };
 

@@ -113,6 +113,13 @@ struct ResultBuffer {
     void rewind() { served = 0; }
 };
 
+// Bytes the scans streamed into device memory through the overlapped
+// upload ring, and the wall time those loads took (the driver prints both).
+struct ScanIngest {
+    static int64_t bytes;
+    static double seconds;
+};
+
 // Serves a materialised relation as pages of buffsize bytes.
 class MaterializedOp : public Operator {
 public:

@@ -61,6 +61,8 @@ int main(int argc, char** argv)
         for (auto& line : q.counter_report()) std::cout << line << std::endl;
         std::cout << "GpuKernelLaunches: " << pyg_ctx_kernel_launches(Operator::ctx) << std::endl;
         std::cout << "DeviceToHostResultBytes: " << ResultBuffer::d2h_bytes << std::endl;
+        std::cout << "IngestToDeviceBytes: " << ScanIngest::bytes << std::endl;
+        std::cout << "IngestSeconds: " << ScanIngest::seconds << std::endl;
         q.threadClose();
         pyg_ctx_destroy(Operator::ctx);
     } catch (const std::exception& e) {

@@ -136,6 +136,11 @@ SIGNATURES = [
     ("pyg_memcpy_h2d", C.c_int, [_P, _P, _P, C.c_size_t]),
     ("pyg_memcpy_d2h", C.c_int, [_P, _P, _P, C.c_size_t]),
     ("pyg_memcpy_d2d", C.c_int, [_P, _P, _P, C.c_size_t]),
+    ("pyg_upload_open", C.c_int, [_P, C.c_size_t, C.c_size_t, _I32, C.POINTER(_P)]),
+    ("pyg_upload_slot", C.c_int, [_P, _P, C.POINTER(_P), C.POINTER(C.c_size_t)]),
+    ("pyg_upload_commit", C.c_int, [_P, _P, C.c_size_t]),
+    ("pyg_upload_finish", C.c_int, [_P, _P, C.POINTER(_P), C.POINTER(C.c_size_t)]),
+    ("pyg_upload_abort", C.c_int, [_P, _P]),
     ("pyg_hashjoin_build", C.c_int, [_P, C.POINTER(pyg_rel), _PI32, _I32, _PI32, _I32, _I32, C.c_float, C.POINTER(_P)]),
     ("pyg_hashtable_free", C.c_int, [_P, _P]),
     ("pyg_hashtable_stats", C.c_int, [_P, _P, _PI64, _PI64, _PI32]),
@@ -271,9 +276,12 @@ def host_rel(arr, types):
 
 
 class DevBuf:
-    def __init__(self, ctx, nbytes):
+    def __init__(self, ctx, nbytes, adopt=None):
         self.ctx = ctx
         self.nbytes = nbytes
+        if adopt is not None:  # take ownership of a pyg_alloc'd pointer
+            self.ptr = adopt
+            return
         p = C.c_void_p()
         check(lib().pyg_alloc(ctx.h, nbytes, C.byref(p)))
         self.ptr = p.value
@@ -341,6 +349,31 @@ class Ctx:
 
     def d2h(self, dst_np, src):
         check(lib().pyg_memcpy_d2h(self.h, dst_np.ctypes.data, _ptr(src), dst_np.nbytes))
+
+    def upload(self, chunks, capacity=0, slot_bytes=32 << 20, slots=3):
+        """Streams an iterable of byte-like numpy arrays into one device
+        buffer through the overlapped upload ring (pyg_upload_*); each
+        chunk is split into slot-sized pieces.  Returns a DevBuf."""
+        L = lib()
+        up = C.c_void_p()
+        check(L.pyg_upload_open(self.h, capacity, slot_bytes, slots, C.byref(up)))
+        try:
+            for chunk in chunks:
+                b = np.ascontiguousarray(chunk).view(np.uint8).reshape(-1)
+                off = 0
+                while off < b.size:
+                    buf, cap = C.c_void_p(), C.c_size_t()
+                    check(L.pyg_upload_slot(self.h, up, C.byref(buf), C.byref(cap)))
+                    k = min(cap.value, b.size - off)
+                    C.memmove(buf.value, b.ctypes.data + off, k)
+                    check(L.pyg_upload_commit(self.h, up, k))
+                    off += k
+        except BaseException:
+            L.pyg_upload_abort(self.h, up)
+            raise
+        dev, total = C.c_void_p(), C.c_size_t()
+        check(L.pyg_upload_finish(self.h, up, C.byref(dev), C.byref(total)))
+        return DevBuf(self, total.value, adopt=dev.value)
 
     # -- hash join ----------------------------------------------------
     def hashjoin_build(self, rel, key_cols, payload_cols=(), mode=HT_AGGREGATE, load_factor=0.5):
