@@ -760,7 +760,9 @@ def workload_line(args, torch, pyg, ctx, rank, world, local, dist, stream):
         abytes = units * 16
         metric = "batched fragments tuples/sec (256 PK-FK join+sum fragments, persistent kernel in a CUDA graph)"
         workload = {"workload": "256 join fragments", "fragments": 256, "tuples": units,
-                    "tuning": {"block_threads": tuning.block_threads, "blocks_per_sm": tuning.blocks_per_sm}}
+                    "tuning": {"block_threads": tuning.block_threads, "blocks_per_sm": tuning.blocks_per_sm,
+                               "load_factor": round(tuning.load_factor, 2), "chunk_tuples": tuning.chunk_tuples,
+                               "large_build": tuning.large_build}}
 
     ms, outs = _device_timed(torch, stream, fn, args.steps, args.warmup, dist)
     # A second timed run with the clock sampler on; the line reports it.
@@ -773,9 +775,14 @@ def workload_line(args, torch, pyg, ctx, rank, world, local, dist, stream):
         lat = np.concatenate([o[1] for o in outs])
         extra["fragment_latency_ms"] = {"p50": round(float(np.percentile(lat, 50)), 4),
                                         "p99": round(float(np.percentile(lat, 99)), 4)}
-        plain_ms, _ = _device_timed(torch, stream, lambda: ctx.batch_run_plain(frags), max(1, args.steps // 2), 1,
-                                    dist)
-        extra["plain_launches_ms_per_step"] = round(plain_ms / max(1, args.steps // 2), 4)
+        plain_ms, plain_outs = _device_timed(torch, stream, lambda: ctx.batch_run_plain(frags)[2],
+                                             max(1, args.steps // 2), 1, dist)
+        plat = np.concatenate(plain_outs)
+        extra["plain"] = {"ms_per_step": round(plain_ms / max(1, args.steps // 2), 4),
+                          "fragment_latency_ms": {"p50": round(float(np.percentile(plat, 50)), 4),
+                                                  "p99": round(float(np.percentile(plat, 99)), 4)},
+                          "what": "the same fragments one pyg_hashjoin_agg call after another"}
+        extra["batched_over_plain"] = round(extra["plain"]["ms_per_step"] / step_ms, 3)
         ctx.batch_free(b)
     achieved = abytes / (step_ms / 1e3) / 1e9
     line = {"metric": metric, "value": units * args.steps * world / (ms / 1e3), "unit": UNIT, "n_gpus": world,
@@ -820,7 +827,7 @@ def run_secondary(args, torch, pyg, ctx, local, stream):
             out[name] = {"metric": line["metric"], "value": line["value"], "ms_per_step": line["ms_per_step"],
                          "roofline_frac": line["roofline"]["frac"], "config": line["config"],
                          "clocks": line["clocks"]}
-            for k in ("mpsm", "fragment_latency_ms", "plain_launches_ms_per_step"):
+            for k in ("mpsm", "fragment_latency_ms", "plain", "batched_over_plain"):
                 if k in line:
                     out[name][k] = line[k]
         except Exception as ex:  # a secondary must not hide the headline

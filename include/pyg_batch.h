@@ -10,6 +10,13 @@
  * reports PYG_ERR_TIMEOUT instead of hanging) only for build items of its
  * own fragment that other CTAs already dequeued.  The queue reset and the
  * kernel are captured once in a CUDA graph and replayed per run.
+ *
+ * Fragments whose build side has at least `large_build` tuples are not
+ * queued: their tables would not stay in L2 beside the others', and their
+ * work dwarfs a call's fixed cost, so after the graph they run one by one
+ * through the partitioned join (pyg_hashjoin_agg).  The persistent kernel
+ * takes the many small and medium fragments, whose separate calls would be
+ * dominated by launches and host synchronisations.
  */
 #ifndef PYG_BATCH_H
 #define PYG_BATCH_H
@@ -37,7 +44,8 @@ typedef struct pyg_tuning {
     int32_t blocks_per_sm;       /* resident CTAs per SM                     */
     float load_factor;           /* per-fragment table load factor           */
     int32_t chunk_tuples;        /* work-item grain in tuples                */
-    int32_t fanout;              /* radix bits of the single large join      */
+    int32_t large_build;         /* build tuples from which a fragment runs
+                                    as its own partitioned join (0: 2^20) */
 } pyg_tuning;
 
 /* Plans n fragments (tuning NULL: the autotuner's cached choice, else

@@ -1,7 +1,9 @@
 // Batched PK-FK join + sum fragments: one persistent kernel over a device
-// work queue, captured in a CUDA graph; plain sequential baseline; and the
-// autotuner that picks the persistent kernel's launch shape, the table load
-// factor and the work-item grain.
+// work queue for the small and medium fragments, captured in a CUDA graph,
+// then the large fragments as their own partitioned joins; the plain
+// sequential baseline; and the autotuner that picks the persistent kernel's
+// launch shape, the table load factor, the work-item grain and the size
+// from which a fragment runs on its own.
 #include <string.h>
 
 #include <algorithm>
@@ -48,6 +50,10 @@ struct BatchState {
 
 constexpr int RES_WORDS = 6;  // count, sum, then empty-marker key stats: build count/sum, probe count/sum
 constexpr long long kWaitLimit = 1LL << 22;  // x ~256 ns sleeps, about one second
+// Build tuples from which a fragment runs as its own partitioned join by
+// default: its table (32 MB and more at load factor 0.5) would crowd the
+// other fragments' tables out of L2.
+constexpr int64_t kLargeBuild = (int64_t)1 << 20;
 
 struct BatchDev {
     const FragDesc* frags;
@@ -256,6 +262,9 @@ struct pyg_batch {
     cudaGraphExec_t exec = nullptr;
     std::vector<int32_t> order;  // fragments with no work item (empty) still report results
     std::vector<char> empty_frag;
+    // Fragments run after the graph as their own partitioned joins.
+    std::vector<int32_t> large;
+    std::vector<pyg_fragment> large_frag;
 };
 
 namespace pyg {
@@ -270,7 +279,7 @@ static pyg_tuning default_tuning()
     t.blocks_per_sm = 2;
     t.load_factor = 0.7f;  // 16-byte slots: a 2^22-tuple build's table (96 MB) stays in L2
     t.chunk_tuples = 16384;
-    t.fanout = 0;
+    t.large_build = 0;
     return t;
 }
 
@@ -284,6 +293,34 @@ static std::string signature(const pyg_fragment* fr, int n)
     std::ostringstream os;
     os << "n" << n << "_b" << (int)(b > 0 ? log2(b) : 0) << "_p" << (int)(p > 0 ? log2(p) : 0);
     return os.str();
+}
+
+// One fragment through pyg_hashjoin_agg with the automatic algorithm (the
+// best single call): count and sum(build payload + probe value).
+static int join_fragment(pyg_ctx* ctx, const pyg_fragment& f, int64_t* count, int64_t* sum)
+{
+    pyg_rel R, S;
+    memset(&R, 0, sizeof(R));
+    R.base = f.build;
+    R.ntuples = f.nbuild;
+    R.tuple_bytes = 16;
+    R.ncols = 2;
+    R.col_offset[1] = 8;
+    R.col_type[0] = R.col_type[1] = PYG_INT64;
+    R.on_device = 1;
+    S = R;
+    S.base = f.probe;
+    S.ntuples = f.nprobe;
+    int32_t k = 0;
+    pyg_proj proj[2] = {{0, 1}, {1, 1}};
+    pyg_join_opts o = {PYG_JOIN_AUTO, 0, 0.5f, 0};
+    pyg_join_result r;
+    int rc = pyg_hashjoin_agg(ctx, &R, &k, &S, &k, 1, proj, 2, &o, &r, nullptr);
+    if (!rc) {
+        *count = r.count;
+        *sum = (int64_t)((uint64_t)r.sums[0] + (uint64_t)r.sums[1]);
+    }
+    return rc;
 }
 
 static int batch_alloc(pyg_ctx* ctx, pyg_batch* b, void** p, size_t bytes)
@@ -331,7 +368,8 @@ int pyg_batch_create(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const p
         if (it != g_tune_cache.end()) t = it->second;
     }
     if (t.block_threads < 64 || t.block_threads > 1024 || (t.block_threads & 31) || t.blocks_per_sm < 1 ||
-        t.blocks_per_sm > 16 || !(t.load_factor > 0 && t.load_factor <= 0.9f) || t.chunk_tuples < 256) {
+        t.blocks_per_sm > 16 || !(t.load_factor > 0 && t.load_factor <= 0.9f) || t.chunk_tuples < 256 ||
+        t.large_build < 0) {
         set_error("pyg_batch_create: bad tuning");
         return PYG_ERR_ARG;
     }
@@ -344,19 +382,27 @@ int pyg_batch_create(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const p
     pyg_batch* b = new pyg_batch();
     b->n = n;
     b->tuning = t;
+    const int64_t large_build = t.large_build > 0 ? t.large_build : kLargeBuild;
+    std::vector<char> is_large(n, 0);
+    for (int i = 0; i < n; ++i)
+        if (frags[i].nbuild >= large_build) {
+            is_large[i] = 1;
+            b->large.push_back(i);
+            b->large_frag.push_back(frags[i]);
+        }
     // Tables: one arena of 16-byte slots and one of extra-copy counters,
-    // per-fragment capacity nbuild / load factor.
+    // per-fragment capacity nbuild / load factor (queued fragments only).
     std::vector<FragDesc> fd(n);
     uint64_t total_slots = 0;
     for (int i = 0; i < n; ++i) {
-        uint64_t cap = (uint64_t)((double)frags[i].nbuild / t.load_factor) + 64;
+        uint64_t cap = is_large[i] ? 0 : (uint64_t)((double)frags[i].nbuild / t.load_factor) + 64;
         fd[i].cap = cap;
         total_slots += cap;
     }
     ulonglong2* arena;
     unsigned* extra;
-    if ((rc = batch_alloc(ctx, b, (void**)&arena, total_slots * sizeof(ulonglong2))) ||
-        (rc = batch_alloc(ctx, b, (void**)&extra, total_slots * sizeof(unsigned)))) {
+    if ((rc = batch_alloc(ctx, b, (void**)&arena, std::max<uint64_t>(total_slots, 1) * sizeof(ulonglong2))) ||
+        (rc = batch_alloc(ctx, b, (void**)&extra, std::max<uint64_t>(total_slots, 1) * sizeof(unsigned)))) {
         pyg_batch_free(ctx, b);
         return rc;
     }
@@ -378,9 +424,9 @@ int pyg_batch_create(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const p
     for (int i : order) {
         FragDesc& f = fd[i];
         f.build = (const longlong2*)frags[i].build;
-        f.nb = frags[i].nbuild;
+        f.nb = is_large[i] ? 0 : frags[i].nbuild;
         f.probe = (const longlong2*)frags[i].probe;
-        f.np = frags[i].nprobe;
+        f.np = is_large[i] ? 0 : frags[i].nprobe;
         f.table = arena + toff[i];
         f.extra = extra + toff[i];
         f.n_init = f.n_build = f.n_probe = 0;
@@ -397,7 +443,7 @@ int pyg_batch_create(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const p
     WorkItem* ditems;
     b->state_bytes = sizeof(BatchState) + (size_t)n * (4 * sizeof(unsigned) + (RES_WORDS + 1) * 8) + 64;
     if ((rc = batch_alloc(ctx, b, (void**)&dfd, n * sizeof(FragDesc))) ||
-        (rc = batch_alloc(ctx, b, (void**)&ditems, items.size() * sizeof(WorkItem))) ||
+        (rc = batch_alloc(ctx, b, (void**)&ditems, std::max<size_t>(items.size(), 1) * sizeof(WorkItem))) ||
         (rc = batch_alloc(ctx, b, &b->state, b->state_bytes))) {
         pyg_batch_free(ctx, b);
         return rc;
@@ -448,11 +494,28 @@ int pyg_batch_run(pyg_ctx* ctx, pyg_batch* b, int64_t* counts, int64_t* sums, do
         set_error("pyg_batch_run: null batch");
         return PYG_ERR_ARG;
     }
+    // Queued fragments: the graph.  Large fragments: their own partitioned
+    // joins, after it on the same stream; their latency is taken from
+    // events against one recorded just before the graph.
+    const size_t nl = b->large.size();
+    std::vector<cudaEvent_t> ev(nl ? nl + 1 : 0);
+    for (auto& e : ev) PYG_CUDA(cudaEventCreate(&e));
+    if (nl) cudaEventRecord(ev[0], ctx->stream);
     PYG_CUDA(cudaGraphLaunch(b->exec, ctx->stream));
     ctx->launches += 1;
     std::vector<unsigned char> st(b->state_bytes);
     PYG_CUDA(cudaMemcpyAsync(st.data(), b->state, b->state_bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::vector<int64_t> lc(nl), ls(nl);
+    for (size_t j = 0; j < nl && !rc; ++j) {
+        rc = join_fragment(ctx, b->large_frag[j], &lc[j], &ls[j]);
+        cudaEventRecord(ev[j + 1], ctx->stream);
+    }
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    std::vector<float> lat_large(nl, 0.f);
+    for (size_t j = 0; j < nl && !rc && e == cudaSuccess; ++j) cudaEventElapsedTime(&lat_large[j], ev[0], ev[j + 1]);
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_status(e, "pyg_batch_run");
     const BatchState* bs = (const BatchState*)st.data();
     if (bs->error) {
         set_error("pyg_batch_run: a bounded wait for a fragment's build gave up");
@@ -470,6 +533,12 @@ int pyg_batch_run(pyg_ctx* ctx, pyg_batch* b, int64_t* counts, int64_t* sums, do
         if (sums) sums[i] = (int64_t)sum;
         if (latency_ms) latency_ms[i] = td[i] > bs->t0 ? (double)(td[i] - bs->t0) / 1e6 : 0.0;
     }
+    for (size_t j = 0; j < nl; ++j) {
+        const int i = b->large[j];
+        if (counts) counts[i] = lc[j];
+        if (sums) sums[i] = ls[j];
+        if (latency_ms) latency_ms[i] = lat_large[j];
+    }
     return PYG_OK;
 }
 
@@ -486,27 +555,12 @@ int pyg_batch_run_plain(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, int6
     for (auto& e : ev) cudaEventCreate(&e);
     cudaEventRecord(ev[0], ctx->stream);
     for (int i = 0; i < n && !rc; ++i) {
-        pyg_rel R, S;
-        memset(&R, 0, sizeof(R));
-        R.base = frags[i].build;
-        R.ntuples = frags[i].nbuild;
-        R.tuple_bytes = 16;
-        R.ncols = 2;
-        R.col_offset[1] = 8;
-        R.col_type[0] = R.col_type[1] = PYG_INT64;
-        R.on_device = 1;
-        S = R;
-        S.base = frags[i].probe;
-        S.ntuples = frags[i].nprobe;
-        int32_t k = 0;
-        pyg_proj proj[2] = {{0, 1}, {1, 1}};
-        pyg_join_opts o = {PYG_JOIN_AUTO, 0, 0.5f, 0};  // the best single-call algorithm per fragment
-        pyg_join_result r;
-        rc = pyg_hashjoin_agg(ctx, &R, &k, &S, &k, 1, proj, 2, &o, &r, nullptr);
+        int64_t c = 0, sm = 0;
+        rc = join_fragment(ctx, frags[i], &c, &sm);
         cudaEventRecord(ev[i + 1], ctx->stream);
         if (!rc) {
-            if (counts) counts[i] = r.count;
-            if (sums) sums[i] = (int64_t)((uint64_t)r.sums[0] + (uint64_t)r.sums[1]);
+            if (counts) counts[i] = c;
+            if (sums) sums[i] = sm;
         }
     }
     cudaStreamSynchronize(ctx->stream);
@@ -523,8 +577,9 @@ int pyg_batch_inject_stall(pyg_ctx* ctx, pyg_batch* b, int32_t frag)
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (!b || frag < 0 || frag >= b->n) {
-        set_error("pyg_batch_inject_stall: bad fragment");
+    if (!b || frag < 0 || frag >= b->n ||
+        std::find(b->large.begin(), b->large.end(), frag) != b->large.end()) {
+        set_error("pyg_batch_inject_stall: not a queued fragment");
         return PYG_ERR_ARG;
     }
     // Raise the fragment's expected build-item count by one: its probe
@@ -557,7 +612,7 @@ int pyg_autotune(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const char*
         std::ifstream in(cache_path);
         std::string s;
         pyg_tuning t;
-        while (in >> s >> t.block_threads >> t.blocks_per_sm >> t.load_factor >> t.chunk_tuples >> t.fanout) {
+        while (in >> s >> t.block_threads >> t.blocks_per_sm >> t.load_factor >> t.chunk_tuples >> t.large_build) {
             if (s == sig) {
                 std::lock_guard<std::mutex> g(g_tune_mu);
                 g_tune_cache[sig] = t;
@@ -566,11 +621,13 @@ int pyg_autotune(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const char*
             }
         }
     }
-    // Candidate grid: block shape x occupancy x load factor x grain.
+    // Candidate grid of the persistent kernel (block shape x occupancy x
+    // load factor x grain), timed on the graph alone; then the size from
+    // which fragments run as their own joins, timed on whole runs.
     const int bts[] = {256, 512, 1024};
     const int bps[] = {1, 2, 4};
-    const float lfs[] = {0.5f, 0.7f, 0.8f};
-    const int chunks[] = {4096, 16384, 65536};
+    const float lfs[] = {0.5f, 0.7f};
+    const int chunks[] = {16384, 65536};
     float best = 1e30f;
     pyg_tuning best_t = default_tuning();
     cudaEvent_t e0, e1;
@@ -602,6 +659,33 @@ int pyg_autotune(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const char*
                     }
                 }
         }
+    {
+        const int32_t larges[] = {1 << 18, 1 << 20, 1 << 22};
+        pyg_tuning base = best_t;
+        best = 1e30f;
+        for (int32_t lb : larges) {
+            pyg_tuning t = base;
+            t.large_build = lb;
+            pyg_batch* b = nullptr;
+            if (pyg_batch_create(ctx, frags, n, &t, &b)) continue;
+            float ms = 1e30f;
+            bool good = pyg_batch_run(ctx, b, nullptr, nullptr, nullptr) == PYG_OK;
+            for (int rep = 0; rep < 2 && good; ++rep) {
+                cudaEventRecord(e0, ctx->stream);
+                good = pyg_batch_run(ctx, b, nullptr, nullptr, nullptr) == PYG_OK;
+                cudaEventRecord(e1, ctx->stream);
+                cudaEventSynchronize(e1);
+                float x = 0;
+                cudaEventElapsedTime(&x, e0, e1);
+                ms = std::min(ms, x);
+            }
+            pyg_batch_free(ctx, b);
+            if (good && ms < best) {
+                best = ms;
+                best_t = t;
+            }
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     {
@@ -611,7 +695,7 @@ int pyg_autotune(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const char*
     if (cache_path) {
         std::ofstream o(cache_path, std::ios::app);
         o << sig << " " << best_t.block_threads << " " << best_t.blocks_per_sm << " " << best_t.load_factor << " "
-          << best_t.chunk_tuples << " " << best_t.fanout << "\n";
+          << best_t.chunk_tuples << " " << best_t.large_build << "\n";
     }
     *out = best_t;
     return PYG_OK;

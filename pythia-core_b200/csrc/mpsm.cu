@@ -493,6 +493,12 @@ static int mpsm_run(pyg_ctx* ctx, const pyg_rel* build, int32_t bkey, const pyg_
             double rate = o->sample_rate > 0 ? o->sample_rate : 0.01;
             int64_t stride = (int64_t)llround(1.0 / rate);
             if (stride < 1) stride = 1;
+            // The learned model needs far fewer samples than quantile
+            // splitters (which want tens of samples per range): its leaves
+            // are fitted lines, so at most CDF_MPSM_SAMPLE keys (about 256
+            // per leaf) are drawn for it.
+            if (o->splitter_kind == PYG_MPSM_SPLIT_LEARNED && nS / stride > CDF_MPSM_SAMPLE)
+                stride = (nS + CDF_MPSM_SAMPLE - 1) / CDF_MPSM_SAMPLE;
             int64_t ns = (nS + stride - 1) / stride;
             if (ns < 2) {
                 stride = 1;

@@ -110,7 +110,7 @@ class pyg_fragment(C.Structure):
 
 class pyg_tuning(C.Structure):
     _fields_ = [("block_threads", C.c_int32), ("blocks_per_sm", C.c_int32), ("load_factor", C.c_float),
-                ("chunk_tuples", C.c_int32), ("fanout", C.c_int32)]
+                ("chunk_tuples", C.c_int32), ("large_build", C.c_int32)]
 
 
 _lib = None

@@ -162,3 +162,26 @@ def test_bounded_wait_reports_timeout_and_context_survives(ctx, torch_cuda):
         assert rc == pyg.PYG_OK and [(int(x), int(y)) for x, y in zip(c, s)] == expected(host)
     finally:
         ctx.batch_free(b)
+
+
+@pytest.mark.parametrize("large_build", [1 << 8, 1 << 11])
+def test_large_fragments_run_as_their_own_joins(ctx, torch_cuda, large_build):
+    """Fragments with at least large_build build tuples leave the queue and
+    run after the graph as their own joins (duplicate keys, INT64_MIN keys
+    and empty sides among them); every fragment's result still equals the
+    oracle's, latencies are reported for all, and the stall hook refuses a
+    fragment that is not queued."""
+    host, dev = make_fragments(torch_cuda, 16, 8, max_log=13)
+    frags = ctx.fragments(dev)
+    b = ctx.batch_create(frags, pyg.pyg_tuning(512, 2, 0.7, 4096, large_build))
+    try:
+        for _ in range(2):
+            rc, c, s, lat = ctx.batch_run(b, len(dev))
+            assert rc == pyg.PYG_OK
+            assert [(int(x), int(y)) for x, y in zip(c, s)] == expected(host)
+            assert all(x >= 0 for x in lat)
+        large = [i for i, d in enumerate(dev) if d[1] >= large_build]
+        assert large
+        assert pyg.lib().pyg_batch_inject_stall(ctx.h, b, large[0]) == pyg.PYG_ERR_ARG
+    finally:
+        ctx.batch_free(b)
