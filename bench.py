@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--theta", type=float, default=0.0)
     ap.add_argument("--impl", default="pyg", choices=["pyg", "reference"])
     ap.add_argument("--load-factor", type=float, default=0.5)
-    ap.add_argument("--algo", default="radix", choices=["radix", "radix-l2", "direct", "auto"])
+    ap.add_argument("--algo", default="radix", choices=["radix", "direct", "auto"])
     ap.add_argument("--radix-bits", type=int, default=0, help="log2 partition fan-out (0 = automatic)")
     ap.add_argument("--scale-shift", type=int, default=0, help="shrink both relations by 2^s (debug only)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -357,8 +357,7 @@ def main_gpu(args):
     Sr = pyg.Rel(S, nS, [pyg.INT64, pyg.INT64])
     proj = [(0, 1), (1, 1)]
 
-    algo = {"radix": pyg.JOIN_RADIX, "radix-l2": pyg.JOIN_RADIX_L2, "direct": pyg.JOIN_DIRECT,
-            "auto": pyg.JOIN_AUTO}[args.algo]
+    algo = {"radix": pyg.JOIN_RADIX, "direct": pyg.JOIN_DIRECT, "auto": pyg.JOIN_AUTO}[args.algo]
 
     def step(rrel, srel, stats=False):
         r = ctx.hashjoin_agg(rrel, [0], srel, [0], proj, algo, args.radix_bits, args.load_factor, stats=stats)
@@ -645,8 +644,7 @@ def workload_line(args, torch, pyg, ctx, rank, world, local, dist, stream):
         ctx.gen_pk(R, nR, 7, SEED_KEYS)
         ctx.gen_fk(S, nS, nR, 0.0, SEED_KEYS, 1000, SEED_PROBE + rank)
         Rr, Sr = pyg.Rel(R, nR, [I64, I64]), pyg.Rel(S, nS, [I64, I64])
-        algo = {"radix": pyg.JOIN_RADIX, "radix-l2": pyg.JOIN_RADIX_L2, "direct": pyg.JOIN_DIRECT,
-            "auto": pyg.JOIN_AUTO}[args.algo]
+        algo = {"radix": pyg.JOIN_RADIX, "direct": pyg.JOIN_DIRECT, "auto": pyg.JOIN_AUTO}[args.algo]
         # One C-ABI call per step (arguments marshalled once): the step is
         # the library's join + sum with its result read back to the host.
         fn = ctx.hashjoin_agg_prepared(Rr, [0], Sr, [0], [(1, 1)], algo)

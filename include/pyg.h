@@ -168,20 +168,13 @@ int pyg_hashjoin_probe_materialize(pyg_ctx* ctx, const pyg_hashtable* ht, const 
  * PYG_JOIN_RADIX: both sides partitioned by the top radix_bits bits of the
  * key hash first, then joined partition by partition with shared-memory
  * tables (16-byte (int64, int64) device relations, projection over
- * {B$1, P$1}; other shapes use DIRECT).  PYG_JOIN_RADIX_L2: the same
- * inputs partitioned once per side (up to 2^9 partitions, 8-byte packed
- * words in one key frame), then each partition's table built in global
- * memory sized to stay in L2 while the probe partition streams past it:
- * the probe side is written and read once instead of twice (falls back to
- * RADIX when the key ranges allow no shared packed frame or a build key
- * repeats).  PYG_JOIN_AUTO picks RADIX for
+ * {B$1, P$1}; other shapes use DIRECT).  PYG_JOIN_AUTO picks RADIX for
  * eligible inputs whose direct table would exceed 64 MB (so not stay in
  * L2) and whose probe side has at least 2^22 tuples.  stats (optional)
  * receives phase timings. */
 #define PYG_JOIN_AUTO   0
 #define PYG_JOIN_DIRECT 1
 #define PYG_JOIN_RADIX  2
-#define PYG_JOIN_RADIX_L2 3
 
 typedef struct pyg_join_opts {
     int32_t algorithm;     /* PYG_JOIN_*                               */

@@ -982,10 +982,9 @@ int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_ke
     // AUTO: the direct join while its table (16 bytes per slot at load
     // factor lf) fits well inside the 126 MB L2, the radix join beyond.
     const double table_bytes = 16.0 * (double)build->ntuples / (double)lf;
-    bool radix = eligible && (algorithm == PYG_JOIN_RADIX || algorithm == PYG_JOIN_RADIX_L2 ||
+    bool radix = eligible && (algorithm == PYG_JOIN_RADIX ||
                               (algorithm == PYG_JOIN_AUTO && table_bytes > 64.0 * 1024 * 1024 &&
                                probe->ntuples >= ((int64_t)1 << 22)));
-    const bool l2 = algorithm == PYG_JOIN_RADIX_L2;
     PhaseTimer tm;
     if (!radix && eligible) {
         // 16-byte device relations: the one-shot direct join (falls back
@@ -1028,7 +1027,7 @@ int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_ke
     // shared-memory table per CTA (radixjoin.cu).
     unsigned long long r3[3];
     if ((rc = radix_join16(ctx, build->base, build->ntuples, probe->base, probe->ntuples, opts ? opts->radix_bits : 0,
-                           l2, r3, stats)))
+                           r3, stats)))
         return rc;
     memset(out, 0, sizeof(*out));
     out->count = (int64_t)r3[0];

@@ -268,7 +268,15 @@ constexpr int RJ32_THREADS = 512;
 constexpr int RJ32_TABLE_BYTES = 96 * 1024;
 constexpr unsigned RJ32_SLOTS = RJ32_TABLE_BYTES / 8;
 constexpr unsigned RJ32_RCAP = RJ32_SLOTS / 2;
-constexpr int RJ32_U = 8;  // probe words in flight per thread
+#ifndef PYG_RJ32_U
+#define PYG_RJ32_U 8
+#endif
+#ifndef PYG_RJ32_PREFETCH
+#define PYG_RJ32_PREFETCH 8192
+#endif
+constexpr int RJ32_U = PYG_RJ32_U;  // probe words in flight per thread
+// Words of the next item's probe chunk pulled into L2 ahead of use.
+constexpr unsigned RJ32_PREFETCH = PYG_RJ32_PREFETCH;
 constexpr unsigned long long kEmptyWord = ~0ULL;
 
 // Slot of a key offset: the MurmurHash3 32-bit finaliser, then
@@ -301,7 +309,7 @@ __global__ void __launch_bounds__(RJ32_THREADS, 2) rj_join32_kernel(RJJoinArgs a
                 if (item_next < a.nitems) {
                     const RJItem nx = a.items[item_next];
                     rj_prefetch_l2(Rw + nx.r0, (unsigned long long)nx.rn * 8);
-                    rj_prefetch_l2(Sw + nx.s0, (unsigned long long)min(nx.sn, 8192u) * 8);
+                    rj_prefetch_l2(Sw + nx.s0, (unsigned long long)min(nx.sn, RJ32_PREFETCH) * 8);
                 }
             }
         }
@@ -364,172 +372,6 @@ __global__ void __launch_bounds__(RJ32_THREADS, 2) rj_join32_kernel(RJJoinArgs a
         atomicAdd(&a.acc[0], (unsigned long long)cnt);
         atomicAdd(&a.acc[1], (unsigned long long)b);
         atomicAdd(&a.acc[2], (unsigned long long)p);
-    }
-    if (__any_sync(0xffffffffu, dup) && (threadIdx.x & 31) == 0) atomicOr(a.dup, 1u);
-}
-
-// ---------------------------------------------------------------------------
-// One partition pass per relation, L2-resident partition tables.
-//
-// Both relations are hash-partitioned once (at most 2^9 partitions) and
-// packed in one key frame.  Partition c's table is the build words of R_c
-// in open addressing (8-byte slots, load factor <= 0.5) in global memory,
-// a few MB, so a wave of W partitions' tables stays in L2 while S_c
-// streams past it: S is read once from HBM after its single pass, instead
-// of being written and read again by a second pass.  Launch k probes wave
-// k-1, builds wave k and clears the buffer wave k+1 will use; three
-// buffers rotate, so within a launch the three kinds of items touch
-// different tables and need no ordering.  Items are decoded on the device
-// from per-partition tile prefixes; CTAs take them from a queue.
-
-constexpr int L2J_THREADS = 512;
-constexpr int L2J_U = 8;                    // probe words in flight per thread
-constexpr unsigned L2J_TILE = 8192;         // words per build / probe item
-constexpr unsigned L2J_CLEAR = 1u << 16;    // slots per clear item
-constexpr size_t L2J_BUDGET = 72ull << 20;  // bytes of the three table buffers
-
-struct L2Part {
-    unsigned long long rstart, rcount, sstart, scount;  // words
-};
-
-struct L2JoinArgs {
-    const unsigned long long* R;
-    const unsigned long long* S;
-    unsigned long long* tables;       // 3 buffers x W tables x slots
-    unsigned long long slots;         // per table (a multiple of 64)
-    const L2Part* parts;              // F partitions
-    const unsigned long long* btile;  // F + 1: prefix of build tiles
-    const unsigned long long* ptile;  // F + 1: prefix of probe tiles
-    int W;                            // partitions per wave
-    // This launch: probe partitions [pb, pe) from buffer pbuf, build
-    // partitions [bb, be) into buffer bbuf, clear buffer cbuf (-1: none).
-    int pb, pe, pbuf, bb, be, bbuf, cbuf;
-    unsigned long long np, nb, nc;    // items of each kind
-    unsigned* next;
-    unsigned long long* acc;
-    unsigned* dup;
-    unsigned long long rp, sp;        // payload bases of the shared frame
-};
-
-// Slot of a key offset: the MurmurHash3 32-bit finaliser, scaled into the
-// table by a 32 x 64-bit multiply-high.
-__device__ __forceinline__ unsigned long long l2j_slot(unsigned off, unsigned long long slots)
-{
-    off ^= off >> 16;
-    off *= 0x85ebca6bu;
-    off ^= off >> 13;
-    off *= 0xc2b2ae35u;
-    off ^= off >> 16;
-    return ((unsigned long long)off * slots) >> 32;
-}
-
-// The partition among [lo, hi) whose tile range holds tile t of the prefix.
-__device__ __forceinline__ int l2j_part(const unsigned long long* prefix, int lo, int hi, unsigned long long t)
-{
-    while (hi - lo > 1) {  // prefix[lo] <= t < prefix[hi]
-        const int mid = (lo + hi) >> 1;
-        if (prefix[mid] <= t) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
-__global__ void __launch_bounds__(L2J_THREADS, 2) rj_l2join_kernel(L2JoinArgs a)
-{
-    __shared__ unsigned long long item_cur;
-    uint64_t cnt = 0, bsum = 0, psum = 0;
-    bool dup = false;
-    const unsigned long long nitems = a.np + a.nb + a.nc;
-    const unsigned long long S_ = a.slots;
-    for (;;) {
-        if (threadIdx.x == 0) item_cur = atomicAdd(a.next, 1u);
-        __syncthreads();
-        const unsigned long long it = item_cur;
-        __syncthreads();  // every thread has read item_cur before it changes
-        if (it >= nitems) break;
-        if (it < a.np) {
-            // Probe a tile of S_c against table c (built by an earlier launch).
-            const unsigned long long t = a.ptile[a.pb] + it;
-            const int c = l2j_part(a.ptile, a.pb, a.pe, t);
-            const L2Part p = a.parts[c];
-            const unsigned long long w0 = (t - a.ptile[c]) * L2J_TILE;
-            const unsigned n = (unsigned)min((unsigned long long)L2J_TILE, p.scount - w0);
-            const unsigned long long* T =
-                a.tables + ((unsigned long long)a.pbuf * a.W + (unsigned)(c - a.pb)) * S_;
-            const unsigned long long* S = a.S + p.sstart + w0;
-            auto finish = [&](unsigned long long w, unsigned long long pos, unsigned long long e) {
-                const unsigned off = (unsigned)w;
-                for (unsigned long long steps = 0; steps < S_; ++steps) {
-                    if ((unsigned)e == off) {  // an empty slot's low half is never an offset
-                        cnt += 1;
-                        bsum += e >> 32;
-                        psum += w >> 32;
-                        return;
-                    }
-                    if (e == kEmptyWord) return;
-                    pos = pos + 1 == S_ ? 0 : pos + 1;
-                    e = __ldg(&T[pos]);
-                }
-            };
-            unsigned i = threadIdx.x;
-            for (; i + (L2J_U - 1) * L2J_THREADS < n; i += L2J_U * L2J_THREADS) {
-                unsigned long long w[L2J_U], pos[L2J_U], e[L2J_U];
-#pragma unroll
-                for (int u = 0; u < L2J_U; ++u) w[u] = __ldcs(&S[i + u * L2J_THREADS]);
-#pragma unroll
-                for (int u = 0; u < L2J_U; ++u) {
-                    pos[u] = l2j_slot((unsigned)w[u], S_);
-                    e[u] = __ldg(&T[pos[u]]);
-                }
-#pragma unroll
-                for (int u = 0; u < L2J_U; ++u) finish(w[u], pos[u], e[u]);
-            }
-            for (; i < n; i += L2J_THREADS) {
-                const unsigned long long w = __ldcs(&S[i]);
-                const unsigned long long pos = l2j_slot((unsigned)w, S_);
-                finish(w, pos, __ldg(&T[pos]));
-            }
-        } else if (it < a.np + a.nb) {
-            // Build: one 64-bit CAS per word; a table holds at most half
-            // its slots, so a free slot always exists.
-            const unsigned long long t = a.btile[a.bb] + (it - a.np);
-            const int c = l2j_part(a.btile, a.bb, a.be, t);
-            const L2Part p = a.parts[c];
-            const unsigned long long w0 = (t - a.btile[c]) * L2J_TILE;
-            const unsigned n = (unsigned)min((unsigned long long)L2J_TILE, p.rcount - w0);
-            unsigned long long* T = a.tables + ((unsigned long long)a.bbuf * a.W + (unsigned)(c - a.bb)) * S_;
-            const unsigned long long* R = a.R + p.rstart + w0;
-            for (unsigned i = threadIdx.x; i < n; i += L2J_THREADS) {
-                const unsigned long long w = R[i];
-                const unsigned off = (unsigned)w;
-                unsigned long long pos = l2j_slot(off, S_);
-                for (unsigned long long steps = 0; steps < S_; ++steps) {
-                    const unsigned long long prev = atomicCAS(&T[pos], kEmptyWord, w);
-                    if (prev == kEmptyWord) break;
-                    if ((unsigned)prev == off) {  // a repeated build key: the caller takes another path
-                        dup = true;
-                        break;
-                    }
-                    pos = pos + 1 == S_ ? 0 : pos + 1;
-                }
-            }
-        } else {
-            // Clear a chunk of the buffer the next launch builds into.
-            const unsigned long long c0 = (it - a.np - a.nb) * (unsigned long long)L2J_CLEAR;
-            ulonglong2* B = reinterpret_cast<ulonglong2*>(a.tables + (unsigned long long)a.cbuf * a.W * S_ + c0);
-            const unsigned long long end = min((unsigned long long)L2J_CLEAR, (unsigned long long)a.W * S_ - c0) / 2;
-            for (unsigned long long i = threadIdx.x; i < end; i += L2J_THREADS)
-                B[i] = make_ulonglong2(kEmptyWord, kEmptyWord);
-        }
-    }
-    uint64_t b = cnt * a.rp + bsum, q = cnt * a.sp + psum;
-    cnt = warp_sum_u64(cnt);
-    b = warp_sum_u64(b);
-    q = warp_sum_u64(q);
-    if ((threadIdx.x & 31) == 0 && (cnt | b | q)) {
-        atomicAdd(&a.acc[0], (unsigned long long)cnt);
-        atomicAdd(&a.acc[1], (unsigned long long)b);
-        atomicAdd(&a.acc[2], (unsigned long long)q);
     }
     if (__any_sync(0xffffffffu, dup) && (threadIdx.x & 31) == 0) atomicOr(a.dup, 1u);
 }
@@ -601,187 +443,14 @@ void* join_fn(bool rp, bool sp)
     return sp ? (void*)rj_join_kernel<UNIQUE, false, true> : (void*)rj_join_kernel<UNIQUE, false, false>;
 }
 
-// The L2-table join over single-pass packed partitions in one key frame
-// (rj_l2join_kernel).  *dup is set (and out left undefined) when a build
-// key repeats.
-int l2_join(pyg_ctx* ctx, const void* R1, const RJLayout& LR, const void* S1, const RJLayout& LS, int F,
-            unsigned long long out[3], bool* dup)
-{
-    *dup = false;
-    unsigned long long maxr = 1;
-    for (int c = 0; c < F; ++c) maxr = std::max(maxr, LR.count[c]);
-    const unsigned long long slots = (2 * maxr + 63) / 64 * 64;
-    const size_t table_bytes = slots * 8;
-    const int W = (int)std::max<size_t>(1, std::min<size_t>((size_t)F, L2J_BUDGET / (3 * table_bytes)));
-    const int nw = (F + W - 1) / W;
-    // Per partition: regions and counts; tile prefixes of both sides.
-    std::vector<L2Part> parts(F);
-    std::vector<unsigned long long> pre(2 * (F + 1));
-    unsigned long long* btile = pre.data();
-    unsigned long long* ptile = pre.data() + F + 1;
-    btile[0] = ptile[0] = 0;
-    for (int c = 0; c < F; ++c) {
-        parts[c].rstart = LR.fstart[c];
-        parts[c].rcount = LR.count[c];
-        parts[c].sstart = LS.fstart[c];
-        parts[c].scount = LS.count[c];
-        btile[c + 1] = btile[c] + (LR.count[c] + L2J_TILE - 1) / L2J_TILE;
-        ptile[c + 1] = ptile[c] + (LS.count[c] + L2J_TILE - 1) / L2J_TILE;
-    }
-    const size_t buf_words = (size_t)W * slots;
-    const size_t meta_bytes = parts.size() * sizeof(L2Part) + pre.size() * 8 + (size_t)(nw + 1) * 4;
-    // One arena: three table buffers, then the partition records, tile
-    // prefixes and one queue head per launch.
-    char* arena = nullptr;
-    int rc = dalloc(ctx, (void**)&arena, 3 * buf_words * 8 + meta_bytes);
-    if (rc) return rc;
-    unsigned long long* tables = (unsigned long long*)arena;
-    L2Part* dparts = (L2Part*)(arena + 3 * buf_words * 8);
-    unsigned long long* dpre = (unsigned long long*)(dparts + F);
-    unsigned* heads = (unsigned*)(dpre + pre.size());
-    unsigned long long* acc = ctx->dcounters + 8;
-    unsigned* dupf = (unsigned*)(ctx->dcounters + 201);
-    unsigned long long* h = (unsigned long long*)ctx->pinned;
-    auto cu_ok = [](cudaError_t e, const char* what) { return e == cudaSuccess ? PYG_OK : cuda_status(e, what); };
-    do {
-        if ((rc = cu_ok(cudaMemcpyAsync(dparts, parts.data(), parts.size() * sizeof(L2Part),
-                                              cudaMemcpyHostToDevice, ctx->stream), "l2 join parts"))) break;
-        if ((rc = cu_ok(cudaMemcpyAsync(dpre, pre.data(), pre.size() * 8, cudaMemcpyHostToDevice, ctx->stream),
-                              "l2 join prefixes"))) break;
-        if ((rc = cu_ok(cudaMemsetAsync(heads, 0, (size_t)(nw + 1) * 4, ctx->stream), "l2 join heads"))) break;
-        if ((rc = cu_ok(cudaMemsetAsync(acc, 0, 3 * 8, ctx->stream), "l2 join acc"))) break;
-        if ((rc = cu_ok(cudaMemsetAsync(dupf, 0, 4, ctx->stream), "l2 join dup"))) break;
-        // Buffer 0 (wave 0's tables) starts empty; every later buffer is
-        // cleared by the launch before the one that builds into it.
-        if ((rc = cu_ok(cudaMemsetAsync(tables, 0xFF, buf_words * 8, ctx->stream), "l2 join clear"))) break;
-        L2JoinArgs a;
-        a.R = (const unsigned long long*)R1;
-        a.S = (const unsigned long long*)S1;
-        a.tables = tables;
-        a.slots = slots;
-        a.parts = dparts;
-        a.btile = dpre;
-        a.ptile = dpre + F + 1;
-        a.W = W;
-        a.acc = acc;
-        a.dup = dupf;
-        a.rp = LR.pbase;
-        a.sp = LS.pbase;
-        const unsigned grid = (unsigned)ctx->sm_count * 2;
-        for (int k = 0; k <= nw && !rc; ++k) {
-            a.pb = std::max(0, (k - 1) * W);
-            a.pe = k >= 1 ? std::min(F, k * W) : a.pb;
-            a.pbuf = (k + 2) % 3;  // (k - 1) mod 3
-            a.bb = std::min(F, k * W);
-            a.be = k < nw ? std::min(F, (k + 1) * W) : a.bb;
-            a.bbuf = k % 3;
-            a.cbuf = k + 1 < nw ? (k + 1) % 3 : -1;
-            a.np = ptile[a.pe] - ptile[a.pb];
-            a.nb = btile[a.be] - btile[a.bb];
-            a.nc = a.cbuf >= 0 ? (buf_words + L2J_CLEAR - 1) / L2J_CLEAR : 0;
-            a.next = heads + k;
-            if (a.np + a.nb + a.nc == 0) continue;
-            rj_l2join_kernel<<<grid, L2J_THREADS, 0, ctx->stream>>>(a);
-            rc = cu_ok(cudaGetLastError(), "rj_l2join_kernel");
-            ctx->launches++;
-        }
-        if (rc) break;
-        if ((rc = cu_ok(cudaMemcpyAsync(h, acc, 3 * 8, cudaMemcpyDeviceToHost, ctx->stream), "l2 join result")))
-            break;
-        if ((rc = cu_ok(cudaMemcpyAsync(h + 3, dupf, 4, cudaMemcpyDeviceToHost, ctx->stream), "l2 join dup")))
-            break;
-        if ((rc = cu_ok(cudaStreamSynchronize(ctx->stream), "l2 join"))) break;
-        out[0] = h[0];
-        out[1] = h[1];
-        out[2] = h[2];
-        *dup = (unsigned)h[3] != 0;
-    } while (0);
-    dfree(ctx, arena);
-    return rc;
-}
-
 }  // namespace
 
-// One packed partition pass per relation into 2^FB partitions sharing a key
-// frame, then the L2-table join.  *fallback: the inputs need the two-level
-// path instead (no shared packed frame, or a repeated build key).
-static int l2_radix_join(pyg_ctx* ctx, const longlong2* R, int64_t nR, const longlong2* S, int64_t nS,
-                         unsigned long long out[3], pyg_join_stats* stats, bool* fallback)
-{
-    *fallback = false;
-    // Partitions whose tables (8-byte slots, load factor 0.5) are about
-    // 4 MB: 2^18 build tuples each.
-    int FB = 1;
-    while (FB < RJ_MAX_LOCAL_BITS && ((unsigned long long)nR >> FB) > (1ull << 18)) ++FB;
-    const int F = 1 << FB;
-    RJEvents tm;
-    tm.start(ctx, stats != nullptr);
-    int rc = PYG_OK;
-    RPSide side[2];
-    do {
-        unsigned* flags = (unsigned*)(ctx->dcounters + 224);
-        unsigned* hflags = (unsigned*)((unsigned long long*)ctx->pinned + 6);
-        for (int s = 0; s < 2; ++s) {
-            side[s].in = s ? S : R;
-            side[s].n = s ? nS : nR;
-            side[s].allow_pack = true;
-            side[s].begin = tm.on ? tm.ev[5 + 2 * s] : nullptr;
-            side[s].done = tm.on ? tm.ev[2 + s] : nullptr;
-        }
-        if ((rc = rp_partition_sides(ctx, side, 2, FB, false, flags, hflags, tm.on ? tm.ev[1] : nullptr, true))) break;
-        const RJLayout& LR = side[0].L;
-        const RJLayout& LS = side[1].L;
-        if (!(LR.packed && LS.packed && LR.kbase == LS.kbase)) {
-            *fallback = true;
-            break;
-        }
-        bool dup = false;
-        if ((rc = l2_join(ctx, side[0].P1, LR, side[1].P1, LS, F, out, &dup))) break;
-        if (dup) {
-            *fallback = true;
-            break;
-        }
-        tm.mark(ctx, 4);
-        if (stats) {
-            cudaEventSynchronize(tm.ev[4]);
-            stats->algorithm = PYG_JOIN_RADIX_L2;
-            stats->radix_bits = FB;
-            stats->histogram_ms = tm.ms(0, 1);
-            stats->histogram_tuples = side[0].hist_tuples + side[1].hist_tuples;
-            stats->build_partition_ms = tm.ms(1, 2);
-            stats->build_ms = 0;
-            stats->probe_partition_ms = tm.ms(2, 3);
-            stats->probe_ms = tm.ms(3, 4);
-            for (int s = 0; s < 2; ++s) {
-                double* pm = s ? stats->probe_pass_ms : stats->build_pass_ms;
-                pm[0] = side[s].begin ? tm.ms(5 + 2 * s, 2 + s) : 0;
-                pm[1] = 0;
-            }
-            stats->build_packed = 1;
-            stats->probe_packed = 1;
-            stats->padded_tuples = (int64_t)((LR.p2 + LS.p2) - (unsigned long long)(nR + nS));
-            stats->overflow_tuples = (side[0].overflowed ? 1 : 0) + (side[1].overflowed ? 1 : 0);
-        }
-    } while (0);
-    for (int s = 0; s < 2; ++s) {
-        dfree(ctx, side[s].P1);
-        dfree(ctx, side[s].P2);
-    }
-    return rc;
-}
-
-int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t nS, int fine_bits, bool l2,
+int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t nS, int fine_bits,
                  unsigned long long out[3], pyg_join_stats* stats)
 {
     const longlong2* R = (const longlong2*)Rv;
     const longlong2* S = (const longlong2*)Sv;
     out[0] = out[1] = out[2] = 0;
-    if (l2 && nR > 0 && nS > 0) {
-        bool fallback = false;
-        int rc = l2_radix_join(ctx, R, nR, S, nS, out, stats, &fallback);
-        if (rc || !fallback) return rc;
-        out[0] = out[1] = out[2] = 0;
-    }
     if (fine_bits <= 0) {
         // Partitions of about 0.7 x the table's build capacity.
         fine_bits = 1;

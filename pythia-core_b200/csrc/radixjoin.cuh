@@ -9,14 +9,15 @@ struct pyg_ctx;
 
 namespace pyg {
 
+
+
+
+
 // Joins 16-byte (int64 key, int64 payload) device relations R and S on the
 // key and returns out = {match count, wrapped sum of R payloads, wrapped sum
 // of S payloads} over the joined pairs.  fine_bits <= 0 picks the partition
-// count from |R|.  l2: one packed partition pass per relation and
-// L2-resident partition tables (falls back to the two-level path when the
-// relations share no packed key frame or a build key repeats).  Fills the
-// timing fields of stats when it is not null.
-int radix_join16(pyg_ctx* ctx, const void* R, int64_t nR, const void* S, int64_t nS, int fine_bits, bool l2,
+// count from |R|.  Fills the timing fields of stats when it is not null.
+int radix_join16(pyg_ctx* ctx, const void* R, int64_t nR, const void* S, int64_t nS, int fine_bits,
                  unsigned long long out[3], pyg_join_stats* stats);
 
 }  // namespace pyg

@@ -156,7 +156,7 @@ def case_batch(torch, ctx, a):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["radix", "radix-l2", "direct", "groupby16", "composite", "partition", "sort", "mpsm",
+    ap.add_argument("case", choices=["radix", "direct", "groupby16", "composite", "partition", "sort", "mpsm",
                                      "mpsm-mat", "cdf", "batch"])
     ap.add_argument("--shift", type=int, default=0, help="shrink the inputs by 2^shift")
     ap.add_argument("--reps", type=int, default=2)
@@ -170,8 +170,6 @@ def main():
     try:
         if a.case == "radix":
             case_join(torch, ctx, a, pyg.JOIN_RADIX, (1 << 24) >> a.shift, (1 << 27) >> a.shift)
-        elif a.case == "radix-l2":
-            case_join(torch, ctx, a, pyg.JOIN_RADIX_L2, (1 << 24) >> a.shift, (1 << 27) >> a.shift)
         elif a.case == "direct":
             case_join(torch, ctx, a, pyg.JOIN_DIRECT, (1 << 20) >> a.shift, (1 << 24) >> a.shift)
         elif a.case == "groupby16":

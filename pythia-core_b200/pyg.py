@@ -42,7 +42,6 @@ SPLIT_HASH = 3
 JOIN_AUTO = 0
 JOIN_DIRECT = 1
 JOIN_RADIX = 2
-JOIN_RADIX_L2 = 3
 
 # Largest build side of pyg_hashjoin_agg_noalloc (PYG_NOALLOC_MAX_BUILD).
 NOALLOC_MAX_BUILD = 1 << 18

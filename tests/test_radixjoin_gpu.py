@@ -256,71 +256,3 @@ def test_host_probe_streams_in_chunks(ctx, torch_cuda):
     S = struct([rng.integers(0, n + 100, m), rng.integers(0, 1 << 20, m)], [I64, I64])
     got = ctx.hashjoin_agg(host_rel(R, [I64, I64]), [0], host_rel(S, [I64, I64]), [0], PROJ, pyg.JOIN_AUTO)
     assert got == O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ, buckets=n)
-
-
-@pytest.mark.parametrize("theta", [0.0, 1.25])
-def test_radix_l2_equals_oracle(ctx, torch_cuda, theta):
-    """One partition pass per side and L2-resident partition tables
-    (JOIN_RADIX_L2): the same count and sums as the oracle, a few probe keys
-    missing from the build side."""
-    rng = np.random.default_rng(int(theta * 100) + 77)
-    n, m = 1 << 17, 1 << 21
-    k = rng.permutation(n).astype(np.int64) * 3 - 1000
-    R = struct([k, rng.integers(-(1 << 60), 1 << 60, n)], [I64, I64])
-    fk = zipf_keys(rng, m, k, theta) + (rng.random(m) < 0.05)
-    S = struct([fk, rng.integers(-(1 << 60), 1 << 60, m)], [I64, I64])
-    want = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ)
-    Rd, Sd = dev_rel(torch_cuda, R, [I64, I64]), dev_rel(torch_cuda, S, [I64, I64])
-    for proj in (PROJ, [(1, 1), (0, 1)], [(1, 1)], [(0, 1)]):
-        want = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], proj)
-        got, st = ctx.hashjoin_agg(Rd, [0], Sd, [0], proj, pyg.JOIN_RADIX_L2, 0, stats=True)
-        assert st.algorithm == pyg.JOIN_RADIX_L2 and st.build_packed == 1 and st.probe_packed == 1
-        assert got == want
-
-
-@pytest.mark.parametrize("theta", [0.0, 1.25])
-def test_radix_l2_many_waves(ctx, torch_cuda, theta):
-    """2^23 build tuples: 32 partitions of 4 MB tables, more waves than the
-    three rotating table buffers, so buffers are cleared and reused.  PK-FK:
-    count = |S| and sums in closed form."""
-    rng = np.random.default_rng(5 + int(theta))
-    n, m = 1 << 23, 1 << 24
-    k = rng.permutation(n).astype(np.int64) + 1
-    rp = rng.integers(0, 1 << 36, n)
-    idx = zipf_keys(rng, m, np.arange(n), theta)
-    sp = rng.integers(0, 1 << 36, m)
-    R = struct([k, rp], [I64, I64])
-    S = struct([k[idx], sp], [I64, I64])
-    got, st = ctx.hashjoin_agg(dev_rel(torch_cuda, R, [I64, I64]), [0], dev_rel(torch_cuda, S, [I64, I64]), [0], PROJ,
-                               pyg.JOIN_RADIX_L2, 0, stats=True)
-    assert st.algorithm == pyg.JOIN_RADIX_L2 and st.radix_bits == 5
-    assert got == (m, [int(rp[idx].sum()), int(sp.sum())])
-
-
-@pytest.mark.parametrize("case", ["repeated_build_keys", "wide_key_range"])
-def test_radix_l2_falls_back(ctx, torch_cuda, case):
-    """A repeated build key, or keys too far apart for one 32-bit packed
-    frame: the two-level radix path answers instead, with the same result."""
-    rng = np.random.default_rng(3)
-    n, m = 1 << 18, 1 << 21
-    if case == "repeated_build_keys":
-        k = rng.integers(0, 1 << 16, n)
-        fk = rng.integers(0, (1 << 16) + 500, m)
-    else:
-        k = rng.permutation(n).astype(np.int64) * (1 << 20)
-        fk = k[rng.integers(0, n, m)]
-    R = struct([k, rng.integers(-(1 << 50), 1 << 50, n)], [I64, I64])
-    S = struct([fk, rng.integers(-(1 << 50), 1 << 50, m)], [I64, I64])
-    want = O.hashjoin_agg(R, [I64, I64], [0], S, [I64, I64], [0], PROJ)
-    got, st = ctx.hashjoin_agg(dev_rel(torch_cuda, R, [I64, I64]), [0], dev_rel(torch_cuda, S, [I64, I64]), [0], PROJ,
-                               pyg.JOIN_RADIX_L2, 0, stats=True)
-    assert st.algorithm == pyg.JOIN_RADIX and got == want
-
-
-def test_radix_l2_empty_sides(ctx, torch_cuda):
-    R = struct([np.arange(100, dtype=np.int64)] * 2, [I64, I64])
-    E = R[:0]
-    for a, b in ((R, E), (E, R), (E, E)):
-        got = ctx.hashjoin_agg(dev_rel(torch_cuda, a, [I64, I64]), [0], dev_rel(torch_cuda, b, [I64, I64]), [0], PROJ,
-                               pyg.JOIN_RADIX_L2, 0)
-        assert got == (0, [0, 0])
