@@ -50,10 +50,11 @@ struct BatchState {
 
 constexpr int RES_WORDS = 6;  // count, sum, then empty-marker key stats: build count/sum, probe count/sum
 constexpr long long kWaitLimit = 1LL << 22;  // x ~256 ns sleeps, about one second
-// Build tuples from which a fragment runs as its own partitioned join by
-// default: its table (32 MB and more at load factor 0.5) would crowd the
-// other fragments' tables out of L2.
-constexpr int64_t kLargeBuild = (int64_t)1 << 20;
+// Build tuples from which a fragment runs as its own join by default.  On
+// a mix of 256 fragments with builds of 2^12..2^22 tuples, sending builds of
+// 2^16 and more to their own calls measured fastest (58.4 ms against 61.0
+// ms at 2^14 and 61.4-80.7 ms at 2^20 and above).
+constexpr int64_t kLargeBuild = (int64_t)1 << 16;
 
 struct BatchDev {
     const FragDesc* frags;
@@ -277,8 +278,8 @@ static pyg_tuning default_tuning()
     pyg_tuning t;
     t.block_threads = 512;
     t.blocks_per_sm = 2;
-    t.load_factor = 0.7f;  // 16-byte slots: a 2^22-tuple build's table (96 MB) stays in L2
-    t.chunk_tuples = 16384;
+    t.load_factor = 0.5f;
+    t.chunk_tuples = 4096;
     t.large_build = 0;
     return t;
 }
@@ -621,71 +622,65 @@ int pyg_autotune(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const char*
             }
         }
     }
-    // Candidate grid of the persistent kernel (block shape x occupancy x
-    // load factor x grain), timed on the graph alone; then the size from
-    // which fragments run as their own joins, timed on whole runs.
-    const int bts[] = {256, 512, 1024};
-    const int bps[] = {1, 2, 4};
-    const float lfs[] = {0.5f, 0.7f};
-    const int chunks[] = {16384, 65536};
-    float best = 1e30f;
-    pyg_tuning best_t = default_tuning();
+    // First the size from which fragments run as their own joins, timed on
+    // whole runs with the default kernel shape; then the persistent
+    // kernel's candidate grid (block shape x occupancy x load factor x
+    // grain) for the fragments that stay queued, timed on the graph alone.
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (int bt : bts)
-        for (int bp : bps) {
-            if (bt * bp > 2048) continue;
-            for (float lf : lfs)
-                for (int ch : chunks) {
-                    pyg_tuning t = {bt, bp, lf, ch, 0};
-                    pyg_batch* b = nullptr;
-                    if (pyg_batch_create(ctx, frags, n, &t, &b)) continue;
-                    float ms = 1e30f;
-                    bool good = pyg_batch_run(ctx, b, nullptr, nullptr, nullptr) == PYG_OK;
-                    for (int rep = 0; rep < 3 && good; ++rep) {
-                        cudaEventRecord(e0, ctx->stream);
-                        cudaGraphLaunch(b->exec, ctx->stream);
-                        cudaEventRecord(e1, ctx->stream);
-                        cudaEventSynchronize(e1);
-                        float x = 0;
-                        cudaEventElapsedTime(&x, e0, e1);
-                        ms = std::min(ms, x);
-                    }
-                    pyg_batch_free(ctx, b);
-                    if (good && ms < best) {
-                        best = ms;
-                        best_t = t;
-                    }
-                }
+    auto time_tuning = [&](const pyg_tuning& t, bool whole, int reps) -> float {
+        pyg_batch* b = nullptr;
+        if (pyg_batch_create(ctx, frags, n, &t, &b)) return 1e30f;
+        float ms = 1e30f;
+        bool good = pyg_batch_run(ctx, b, nullptr, nullptr, nullptr) == PYG_OK;
+        for (int rep = 0; rep < reps && good; ++rep) {
+            cudaEventRecord(e0, ctx->stream);
+            if (whole) good = pyg_batch_run(ctx, b, nullptr, nullptr, nullptr) == PYG_OK;
+            else cudaGraphLaunch(b->exec, ctx->stream);
+            cudaEventRecord(e1, ctx->stream);
+            cudaEventSynchronize(e1);
+            float x = 0;
+            cudaEventElapsedTime(&x, e0, e1);
+            ms = std::min(ms, x);
         }
+        pyg_batch_free(ctx, b);
+        return good ? ms : 1e30f;
+    };
+    pyg_tuning best_t = default_tuning();
+    float best = 1e30f;
     {
-        const int32_t larges[] = {1 << 18, 1 << 20, 1 << 22};
-        pyg_tuning base = best_t;
-        best = 1e30f;
+        const int32_t larges[] = {1 << 14, 1 << 16, 1 << 18, 1 << 20};
+        const pyg_tuning base = best_t;
         for (int32_t lb : larges) {
             pyg_tuning t = base;
             t.large_build = lb;
-            pyg_batch* b = nullptr;
-            if (pyg_batch_create(ctx, frags, n, &t, &b)) continue;
-            float ms = 1e30f;
-            bool good = pyg_batch_run(ctx, b, nullptr, nullptr, nullptr) == PYG_OK;
-            for (int rep = 0; rep < 2 && good; ++rep) {
-                cudaEventRecord(e0, ctx->stream);
-                good = pyg_batch_run(ctx, b, nullptr, nullptr, nullptr) == PYG_OK;
-                cudaEventRecord(e1, ctx->stream);
-                cudaEventSynchronize(e1);
-                float x = 0;
-                cudaEventElapsedTime(&x, e0, e1);
-                ms = std::min(ms, x);
-            }
-            pyg_batch_free(ctx, b);
-            if (good && ms < best) {
+            const float ms = time_tuning(t, true, 2);
+            if (ms < best) {
                 best = ms;
                 best_t = t;
             }
         }
     }
+    const int bts[] = {256, 512, 1024};
+    const int bps[] = {1, 2, 4};
+    const float lfs[] = {0.5f, 0.7f};
+    const int chunks[] = {4096, 16384, 65536};
+    const int32_t lb = best_t.large_build;
+    best = 1e30f;
+    for (int bt : bts)
+        for (int bp : bps) {
+            if (bt * bp > 2048) continue;
+            for (float lf : lfs)
+                for (int ch : chunks) {
+                    const pyg_tuning t = {bt, bp, lf, ch, lb};
+                    const float ms = time_tuning(t, false, 3);
+                    if (ms < best) {
+                        best = ms;
+                        best_t = t;
+                    }
+                }
+        }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     {

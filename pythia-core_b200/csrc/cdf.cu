@@ -475,8 +475,7 @@ static int cdf_assign(pyg_ctx* ctx, CdfWork& w, const int64_t* keys, int64_t n, 
     PYG_LAUNCHED(ctx);
     leaf_range_kernel<<<grid_for(ctx, L, 256, 1, 4), 256, 0, ctx->stream>>>(w.st, n, L, d_yr, w.gscale);
     PYG_LAUNCHED(ctx);
-    PYG_CUDA(cudaStreamSynchronize(ctx->stream));  // keeps `init` alive until the copy ran
-    return PYG_OK;
+    return PYG_OK;  // `init` was staged by the (pageable) copy before it returned
 }
 
 // Packed key words of every step-th tuple (m of them).
@@ -537,8 +536,6 @@ int pyg_cdf_train(pyg_ctx* ctx, const int64_t* sample_keys, int64_t n, const pyg
     m->n_sample = n;
     CdfWork w;
     float* adam = nullptr;  // m and v for 2 + 2L params
-    int64_t ends[2];
-    unsigned long long* hs = (unsigned long long*)ctx->pinned + 128;
     std::vector<long long> run_start, run_end;  // heavy runs in the sorted sample
     int64_t* cont = nullptr;                    // the sample without its heavy runs
     const int64_t* fit = sorted;                // what the root and leaves are fitted to
@@ -548,41 +545,41 @@ int pyg_cdf_train(pyg_ctx* ctx, const int64_t* sample_keys, int64_t n, const pyg
         if ((rc = dalloc(ctx, (void**)&m->d_params, (size_t)(2 + 2 * L) * 4))) break;
         if ((rc = dalloc(ctx, (void**)&m->d_yr, (size_t)2 * L * 8))) break;
         if ((rc = dalloc(ctx, (void**)&adam, (size_t)2 * (2 + 2 * L) * 4))) break;
-        PYG_CUDA(cudaMemcpyAsync(ends, sorted, 8, cudaMemcpyDeviceToHost, ctx->stream));
-        PYG_CUDA(cudaMemcpyAsync(ends + 1, sorted + n - 1, 8, cudaMemcpyDeviceToHost, ctx->stream));
-        unsigned long long* dstat = ctx->dcounters + 80;
-        PYG_CUDA(cudaMemsetAsync(dstat, 0, 16, ctx->stream));
+        // Sample statistics and heavy runs in one round trip: the end keys,
+        // distinct / singleton counts, and up to `cap` heavy runs (start,
+        // key, end) land in the pinned staging area together.
+        const int cap = 4096;
+        const int64_t thr = n / 4096 > 2 ? n / 4096 : 2;
+        unsigned long long* dstat = ctx->dcounters + 80;  // [0..1] run stats, [2] heavy-run count
+        longlong2* runs;
+        long long* rend;
+        if ((rc = dalloc(ctx, (void**)&runs, (size_t)cap * 24))) break;
+        rend = (long long*)(runs + cap);
+        PYG_CUDA(cudaMemsetAsync(dstat, 0, 24, ctx->stream));
         run_stats_kernel<<<grid_for(ctx, n, 256, 4, 8), 256, 0, ctx->stream>>>(sorted, n, dstat);
         PYG_LAUNCHED(ctx);
-        PYG_CUDA(cudaMemcpyAsync(hs, dstat, 16, cudaMemcpyDeviceToHost, ctx->stream));
+        heavy_runs_kernel<<<grid_for(ctx, n, 256, 4, 8), 256, 0, ctx->stream>>>(sorted, n, thr, runs, rend, dstat + 2,
+                                                                              cap);
+        PYG_LAUNCHED(ctx);
+        unsigned char* stage = (unsigned char*)ctx->pinned + kPinnedScalarBytes;
+        int64_t* hends = (int64_t*)stage;
+        unsigned long long* hst = (unsigned long long*)(stage + 16);
+        longlong2* hruns = (longlong2*)(stage + 64);
+        long long* hrend = (long long*)(hruns + cap);
+        PYG_CUDA(cudaMemcpyAsync(hends, sorted, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(hends + 1, sorted + n - 1, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(hst, dstat, 24, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(hruns, runs, (size_t)cap * 24, cudaMemcpyDeviceToHost, ctx->stream));
         PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-        m->kmin = ends[0];
-        m->kmax = ends[1];
-        m->distinct = (int64_t)hs[0];
-        m->f1 = (int64_t)hs[1];
+        dfree(ctx, runs);
+        m->kmin = hends[0];
+        m->kmax = hends[1];
+        m->distinct = (int64_t)hst[0];
+        m->f1 = (int64_t)hst[1];
         {
-            const int cap = 4096;
-            int64_t thr = n / 4096 > 2 ? n / 4096 : 2;
-            longlong2* runs;
-            long long* rend;
-            if ((rc = dalloc(ctx, (void**)&runs, (size_t)cap * 16))) break;
-            if ((rc = dalloc(ctx, (void**)&rend, (size_t)cap * 8))) {
-                dfree(ctx, runs);
-                break;
-            }
-            PYG_CUDA(cudaMemsetAsync(dstat, 0, 8, ctx->stream));
-            heavy_runs_kernel<<<grid_for(ctx, n, 256, 4, 8), 256, 0, ctx->stream>>>(sorted, n, thr, runs, rend, dstat, cap);
-            PYG_LAUNCHED(ctx);
-            PYG_CUDA(cudaMemcpyAsync(hs, dstat, 8, cudaMemcpyDeviceToHost, ctx->stream));
-            PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-            int nh = (int)std::min<unsigned long long>(hs[0], (unsigned long long)cap);
-            std::vector<longlong2> hr(nh);
-            std::vector<long long> he(nh);
-            PYG_CUDA(cudaMemcpyAsync(hr.data(), runs, (size_t)nh * 16, cudaMemcpyDeviceToHost, ctx->stream));
-            PYG_CUDA(cudaMemcpyAsync(he.data(), rend, (size_t)nh * 8, cudaMemcpyDeviceToHost, ctx->stream));
-            PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-            dfree(ctx, runs);
-            dfree(ctx, rend);
+            const int nh = (int)std::min<unsigned long long>(hst[2], (unsigned long long)cap);
+            std::vector<longlong2> hr(hruns, hruns + nh);
+            std::vector<long long> he(hrend, hrend + nh);
             std::vector<int> ord(nh);
             for (int i = 0; i < nh; ++i) ord[i] = i;
             std::sort(ord.begin(), ord.end(), [&](int a, int b) { return hr[a].x < hr[b].x; });
@@ -620,7 +617,8 @@ int pyg_cdf_train(pyg_ctx* ctx, const int64_t* sample_keys, int64_t n, const pyg
             drop_runs_kernel<<<grid_for(ctx, n, 256, 4, 8), 256, 0, ctx->stream>>>(sorted, n, runs, runs + nh,
                                                                                    runs + 2 * nh, nh, cont);
             PYG_LAUNCHED(ctx);
-            PYG_CUDA(cudaStreamSynchronize(ctx->stream));  // keeps the host vectors alive until the copies ran
+            // Copies from pageable host memory are staged before the calls
+            // return, so the host vectors may go; runs is freed in stream order.
             dfree(ctx, runs);
             fit = cont;
             nfit = n - heavy_n;
