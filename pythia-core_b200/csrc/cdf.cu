@@ -746,15 +746,33 @@ static double cdf_continuous(const pyg_cdf* m, int64_t k)
 // The key at which C reaches c: the leaf whose target range holds c, its
 // line inverted to a leaf coordinate, the root line inverted to a key;
 // `past` (one past the largest sample key) when c is beyond the model.
-static int64_t cdf_invert(const pyg_cdf* m, const std::vector<int>& ne, double c, int64_t past)
+// `hint` is the leaf position found for the previous, smaller c: the
+// splitters ask for increasing c, so the search mostly steps forward.
+static int64_t cdf_invert(const pyg_cdf* m, const std::vector<int>& ne, double c, int64_t past, size_t* hint)
 {
     if (ne.empty() || m->key_scale == 0) return past;
-    size_t lo = 0, hi = ne.size();
-    while (lo + 1 < hi) {
-        const size_t mid = (lo + hi) / 2;
-        if (m->ylo[ne[mid]] <= c) lo = mid;
-        else hi = mid;
+    size_t lo = *hint < ne.size() ? *hint : 0;
+    if (m->ylo[ne[lo]] <= c) {
+        size_t step = 0;
+        while (lo + 1 < ne.size() && m->ylo[ne[lo + 1]] <= c && ++step < 64) ++lo;
+        if (lo + 1 < ne.size() && m->ylo[ne[lo + 1]] <= c) {  // far ahead: search the rest
+            size_t hi = ne.size();
+            while (lo + 1 < hi) {
+                const size_t mid = (lo + hi) / 2;
+                if (m->ylo[ne[mid]] <= c) lo = mid;
+                else hi = mid;
+            }
+        }
+    } else {
+        size_t hi = lo;
+        lo = 0;
+        while (lo + 1 < hi) {
+            const size_t mid = (lo + hi) / 2;
+            if (m->ylo[ne[mid]] <= c) lo = mid;
+            else hi = mid;
+        }
     }
+    *hint = lo;
     const int l = ne[lo];
     const double t = (c - m->ylo[l]) / (m->yhi[l] - m->ylo[l]);
     const double a = m->la[l], b = m->lb[l];
@@ -798,6 +816,7 @@ int pyg_cdf_splitters(pyg_ctx* ctx, const pyg_cdf* m, int32_t fanout, int64_t* o
     }
     std::vector<int> inside(fanout, -1);  // splitter j (1-based) falls in heavy key h's span
     int64_t prev = m->kmin;
+    size_t hint = 0;
     for (int j = 1; j < fanout; ++j) {
         const double q = (double)j / (double)fanout;
         // First heavy key whose span ends after q.
@@ -815,7 +834,7 @@ int pyg_cdf_splitters(pyg_ctx* ctx, const pyg_cdf* m, int32_t fanout, int64_t* o
             // In the continuous part between heavy keys a - 1 and a.
             const double below = a < H ? m->heavy_before[a] : W;
             const double c = cont > 1e-12 ? (q - below) / cont : 0.0;
-            key = cdf_invert(m, ne, c, past);
+            key = cdf_invert(m, ne, c, past, &hint);
             if (a > 0) key = std::max(key, m->heavy_key[a - 1] == INT64_MAX ? INT64_MAX : m->heavy_key[a - 1] + 1);
             if (a < H) key = std::min(key, m->heavy_key[a]);
         }

@@ -495,7 +495,7 @@ static int mpsm_run(pyg_ctx* ctx, const pyg_rel* build, int32_t bkey, const pyg_
             if (stride < 1) stride = 1;
             // The learned model needs far fewer samples than quantile
             // splitters (which want tens of samples per range): its leaves
-            // are fitted lines, so at most CDF_MPSM_SAMPLE keys (about 256
+            // are fitted lines, so at most CDF_MPSM_SAMPLE keys (about 64
             // per leaf) are drawn for it.
             if (o->splitter_kind == PYG_MPSM_SPLIT_LEARNED && nS / stride > CDF_MPSM_SAMPLE)
                 stride = (nS + CDF_MPSM_SAMPLE - 1) / CDF_MPSM_SAMPLE;
@@ -514,8 +514,8 @@ static int mpsm_run(pyg_ctx* ctx, const pyg_rel* build, int32_t bkey, const pyg_
             } else {
                 pyg_cdf_train_opts to;
                 to.leaves = o->cdf_leaves > 0 ? o->cdf_leaves : 1024;
-                // Least-squares start, then a short fine-tuning of the leaves.
-                to.epochs = 4;
+                // Least-squares start, then one fine-tuning epoch of the leaves.
+                to.epochs = 1;
                 to.lr = 0.002f;
                 to.seed = o->seed;
                 pyg_cdf* model = nullptr;

@@ -7,11 +7,17 @@
 //   2. partition   both relations range-partitioned by those splitters with
 //                  the radix operators' bulk-copy partitioner (radixpart.cu,
 //                  splitter-search bins; two passes above 2^8 ranges).
-//   3. sort+merge  persistent CTAs take (range, build chunk of <= 4096,
-//                  probe chunk) items: the build chunk is bitonic-sorted in
-//                  shared memory with a prefix sum of its payloads, and every
-//                  probe tuple is merged into the sorted run by a lower-bound
-//                  search, adding the count and payload sums of its key's run.
+//   3. sort+merge  persistent CTAs take (range, build chunk, probe chunk)
+//                  items.  A range whose splitters bound it to at most
+//                  MP16_DSPAN key values is sorted by counting: the build
+//                  chunk (the whole range) is binned by key offset in shared
+//                  memory, each bin holding its key's count and payload sum,
+//                  and a probe tuple finds its key's run at its offset.  Any
+//                  other range is sorted in chunks of <= 4096 by a bitonic
+//                  network with a prefix sum of the payloads, and each probe
+//                  tuple is merged into the run by a lower-bound search.
+//                  Either way a probe tuple adds its key's run's count and
+//                  payload sum.
 // Build keys equal to INT64_MAX (the sort's padding value) are counted on
 // the side per item, as are the probe tuples that match them.
 #include <cuda_runtime.h>
@@ -31,10 +37,17 @@ constexpr int MP16_RCHUNK = 4096;         // build tuples sorted per work item
 constexpr int64_t MP16_SCHUNK = 1 << 16;  // probe tuples per work item
 constexpr int MP16_SMEM = MP16_RCHUNK * 8 * 2 + (MP16_RCHUNK + 1) * 8;
 constexpr long long kPadKey = 0x7FFFFFFFFFFFFFFFLL;
+// Largest key span of a range sorted by counting: 4-byte counts and 8-byte
+// sums per key value, 96 KB, inside the bitonic path's shared memory.
+constexpr unsigned MP16_DSPAN = 8192;
+static_assert(MP16_DSPAN * 12 <= MP16_SMEM, "counting bins fit the sort's shared memory");
 
 struct Mp16Item {
     unsigned long long r0, s0;
     unsigned rn, sn;
+    long long lo;   // counting sort: the range's first key value
+    unsigned span;  // its number of key values (0: bitonic sort)
+    unsigned pad;
 };
 
 struct Mp16Args {
@@ -44,6 +57,7 @@ struct Mp16Args {
     long long nitems;
     unsigned* next;
     unsigned long long* acc;  // count, build sum, probe sum
+    unsigned* bad;            // a key outside its range's span (never set by a correct partition)
 };
 
 __global__ void __launch_bounds__(MP16_THREADS, 2) mp16_join_kernel(Mp16Args a)
@@ -66,6 +80,53 @@ __global__ void __launch_bounds__(MP16_THREADS, 2) mp16_join_kernel(Mp16Args a)
         const long long it = item;
         if (it >= a.nitems) break;
         const Mp16Item m = a.items[it];
+        if (m.span) {
+            // Counting sort of the whole range by key offset: bin o holds
+            // the count and payload sum of key lo + o.
+            unsigned* bc = (unsigned*)mp16_smem;
+            unsigned long long* bs = (unsigned long long*)(mp16_smem + MP16_DSPAN * 4);
+            for (unsigned i = tid; i < m.span; i += MP16_THREADS) {
+                bc[i] = 0;
+                bs[i] = 0;
+            }
+            __syncthreads();
+            bool out_of_span = false;
+            for (unsigned i = tid; i < m.rn; i += MP16_THREADS) {
+                const longlong2 t = a.R[m.r0 + i];
+                const unsigned long long o = (unsigned long long)t.x - (unsigned long long)m.lo;
+                if (o < m.span) {
+                    atomicAdd(&bc[o], 1u);
+                    atomicAdd(&bs[o], (unsigned long long)t.y);
+                } else {
+                    out_of_span = true;
+                }
+            }
+            if (out_of_span) atomicOr(a.bad, 1u);
+            __syncthreads();
+            const longlong2* S = a.S + m.s0;
+            auto probe_bin = [&](const longlong2 t) {
+                const unsigned long long o = (unsigned long long)t.x - (unsigned long long)m.lo;
+                if (o >= m.span) return;
+                const unsigned c = bc[o];
+                if (c) {
+                    cnt += c;
+                    bsum += bs[o];
+                    psum += (uint64_t)c * (uint64_t)t.y;
+                }
+            };
+            constexpr int U = 8;
+            unsigned i = tid;
+            for (; i + (U - 1) * MP16_THREADS < m.sn; i += U * MP16_THREADS) {
+                longlong2 t[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) t[u] = __ldcs(&S[i + u * MP16_THREADS]);
+#pragma unroll
+                for (int u = 0; u < U; ++u) probe_bin(t[u]);
+            }
+            for (; i < m.sn; i += MP16_THREADS) probe_bin(__ldcs(&S[i]));
+            __syncthreads();  // the bins are reused by the next item
+            continue;
+        }
         int N = 32;
         while (N < (int)m.rn) N <<= 1;
         // Load the build chunk; INT64_MAX keys go to the side counters and
@@ -242,23 +303,39 @@ int mpsm16_agg(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t
         if ((rc = rp_partition(ctx, S, nS, FB, two, true, cs, fs, LS, &S1, &S2, flags, hflags))) break;
         cudaEventRecord(ev[1], ctx->stream);
         if (sizes) *sizes = LS.count;
-        // Items: every (build chunk, probe chunk) pair of each range.
+        // Items: every (build chunk, probe chunk) pair of each range.  Range
+        // f holds keys in [sp[f - 1], sp[f]); a bounded range of at most
+        // MP16_DSPAN key values is one build chunk, sorted by counting.
         std::vector<Mp16Item> items;
         for (int f = 0; f < F; ++f) {
             const unsigned long long rn = LR.count[f], sn = LS.count[f];
             if (!rn || !sn) continue;
-            for (unsigned long long r = 0; r < rn; r += MP16_RCHUNK)
+            long long lo = 0;
+            unsigned span = 0;
+            if (f > 0 && f < F - 1) {
+                const __int128 w = (__int128)sp[f] - (__int128)sp[f - 1];
+                if (w > 0 && w <= (__int128)MP16_DSPAN && rn <= 0xFFFFFFFFULL) {
+                    lo = sp[f - 1];
+                    span = (unsigned)w;
+                }
+            }
+            const unsigned long long rchunk = span ? rn : (unsigned long long)MP16_RCHUNK;
+            for (unsigned long long r = 0; r < rn; r += rchunk)
                 for (unsigned long long s = 0; s < sn; s += MP16_SCHUNK) {
                     Mp16Item it;
                     it.r0 = LR.fstart[f] + r;
                     it.s0 = LS.fstart[f] + s;
-                    it.rn = (unsigned)std::min<unsigned long long>(MP16_RCHUNK, rn - r);
+                    it.rn = (unsigned)std::min<unsigned long long>(rchunk, rn - r);
                     it.sn = (unsigned)std::min<unsigned long long>(MP16_SCHUNK, sn - s);
+                    it.lo = lo;
+                    it.span = span;
+                    it.pad = 0;
                     items.push_back(it);
                 }
         }
         unsigned long long* acc = ctx->dcounters + 212;
-        unsigned* next = (unsigned*)(ctx->dcounters + 215);
+        unsigned* next = (unsigned*)(ctx->dcounters + 215);  // word 215: queue head, then the bad-key flag
+        unsigned* bad = next + 1;
         PYG_CUDA(cudaMemsetAsync(acc, 0, 32, ctx->stream));
         if (!items.empty()) {
             if ((rc = dalloc(ctx, (void**)&ditems, items.size() * sizeof(Mp16Item)))) break;
@@ -271,6 +348,7 @@ int mpsm16_agg(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t
             ja.nitems = (long long)items.size();
             ja.next = next;
             ja.acc = acc;
+            ja.bad = bad;
             PYG_CUDA(cudaFuncSetAttribute(mp16_join_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MP16_SMEM));
             const unsigned grid = (unsigned)std::min<long long>(2LL * ctx->sm_count, ja.nitems);
             mp16_join_kernel<<<grid, MP16_THREADS, MP16_SMEM, ctx->stream>>>(ja);
@@ -278,8 +356,13 @@ int mpsm16_agg(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t
         }
         cudaEventRecord(ev[2], ctx->stream);
         unsigned long long* h = (unsigned long long*)ctx->pinned + 64;
-        PYG_CUDA(cudaMemcpyAsync(h, acc, 24, cudaMemcpyDeviceToHost, ctx->stream));
+        PYG_CUDA(cudaMemcpyAsync(h, acc, 32, cudaMemcpyDeviceToHost, ctx->stream));
         PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        if ((unsigned)(h[3] >> 32)) {
+            set_error("pyg_mpsm_join_agg: a key fell outside its range's span");
+            rc = PYG_ERR_CUDA;
+            break;
+        }
         out[0] = h[0];
         out[1] = h[1];
         out[2] = h[2];
