@@ -743,23 +743,52 @@ static double cdf_continuous(const pyg_cdf* m, int64_t k)
     return m->ylo[l] + (m->yhi[l] - m->ylo[l]) * f;
 }
 
+// Inversion of C for the splitters: the non-empty leaves in order (their
+// target ranges are ordered and disjoint) with the reciprocals the
+// inversion needs, so that each splitter costs multiplications only.
+struct CdfInverse {
+    std::vector<int> leaf;
+    std::vector<double> ylo, inv_span, slope, inv_slope, icpt;
+    double inv_L = 0, inv_a0 = 0, b0 = 0, key_lo = 0, inv_scale = 0;
+    bool usable = false;
+    explicit CdfInverse(const pyg_cdf* m)
+    {
+        for (int l = 0; l < m->L; ++l) {
+            if (!(m->yhi[l] > m->ylo[l])) continue;
+            leaf.push_back(l);
+            ylo.push_back(m->ylo[l]);
+            inv_span.push_back(1.0 / (m->yhi[l] - m->ylo[l]));
+            slope.push_back(m->la[l]);
+            inv_slope.push_back(m->la[l] > 0 ? 1.0 / (double)m->la[l] : 0.0);
+            icpt.push_back(m->lb[l]);
+        }
+        inv_L = 1.0 / (double)m->L;
+        inv_a0 = m->a0 > 0 ? 1.0 / (double)m->a0 : 0.0;
+        b0 = m->b0;
+        key_lo = m->key_lo;
+        inv_scale = m->key_scale != 0 ? 1.0 / m->key_scale : 0.0;
+        usable = !leaf.empty() && m->key_scale != 0;
+    }
+};
+
 // The key at which C reaches c: the leaf whose target range holds c, its
 // line inverted to a leaf coordinate, the root line inverted to a key;
 // `past` (one past the largest sample key) when c is beyond the model.
 // `hint` is the leaf position found for the previous, smaller c: the
 // splitters ask for increasing c, so the search mostly steps forward.
-static int64_t cdf_invert(const pyg_cdf* m, const std::vector<int>& ne, double c, int64_t past, size_t* hint)
+static int64_t cdf_invert(const pyg_cdf* m, const CdfInverse& v, double c, int64_t past, size_t* hint)
 {
-    if (ne.empty() || m->key_scale == 0) return past;
-    size_t lo = *hint < ne.size() ? *hint : 0;
-    if (m->ylo[ne[lo]] <= c) {
+    if (!v.usable) return past;
+    const size_t n = v.ylo.size();
+    size_t lo = *hint < n ? *hint : 0;
+    if (v.ylo[lo] <= c) {
         size_t step = 0;
-        while (lo + 1 < ne.size() && m->ylo[ne[lo + 1]] <= c && ++step < 64) ++lo;
-        if (lo + 1 < ne.size() && m->ylo[ne[lo + 1]] <= c) {  // far ahead: search the rest
-            size_t hi = ne.size();
+        while (lo + 1 < n && v.ylo[lo + 1] <= c && ++step < 64) ++lo;
+        if (lo + 1 < n && v.ylo[lo + 1] <= c) {  // far ahead: search the rest
+            size_t hi = n;
             while (lo + 1 < hi) {
                 const size_t mid = (lo + hi) / 2;
-                if (m->ylo[ne[mid]] <= c) lo = mid;
+                if (v.ylo[mid] <= c) lo = mid;
                 else hi = mid;
             }
         }
@@ -768,19 +797,17 @@ static int64_t cdf_invert(const pyg_cdf* m, const std::vector<int>& ne, double c
         lo = 0;
         while (lo + 1 < hi) {
             const size_t mid = (lo + hi) / 2;
-            if (m->ylo[ne[mid]] <= c) lo = mid;
+            if (v.ylo[mid] <= c) lo = mid;
             else hi = mid;
         }
     }
     *hint = lo;
-    const int l = ne[lo];
-    const double t = (c - m->ylo[l]) / (m->yhi[l] - m->ylo[l]);
-    const double a = m->la[l], b = m->lb[l];
-    double uu = a > 0 ? (t - b) / a : 0.0;
+    const double t = (c - v.ylo[lo]) * v.inv_span[lo];
+    double uu = v.slope[lo] > 0 ? (t - v.icpt[lo]) * v.inv_slope[lo] : 0.0;
     uu = std::min(1.0, std::max(0.0, uu));
-    const double r = ((double)l + uu) / (double)m->L;
-    const double x = m->a0 > 0 ? (r - (double)m->b0) / (double)m->a0 : 0.0;
-    const double kf = m->key_lo + x / m->key_scale;
+    const double r = ((double)v.leaf[lo] + uu) * v.inv_L;
+    const double x = (r - v.b0) * v.inv_a0;
+    const double kf = v.key_lo + x * v.inv_scale;
     if (!(kf > (double)m->kmin)) return m->kmin;
     if (kf >= (double)m->kmax) return past;
     return (int64_t)ceil(kf);
@@ -797,10 +824,7 @@ int pyg_cdf_splitters(pyg_ctx* ctx, const pyg_cdf* m, int32_t fanout, int64_t* o
         set_error("pyg_cdf_splitters: bad arguments");
         return PYG_ERR_ARG;
     }
-    // Non-empty leaves in order (their target ranges are ordered, disjoint).
-    std::vector<int> ne;
-    for (int l = 0; l < m->L; ++l)
-        if (m->yhi[l] > m->ylo[l]) ne.push_back(l);
+    const CdfInverse inv(m);
     const int64_t past = m->kmax == INT64_MAX ? INT64_MAX : m->kmax + 1;  // past the largest sample key
     // Heavy key h covers [Fb[h], Fb[h] + w_h) of F = (1 - W) C + heavy masses.
     const int H = (int)m->heavy_key.size();
@@ -834,7 +858,7 @@ int pyg_cdf_splitters(pyg_ctx* ctx, const pyg_cdf* m, int32_t fanout, int64_t* o
             // In the continuous part between heavy keys a - 1 and a.
             const double below = a < H ? m->heavy_before[a] : W;
             const double c = cont > 1e-12 ? (q - below) / cont : 0.0;
-            key = cdf_invert(m, ne, c, past, &hint);
+            key = cdf_invert(m, inv, c, past, &hint);
             if (a > 0) key = std::max(key, m->heavy_key[a - 1] == INT64_MAX ? INT64_MAX : m->heavy_key[a - 1] + 1);
             if (a < H) key = std::min(key, m->heavy_key[a]);
         }

@@ -490,25 +490,31 @@ static int mpsm_run(pyg_ctx* ctx, const pyg_rel* build, int32_t bkey, const pyg_
                 spl[j - 1] = v > (__int128)INT64_MAX ? INT64_MAX : (int64_t)v;
             }
         } else {
-            double rate = o->sample_rate > 0 ? o->sample_rate : 0.01;
-            int64_t stride = (int64_t)llround(1.0 / rate);
-            if (stride < 1) stride = 1;
-            // The learned model needs far fewer samples than quantile
-            // splitters (which want tens of samples per range): its leaves
-            // are fitted lines, so at most CDF_MPSM_SAMPLE keys (about 64
-            // per leaf) are drawn for it.
-            if (o->splitter_kind == PYG_MPSM_SPLIT_LEARNED && nS / stride > CDF_MPSM_SAMPLE)
-                stride = (nS + CDF_MPSM_SAMPLE - 1) / CDF_MPSM_SAMPLE;
-            int64_t ns = (nS + stride - 1) / stride;
-            if (ns < 2) {
-                stride = 1;
-                ns = nS;
-            }
-            int64_t offset = (int64_t)(o->seed % (uint64_t)stride);
+            // The sample holds as many keys of each relation (each strided
+            // over its own tuples), so that a range bounds its share of
+            // both: splitters of the probe keys alone leave ranges whose
+            // build side is many times the sort tile where the probe side
+            // is skewed.  sample_rate sets the probe side's count; the
+            // learned model needs far fewer keys than quantile splitters
+            // (which want tens per range): its leaves are fitted lines, so at
+            // most CDF_MPSM_SAMPLE keys (about 256 per leaf) are drawn for it.
+            const double rate = o->sample_rate > 0 ? o->sample_rate : 0.01;
+            int64_t want = (int64_t)llround((double)nS * rate);
+            if (o->splitter_kind == PYG_MPSM_SPLIT_LEARNED) want = std::min<int64_t>(want, CDF_MPSM_SAMPLE / 2);
+            want = std::max<int64_t>(want, 2);
+            const int64_t nsS = std::min<int64_t>(want, nS), nsR = std::min<int64_t>(want, nR);
+            const int64_t ns = nsS + nsR;
+            const int64_t strideS = std::max<int64_t>(1, nS / nsS), strideR = nsR ? std::max<int64_t>(1, nR / nsR) : 1;
             int64_t* sample;
             if ((rc = M.alloc((void**)&sample, (size_t)ns * 8))) return fail(rc);
-            mp_sample_kernel<<<grid_for(ctx, ns, 256, 4, 4), 256, 0, ctx->stream>>>(Si, nS, stride, offset, ns, sample);
+            mp_sample_kernel<<<grid_for(ctx, nsS, 256, 4, 4), 256, 0, ctx->stream>>>(
+                Si, nS, strideS, (int64_t)(o->seed % (uint64_t)strideS), nsS, sample);
             PYG_LAUNCHED(ctx);
+            if (nsR) {
+                mp_sample_kernel<<<grid_for(ctx, nsR, 256, 4, 4), 256, 0, ctx->stream>>>(
+                    Ri, nR, strideR, (int64_t)(o->seed % (uint64_t)strideR), nsR, sample + nsS);
+                PYG_LAUNCHED(ctx);
+            }
             if (o->splitter_kind == PYG_MPSM_SPLIT_SAMPLED || ns < 2) {
                 if ((rc = pyg_sampled_splitters(ctx, sample, ns, Fs, spl.data()))) return fail(rc);
             } else {

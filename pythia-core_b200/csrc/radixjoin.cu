@@ -264,8 +264,15 @@ __global__ void __launch_bounds__(RJ_JOIN_THREADS, RJ_JOIN_BLOCKS) rj_join_kerne
 // payload offsets and rebased at the end: sum = count x base + sum of
 // offsets, modulo 2^64.
 
+#ifndef PYG_RJ32_TABLE_KB
+#define PYG_RJ32_TABLE_KB 96
+#endif
+#ifndef PYG_RJ32_BLOCKS
+#define PYG_RJ32_BLOCKS 2
+#endif
 constexpr int RJ32_THREADS = 512;
-constexpr int RJ32_TABLE_BYTES = 96 * 1024;
+constexpr int RJ32_BLOCKS = PYG_RJ32_BLOCKS;  // CTAs per SM
+constexpr int RJ32_TABLE_BYTES = PYG_RJ32_TABLE_KB * 1024;
 constexpr unsigned RJ32_SLOTS = RJ32_TABLE_BYTES / 8;
 constexpr unsigned RJ32_RCAP = RJ32_SLOTS / 2;
 #ifndef PYG_RJ32_U
@@ -291,7 +298,7 @@ __device__ __forceinline__ unsigned rj32_slot(unsigned off)
     return __umulhi(off, RJ32_SLOTS);
 }
 
-__global__ void __launch_bounds__(RJ32_THREADS, 2) rj_join32_kernel(RJJoinArgs a)
+__global__ void __launch_bounds__(RJ32_THREADS, RJ32_BLOCKS) rj_join32_kernel(RJJoinArgs a)
 {
     extern __shared__ __align__(16) unsigned long long rj32_table[];
     __shared__ long long item_cur, item_next;
@@ -528,7 +535,7 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
                            : (unique ? join_fn<true>(LR.packed, LS.packed) : join_fn<false>(LR.packed, LS.packed));
             const int smem = j32 ? RJ32_TABLE_BYTES : RJ_TABLE_BYTES;
             const int threads = j32 ? RJ32_THREADS : RJ_JOIN_THREADS;
-            const int per_sm = j32 ? 2 : RJ_JOIN_BLOCKS;
+            const int per_sm = j32 ? RJ32_BLOCKS : RJ_JOIN_BLOCKS;
             PYG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
             PYG_CUDA(cudaMemsetAsync(acc, 0, 3 * 8, ctx->stream));
             PYG_CUDA(cudaMemsetAsync(next, 0, 16, ctx->stream));
