@@ -447,7 +447,9 @@ def source_digest(files):
     return h.hexdigest()[:16]
 
 
-RADIX_SOURCES = ["radixpart.cu", "radixpart.cuh", "radixjoin.cu", "bulk.cuh"]
+# The sources each kernel's committed ncu traffic figure depends on.
+TRAFFIC_SOURCES = {"partition": ["radixpart.cu", "radixpart.cuh", "bulk.cuh"],
+                   "join": ["radixjoin.cu", "radixpart.cuh"]}
 
 
 def join_roofline(pyg, phase, nR, nS, step_ms, hbm, peak_kind, theta):
@@ -506,7 +508,8 @@ def join_roofline(pyg, phase, nR, nS, step_ms, hbm, peak_kind, theta):
         with open(tpath) as f:
             tj = json.load(f)
         ent = tj.get(f"{top}@theta={theta}")
-        if ent and ent.get("sources") == source_digest(RADIX_SOURCES):
+        kernel = "join" if top == "join" else "partition"
+        if ent and ent.get("sources") == source_digest(TRAFFIC_SOURCES[kernel]):
             roofline["traffic"] = ent["bytes_per_tuple"] * (nR + nS if top == "join" else
                                                            (nR if top.startswith("build") else nS))
             roofline["traffic_source"] = ent.get("profile")
@@ -769,6 +772,12 @@ def workload_line(args, torch, pyg, ctx, rank, world, local, dist, stream):
         ms, _ = _device_timed(torch, stream, fn, args.steps, 0, dist)
     launches = ctx.launches() - launches0
     step_ms = ms / args.steps
+    if args.workload == "mpsm":
+        # Phase times: medians over the timed calls of the first timed run.
+        sts = [o[2] for o in outs]
+        med = lambda f: round(float(np.median([getattr(x, f) for x in sts])), 3)  # noqa: E731
+        extra["mpsm"].update({f: med(f) for f in ("splitter_ms", "partition_ms", "merge_ms")})
+        extra["mpsm"]["phase_stat"] = f"median of {len(sts)} timed calls"
     if args.workload == "batch":
         lat = np.concatenate([o[1] for o in outs])
         extra["fragment_latency_ms"] = {"p50": round(float(np.percentile(lat, 50)), 4),

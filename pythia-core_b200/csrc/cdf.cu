@@ -771,46 +771,79 @@ struct CdfInverse {
     }
 };
 
-// The key at which C reaches c: the leaf whose target range holds c, its
-// line inverted to a leaf coordinate, the root line inverted to a key;
-// `past` (one past the largest sample key) when c is beyond the model.
-// `hint` is the leaf position found for the previous, smaller c: the
-// splitters ask for increasing c, so the search mostly steps forward.
-static int64_t cdf_invert(const pyg_cdf* m, const CdfInverse& v, double c, int64_t past, size_t* hint)
+// Splitter j of `fanout` (1 <= j < fanout) before the running maximum and
+// the heavy-span fix-up that the host applies: the key at which the
+// model's F reaches j / fanout -- the leaf whose target range holds the
+// continuous part's value, its line inverted to a leaf coordinate, the
+// root line inverted to a key; one thread per splitter -- and the heavy key
+// whose span holds it (-1 if none).
+struct SplitArgs {
+    const double* ylo;        // non-empty leaves, in order
+    const double* inv_span;
+    const double* slope;
+    const double* inv_slope;
+    const double* icpt;
+    const double* leaf;       // leaf index (exact in a double)
+    int nleaf;
+    const double* Fb;         // heavy spans [Fb, Fe) of F
+    const double* Fe;
+    const double* hbefore;
+    const int64_t* hkey;
+    int H;
+    double W, cont, inv_L, inv_a0, b0, key_lo, inv_scale;
+    int64_t kmin, kmax, past;
+    int fanout;
+    int64_t* out;             // fanout - 1 keys
+    int* inside;              // fanout entries, index j
+};
+
+__global__ void cdf_split_kernel(SplitArgs a)
 {
-    if (!v.usable) return past;
-    const size_t n = v.ylo.size();
-    size_t lo = *hint < n ? *hint : 0;
-    if (v.ylo[lo] <= c) {
-        size_t step = 0;
-        while (lo + 1 < n && v.ylo[lo + 1] <= c && ++step < 64) ++lo;
-        if (lo + 1 < n && v.ylo[lo + 1] <= c) {  // far ahead: search the rest
-            size_t hi = n;
-            while (lo + 1 < hi) {
-                const size_t mid = (lo + hi) / 2;
-                if (v.ylo[mid] <= c) lo = mid;
-                else hi = mid;
-            }
-        }
-    } else {
-        size_t hi = lo;
-        lo = 0;
-        while (lo + 1 < hi) {
-            const size_t mid = (lo + hi) / 2;
-            if (v.ylo[mid] <= c) lo = mid;
+    for (int j = 1 + blockIdx.x * blockDim.x + threadIdx.x; j < a.fanout; j += gridDim.x * blockDim.x) {
+        const double q = (double)j / (double)a.fanout;
+        int lo = 0, hi = a.H;
+        while (lo < hi) {  // first heavy key whose span ends after q
+            const int mid = (lo + hi) >> 1;
+            if (a.Fe[mid] <= q) lo = mid + 1;
             else hi = mid;
         }
+        int64_t key;
+        int in = -1;
+        if (lo < a.H && q >= a.Fb[lo]) {
+            key = a.hkey[lo];
+            in = lo;
+        } else {
+            const double below = lo < a.H ? a.hbefore[lo] : a.W;
+            const double c = a.cont > 1e-12 ? (q - below) / a.cont : 0.0;
+            if (a.nleaf == 0) {
+                key = a.past;
+            } else {
+                int l0 = 0, l1 = a.nleaf;  // last leaf with ylo <= c (the first if none)
+                while (l0 + 1 < l1) {
+                    const int mid = (l0 + l1) >> 1;
+                    if (a.ylo[mid] <= c) l0 = mid;
+                    else l1 = mid;
+                }
+                const double t = (c - a.ylo[l0]) * a.inv_span[l0];
+                double uu = a.slope[l0] > 0 ? (t - a.icpt[l0]) * a.inv_slope[l0] : 0.0;
+                uu = fmin(1.0, fmax(0.0, uu));
+                const double r = (a.leaf[l0] + uu) * a.inv_L;
+                const double x = (r - a.b0) * a.inv_a0;
+                const double kf = a.key_lo + x * a.inv_scale;
+                if (!(kf > (double)a.kmin)) key = a.kmin;
+                else if (kf >= (double)a.kmax) key = a.past;
+                else key = (int64_t)ceil(kf);
+            }
+            if (lo > 0) {
+                const int64_t k = a.hkey[lo - 1];
+                const int64_t floor_key = k == INT64_MAX ? INT64_MAX : k + 1;
+                key = key < floor_key ? floor_key : key;
+            }
+            if (lo < a.H && key > a.hkey[lo]) key = a.hkey[lo];
+        }
+        a.out[j - 1] = key;
+        a.inside[j] = in;
     }
-    *hint = lo;
-    const double t = (c - v.ylo[lo]) * v.inv_span[lo];
-    double uu = v.slope[lo] > 0 ? (t - v.icpt[lo]) * v.inv_slope[lo] : 0.0;
-    uu = std::min(1.0, std::max(0.0, uu));
-    const double r = ((double)v.leaf[lo] + uu) * v.inv_L;
-    const double x = (r - v.b0) * v.inv_a0;
-    const double kf = v.key_lo + x * v.inv_scale;
-    if (!(kf > (double)m->kmin)) return m->kmin;
-    if (kf >= (double)m->kmax) return past;
-    return (int64_t)ceil(kf);
 }
 
 }  // namespace pyg
@@ -819,7 +852,10 @@ extern "C" {
 
 int pyg_cdf_splitters(pyg_ctx* ctx, const pyg_cdf* m, int32_t fanout, int64_t* out)
 {
-    (void)ctx;
+    if (fanout > 1) {
+        const int rc0 = check_ctx(ctx);
+        if (rc0) return rc0;
+    }
     if (!m || fanout < 1 || (fanout > 1 && !out)) {
         set_error("pyg_cdf_splitters: bad arguments");
         return PYG_ERR_ARG;
@@ -839,32 +875,83 @@ int pyg_cdf_splitters(pyg_ctx* ctx, const pyg_cdf* m, int32_t fanout, int64_t* o
         }
     }
     std::vector<int> inside(fanout, -1);  // splitter j (1-based) falls in heavy key h's span
-    int64_t prev = m->kmin;
-    size_t hint = 0;
-    for (int j = 1; j < fanout; ++j) {
-        const double q = (double)j / (double)fanout;
-        // First heavy key whose span ends after q.
-        int a = 0, b = H;
-        while (a < b) {
-            const int mid = (a + b) >> 1;
-            if (Fe[mid] <= q) a = mid + 1;
-            else b = mid;
+    if (!inv.usable) {
+        for (int j = 1; j < fanout; ++j) out[j - 1] = past;
+    } else {
+        // One thread per splitter on the device: the model's leaf and heavy
+        // tables go up in one copy, keys and span marks come back.
+        const int n = (int)inv.ylo.size();
+        std::vector<double> hd((size_t)6 * n + 3 * H);
+        double* q = hd.data();
+        for (int i = 0; i < n; ++i) {
+            q[i] = inv.ylo[i];
+            q[n + i] = inv.inv_span[i];
+            q[2 * n + i] = inv.slope[i];
+            q[3 * n + i] = inv.inv_slope[i];
+            q[4 * n + i] = inv.icpt[i];
+            q[5 * n + i] = (double)inv.leaf[i];
         }
-        int64_t key;
-        if (a < H && q >= Fb[a]) {
-            key = m->heavy_key[a];
-            inside[j] = a;
-        } else {
-            // In the continuous part between heavy keys a - 1 and a.
-            const double below = a < H ? m->heavy_before[a] : W;
-            const double c = cont > 1e-12 ? (q - below) / cont : 0.0;
-            key = cdf_invert(m, inv, c, past, &hint);
-            if (a > 0) key = std::max(key, m->heavy_key[a - 1] == INT64_MAX ? INT64_MAX : m->heavy_key[a - 1] + 1);
-            if (a < H) key = std::min(key, m->heavy_key[a]);
+        for (int h = 0; h < H; ++h) {
+            q[6 * n + h] = Fb[h];
+            q[6 * n + H + h] = Fe[h];
+            q[6 * n + 2 * H + h] = m->heavy_before[h];
         }
-        if (key < prev) key = prev;
-        out[j - 1] = key;
-        prev = key;
+        char* dbuf = nullptr;
+        const size_t dbytes = hd.size() * 8 + (size_t)H * 8 + (size_t)(fanout - 1) * 8 + (size_t)fanout * 4;
+        int rc = dalloc(ctx, (void**)&dbuf, dbytes);
+        if (rc) return rc;
+        double* dd = (double*)dbuf;
+        int64_t* dk = (int64_t*)(dbuf + hd.size() * 8);
+        int64_t* dout = dk + H;
+        int* din = (int*)(dout + (fanout - 1));
+        SplitArgs sa;
+        sa.ylo = dd;
+        sa.inv_span = dd + n;
+        sa.slope = dd + 2 * n;
+        sa.inv_slope = dd + 3 * n;
+        sa.icpt = dd + 4 * n;
+        sa.leaf = dd + 5 * n;
+        sa.nleaf = n;
+        sa.Fb = dd + 6 * n;
+        sa.Fe = dd + 6 * n + H;
+        sa.hbefore = dd + 6 * n + 2 * H;
+        sa.hkey = dk;
+        sa.H = H;
+        sa.W = W;
+        sa.cont = cont;
+        sa.inv_L = inv.inv_L;
+        sa.inv_a0 = inv.inv_a0;
+        sa.b0 = inv.b0;
+        sa.key_lo = inv.key_lo;
+        sa.inv_scale = inv.inv_scale;
+        sa.kmin = m->kmin;
+        sa.kmax = m->kmax;
+        sa.past = past;
+        sa.fanout = fanout;
+        sa.out = dout;
+        sa.inside = din;
+        cudaError_t e = cudaMemcpyAsync(dd, hd.data(), hd.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess && H)
+            e = cudaMemcpyAsync(dk, m->heavy_key.data(), (size_t)H * 8, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) {
+            cdf_split_kernel<<<grid_for(ctx, fanout, 256, 1, 4), 256, 0, ctx->stream>>>(sa);
+            e = cudaGetLastError();
+            ctx->launches++;
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(out, dout, (size_t)(fanout - 1) * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(inside.data(), din, (size_t)fanout * 4, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        dfree(ctx, dbuf);
+        if (e != cudaSuccess) return cuda_status(e, "pyg_cdf_splitters");
+        inside[0] = -1;
+        // Running maximum: splitters never decrease.
+        int64_t prev = m->kmin;
+        for (int j = 1; j < fanout; ++j) {
+            if (out[j - 1] < prev) out[j - 1] = prev;
+            prev = out[j - 1];
+        }
     }
     // A heavy key that takes two or more splitters gets a range of its own:
     // the last of them becomes key + 1 (exact quantiles do the same).
