@@ -48,7 +48,8 @@ def parse():
     ap.add_argument("--theta", type=float, default=0.0)
     ap.add_argument("--impl", default="pyg", choices=["pyg", "reference"])
     ap.add_argument("--load-factor", type=float, default=0.5)
-    ap.add_argument("--algo", default="radix", choices=["radix", "direct", "auto"])
+    ap.add_argument("--algo", default=None, choices=["radix", "direct", "auto"],
+                    help="join algorithm (default: radix for the headline join, auto for join-small)")
     ap.add_argument("--radix-bits", type=int, default=0, help="log2 partition fan-out (0 = automatic)")
     ap.add_argument("--scale-shift", type=int, default=0, help="shrink both relations by 2^s (debug only)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -845,6 +846,8 @@ def run_secondary(args, torch, pyg, ctx, local, stream):
 
 def main():
     args = parse()
+    if args.algo is None:
+        args.algo = "auto" if args.workload == "join-small" else "radix"
     if args.impl == "reference":
         main_reference(args)
     elif args.workload != "join":

@@ -3,11 +3,24 @@
 // lists which reference method each member replaces.
 #include "gpuhashjoin.h"
 
+#include <pthread.h>
+#include <stdio.h>
 #include <string.h>
 
 #include "exceptions.h"
 
 pyg_ctx* GpuHashJoinOp::ctx_ = 0;
+
+// A libpyg context serves one host thread at a time, and the leaders of
+// different thread groups join concurrently: they take turns on it.
+static pthread_mutex_t g_ctx_mutex = PTHREAD_MUTEX_INITIALIZER;
+
+namespace {
+struct CtxLock {
+    CtxLock() { pthread_mutex_lock(&g_ctx_mutex); }
+    ~CtxLock() { pthread_mutex_unlock(&g_ctx_mutex); }
+};
+}  // namespace
 
 pyg_ctx* GpuHashJoinOp::context() { return ctx_; }
 
@@ -125,6 +138,7 @@ void GpuHashJoinOp::join_group(unsigned short groupno)
     pyg_rel r = as_rel(buildOp->getOutSchema(), R);
     pyg_rel s = as_rel(probeOp->getOutSchema(), S);
     const unsigned int tb = schema.getTupleSize();
+    CtxLock lock;
     pyg_hashtable* ht = 0;
     void* dev = 0;
     int64_t n = 0;
@@ -144,6 +158,7 @@ void GpuHashJoinOp::join_group(unsigned short groupno)
     if (dev) pyg_free(ctx_, dev);
     if (ht) pyg_hashtable_free(ctx_, ht);
     if (rc != PYG_OK) {
+        fprintf(stderr, "GpuHashJoinOp: group %u: %s\n", (unsigned)groupno, pyg_last_error());
         if (host) pyg_host_free(host);
         g.failed = true;
         return;
@@ -214,6 +229,7 @@ void GpuHashJoinOp::threadClose(unsigned short threadid)
     barriers[groupno].Arrive();
     if (groupleader[groupno] == threadid) {
         Group& g = groups_[groupno];
+        CtxLock lock;
         if (g.out) pyg_host_free(g.out);
         g.out = 0;
         g.nout = 0;

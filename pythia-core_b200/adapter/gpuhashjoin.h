@@ -15,8 +15,9 @@
 //               into its own host buffer, then waits at the group's
 //               barrier; the group leader runs pyg_hashjoin_build +
 //               pyg_hashjoin_probe_materialize over the group's tuples and
-//               copies the joined tuples to pinned host memory; a second
-//               barrier releases the group.
+//               copies the joined tuples to pinned host memory (leaders
+//               of different groups take turns on the one libpyg context);
+//               a second barrier releases the group.
 //   getNext     thread t serves slice t (its position in the group) of the
 //               group's output, as pages of at most `buffsize` bytes that
 //               wrap the output in place.

@@ -6,9 +6,11 @@
 // Semantics follow the reference's HashJoinOp (operators/join.cpp:367-903):
 // every (build, probe) pair with equal keys is one output tuple made of the
 // projected columns.  The bucket function of the reference only places
-// tuples; the join result does not depend on it, so the table here uses its
-// own hash (a 64-bit bijective mix + multiply-high range reduction) and
-// linear probing.
+// tuples; the join result does not depend on it, so the tables here use
+// their own hashes and linear probing: a 64-bit bijective mix with a
+// multiply-high range reduction (general tables), or the top bits of the
+// radix operators' hash over a power-of-two table (the one-shot direct
+// join).
 #include <string.h>
 
 #include <algorithm>
@@ -610,6 +612,25 @@ struct PhaseTimer {
     }
 };
 
+// ---------------------------------------------------------------------------
+// One-shot direct join of 16-byte (int64 key @0, int64 payload @8) device
+// relations.  The table is 2^b 16-byte slots {key, payload} (kEmptyKey marks
+// a free slot), slot = the top b bits of the radix operators' hash (rj_hash:
+// three xor-shifts, then a Fibonacci multiply), linear probing.  A block
+// walks tiles of DJ_THREADS x DJ_U consecutive tuples, thread t taking
+// tuples t, t + DJ_THREADS, ...: one 64-bit tile base per tile, constant
+// offsets inside it, and DJ_U independent loads (and CASes / table reads)
+// in flight per thread.  Build keys equal to kEmptyKey go to a side list;
+// probe keys equal to it are matched against that list.
+
+constexpr int DJ_THREADS = 256;
+#ifndef PYG_DJ_UNROLL
+#define PYG_DJ_UNROLL 4
+#endif
+constexpr int DJ_U = PYG_DJ_UNROLL;
+
+__device__ __forceinline__ uint64_t dj_slot(uint64_t k, int shift) { return rj_hash(k) >> shift; }
+
 // Empty table of cap 16-byte slots and nwords zeroed counter words.
 __global__ void dj_clear_kernel(ulonglong2* __restrict__ slots, uint64_t cap, unsigned long long* __restrict__ words,
                                 int nwords)
@@ -619,22 +640,154 @@ __global__ void dj_clear_kernel(ulonglong2* __restrict__ slots, uint64_t cap, un
     for (; i < cap; i += (uint64_t)gridDim.x * blockDim.x) slots[i] = make_ulonglong2(kEmptyKey, 0ULL);
 }
 
+// Build: one 16-byte CAS stores key and payload together.  flags: [0] a
+// repeated key, [1] no free slot found, [2] side-list entries.  The table
+// has more slots than build tuples, so an insert always finds a free slot.
+__global__ void __launch_bounds__(DJ_THREADS) dj_build_kernel(const longlong2* __restrict__ R, int64_t n,
+                                                              ulonglong2* __restrict__ slots, uint64_t mask, int shift,
+                                                              uint64_t* __restrict__ side, int64_t side_cap,
+                                                              unsigned long long* __restrict__ flags)
+{
+    unsigned __int128* s128 = reinterpret_cast<unsigned __int128*>(slots);
+    const unsigned __int128 empty = slot128(kEmptyKey, 0);
+    const int64_t tile = (int64_t)DJ_THREADS * DJ_U;
+    bool dup = false, full = false;
+    for (int64_t t0 = (int64_t)blockIdx.x * tile; t0 < n; t0 += (int64_t)gridDim.x * tile) {
+        const longlong2* p = R + t0 + threadIdx.x;
+        const int64_t left = n - t0 - (int64_t)threadIdx.x;  // p[u * DJ_THREADS] exists iff u * DJ_THREADS < left
+        longlong2 t[DJ_U];
+        uint64_t s[DJ_U];
+        unsigned long long prev[DJ_U];
+#pragma unroll
+        for (int u = 0; u < DJ_U; ++u)
+            t[u] = u * DJ_THREADS < left ? __ldcs(p + u * DJ_THREADS) : make_longlong2((long long)kEmptyKey, 0);
+#pragma unroll
+        for (int u = 0; u < DJ_U; ++u) {
+            const uint64_t k = (uint64_t)t[u].x;
+            s[u] = dj_slot(k, shift);
+            prev[u] = k == kEmptyKey
+                          ? kEmptyKey
+                          : (unsigned long long)atomicCAS(&s128[s[u]], empty, slot128(k, (uint64_t)t[u].y));
+        }
+#pragma unroll
+        for (int u = 0; u < DJ_U; ++u) {
+            if (u * DJ_THREADS >= left) continue;
+            const uint64_t k = (uint64_t)t[u].x;
+            if (k == kEmptyKey) {
+                const unsigned long long e = atomicAdd(&flags[2], 1ULL);
+                if ((int64_t)e < side_cap) {
+                    side[2 * e] = k;
+                    side[2 * e + 1] = (uint64_t)t[u].y;
+                }
+                continue;
+            }
+            uint64_t ss = s[u];
+            unsigned long long pv = prev[u];  // key word of the slot before the CAS
+            for (uint64_t steps = 0; pv != kEmptyKey && pv != k;) {
+                if (++steps > mask) {
+                    full = true;
+                    break;
+                }
+                ss = (ss + 1) & mask;
+                pv = (unsigned long long)atomicCAS(&s128[ss], empty, slot128(k, (uint64_t)t[u].y));
+            }
+            dup |= pv == k;
+        }
+    }
+    const bool anydup = __any_sync(0xffffffffu, dup), anyfull = __any_sync(0xffffffffu, full);
+    if ((threadIdx.x & 31) == 0) {
+        if (anydup) flags[0] = 1;
+        if (anyfull) flags[1] = 1;
+    }
+}
+
+// Probe of one tuple whose home slot held e.
+__device__ __forceinline__ void dj_match(const longlong2 t, ulonglong2 e, uint64_t s, const ulonglong2* __restrict__ slots,
+                                         uint64_t mask, const uint64_t* __restrict__ side, int64_t nside,
+                                         uint64_t& cnt, uint64_t& bsum, uint64_t& psum)
+{
+    const uint64_t k = (uint64_t)t.x;
+    if (k == kEmptyKey) {
+        for (int64_t j = 0; j < nside; ++j)
+            if (side[2 * j] == k) {
+                ++cnt;
+                bsum += side[2 * j + 1];
+                psum += (uint64_t)t.y;
+            }
+        return;
+    }
+    for (uint64_t steps = 0; e.x != k; ++steps) {
+        if (e.x == kEmptyKey || steps > mask) return;
+        s = (s + 1) & mask;
+        e = __ldg(&slots[s]);
+    }
+    ++cnt;
+    bsum += e.y;
+    psum += (uint64_t)t.y;
+}
+
+// Probe with the fused count / sum sink: out[0] += matches, out[1] += build
+// payloads, out[2] += probe payloads.  flags are the build's: a build that
+// repeated a key or overfilled its side list is probed by the general path,
+// so this launch then does nothing.
+__global__ void __launch_bounds__(DJ_THREADS) dj_probe_kernel(const longlong2* __restrict__ S, int64_t n,
+                                                              const ulonglong2* __restrict__ slots, uint64_t mask,
+                                                              int shift, const uint64_t* __restrict__ side,
+                                                              int64_t side_cap,
+                                                              const unsigned long long* __restrict__ flags,
+                                                              unsigned long long* __restrict__ out)
+{
+    const unsigned long long dup = flags[0], full = flags[1], ns = flags[2];
+    if (dup | full || ns > (unsigned long long)side_cap) return;
+    const int64_t nside = (int64_t)ns;
+    uint64_t cnt = 0, bsum = 0, psum = 0;
+    const int64_t tile = (int64_t)DJ_THREADS * DJ_U;
+    for (int64_t t0 = (int64_t)blockIdx.x * tile; t0 < n; t0 += (int64_t)gridDim.x * tile) {
+        const longlong2* p = S + t0 + threadIdx.x;
+        const int64_t left = n - t0 - (int64_t)threadIdx.x;
+        longlong2 t[DJ_U];
+        ulonglong2 e[DJ_U];
+        uint64_t s[DJ_U];
+        if (left > (int64_t)(DJ_U - 1) * DJ_THREADS) {
+#pragma unroll
+            for (int u = 0; u < DJ_U; ++u) t[u] = __ldcs(p + u * DJ_THREADS);
+#pragma unroll
+            for (int u = 0; u < DJ_U; ++u) {
+                s[u] = dj_slot((uint64_t)t[u].x, shift);
+                e[u] = __ldg(&slots[s[u]]);
+            }
+#pragma unroll
+            for (int u = 0; u < DJ_U; ++u) dj_match(t[u], e[u], s[u], slots, mask, side, nside, cnt, bsum, psum);
+        } else {
+            for (int u = 0; u * DJ_THREADS < left; ++u) {
+                const longlong2 tu = __ldcs(p + u * DJ_THREADS);
+                const uint64_t su = dj_slot((uint64_t)tu.x, shift);
+                dj_match(tu, __ldg(&slots[su]), su, slots, mask, side, nside, cnt, bsum, psum);
+            }
+        }
+    }
+    uint64_t acc[3] = {cnt, bsum, psum};
+    block_flush(acc, 3, out);
+}
+
 // One-shot join + sum of 16-byte (int64 key @0, int64 payload @8) device
 // relations through one table in HBM (L2-resident for build sides up to a
 // few million tuples): clear, build, probe as three launches, one copy of
 // the counter words and one host synchronisation.  The table and its side
 // list live in the context's grow-only arena, so a call allocates nothing
 // once the arena is large enough.  The probe reads the build's flags on
-// the device; when the build side repeated a key, filled the table or had
-// more empty-marker keys than the side list holds, the probe does nothing,
-// *fallback is set and the caller takes the general path.
+// the device; when the build side repeated a key or had more empty-marker
+// keys than the side list holds, the probe does nothing, *fallback is set
+// and the caller takes the general path.
 // res = {count, build payload sum, probe payload sum}.
 static int direct_join16(pyg_ctx* ctx, const longlong2* R, int64_t nR, const longlong2* S, int64_t nS, float lf,
                          unsigned long long res[3], bool* fallback, PhaseTimer* tm)
 {
     *fallback = false;
-    uint64_t cap = (uint64_t)((double)nR / (double)lf) + 1;
-    if (cap < 64) cap = 64;
+    // 2^bits slots, more than nR / lf (so at least one slot stays free).
+    int bits = 6;
+    while (bits < 62 && (double)((uint64_t)1 << bits) * (double)lf <= (double)nR) ++bits;
+    const uint64_t cap = (uint64_t)1 << bits;
     const int64_t side_cap = nR < 1024 ? (nR > 0 ? nR : 1) : 1024;
     const size_t need = (size_t)cap * 16 + (size_t)side_cap * 16;
     if (ctx->join_arena_bytes < need) {
@@ -647,33 +800,20 @@ static int direct_join16(pyg_ctx* ctx, const longlong2* R, int64_t nR, const lon
     }
     ulonglong2* slots = (ulonglong2*)ctx->join_arena;
     uint64_t* side = (uint64_t*)(slots + cap);
-    unsigned long long* words = ctx->dcounters;  // [0..3] build flags, [8..10] probe sums
-    const int threads = 256;
-    dj_clear_kernel<<<grid_for(ctx, (int64_t)cap, threads, 4, 8), threads, 0, ctx->stream>>>(slots, cap, words, 11);
+    unsigned long long* words = ctx->dcounters;  // [0..2] build flags, [8..10] probe sums
+    dj_clear_kernel<<<grid_for(ctx, (int64_t)cap, 256, 4, 8), 256, 0, ctx->stream>>>(slots, cap, words, 11);
     PYG_LAUNCHED(ctx);
-    BuildArgs a;
-    memset(&a, 0, sizeof(a));
-    a.base = (const uint8_t*)R;
-    a.n = nR;
-    a.tb = 16;
-    a.slots = (uint64_t*)slots;
-    a.cap = cap;
-    a.W = 2;
-    a.agg = 1;
-    a.side = side;
-    a.side_cap = side_cap;
-    a.flags = words;
     tm->mark(ctx, 1);
     if (nR > 0) {
-        ht_build16_kernel<4><<<grid_for(ctx, nR, threads, 4, 8), threads, 0, ctx->stream>>>(a);
+        dj_build_kernel<<<grid_for(ctx, nR, DJ_THREADS, DJ_U, 8), DJ_THREADS, 0, ctx->stream>>>(
+            R, nR, slots, cap - 1, 64 - bits, side, side_cap, words);
         PYG_LAUNCHED(ctx);
     }
     tm->mark(ctx, 2);
     tm->mark(ctx, 3);
     if (nS > 0) {
-        constexpr int U = PYG_PROBE_UNROLL;
-        probe_agg16_kernel<U, false><<<grid_for(ctx, nS, threads, U, 8), threads, 0, ctx->stream>>>(
-            S, nS, slots, cap, nullptr, side, 0, words + 8, words, side_cap);
+        dj_probe_kernel<<<grid_for(ctx, nS, DJ_THREADS, DJ_U, 8), DJ_THREADS, 0, ctx->stream>>>(
+            S, nS, slots, cap - 1, 64 - bits, side, side_cap, words, words + 8);
         PYG_LAUNCHED(ctx);
     }
     tm->mark(ctx, 4);

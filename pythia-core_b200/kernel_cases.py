@@ -11,7 +11,7 @@ Inputs are sized to exceed the 126 MB L2 while staying a few GB on the
 device.  Cases and the kernels they launch:
 
   radix      R 2^24 x S 2^27 PK-FK radix join      rj_hist, rj_partition, rj_join
-  direct     R 2^20 x S 2^24 join, one HBM table    ht_init, ht_build16, probe_agg16
+  direct     R 2^20 x S 2^24 join, one HBM table    dj_clear, dj_build, dj_probe
   groupby16  2^26 (int64, int64), G = 16 / 1024 / 2^16   gbr_tiny / gbr_direct / gbr_part
   composite  2^25 (int32, int32, int64), G = 2^16    groupby_kernel
   partition  2^25 tuples, exactrange, fan-out 64     pt_hist, pt_scatter
