@@ -47,6 +47,18 @@ int pyg_cdf_free(pyg_ctx* ctx, pyg_cdf* model);
 /* fanout-1 non-decreasing splitters into host array out: bucket b holds
  * keys in [out[b-1], out[b]). */
 int pyg_cdf_splitters(pyg_ctx* ctx, const pyg_cdf* model, int32_t fanout, int64_t* out);
+/* Partition bins of n device keys computed by the model itself, without a
+ * search: out[i] (device) in [0, 2^fbits), non-decreasing in the key (the
+ * model's CDF scaled to 2^fbits bins, keys at or below the sample minimum
+ * in bin 0, at or above its maximum in the last).  The MPSM join's learned
+ * splitter partitions with these bins; fbits <= 24. */
+int pyg_cdf_bins(pyg_ctx* ctx, const pyg_cdf* model, int32_t fbits, const int64_t* keys, int64_t n,
+                 uint32_t* out);
+/* The 2^fbits - 1 splitters of those bins into host array out: out[j - 1]
+ * is the first key of bin j (bisection over the same device function), so
+ * that bin(k) = number of splitters <= k, as a splitter search would
+ * place k. */
+int pyg_cdf_bin_splitters(pyg_ctx* ctx, const pyg_cdf* model, int32_t fbits, int64_t* out);
 /* Predicted CDF in [0,1] for n device keys into device float array out. */
 int pyg_cdf_predict(pyg_ctx* ctx, const pyg_cdf* model, const int64_t* keys, int64_t n, float* out);
 /* Trained parameters to host: params[0..1] = root (slope, intercept) in

@@ -23,6 +23,7 @@
 
 #include "../../include/pyg_learned.h"
 #include "primitives.cuh"
+#include "radixpart.cuh"
 
 struct pyg_cdf {
     int L = 0;
@@ -45,6 +46,11 @@ struct pyg_cdf {
     int64_t* d_hkeys = nullptr;    // device copies for predict
     double* d_hbefore = nullptr;
     double* d_hw = nullptr;
+    // Device tables of the model's own bins (pyg::cdf_bin_model), built on
+    // first use: L leaves, then the heavy keys and their masses.
+    mutable pyg::RJLeaf* d_bleaf = nullptr;
+    mutable long long* d_bhkey = nullptr;
+    mutable float* d_bhw = nullptr;
 };
 
 namespace pyg {
@@ -718,6 +724,7 @@ int pyg_cdf_free(pyg_ctx* ctx, pyg_cdf* m)
         dfree(ctx, m->d_hkeys);
         dfree(ctx, m->d_hbefore);
         dfree(ctx, m->d_hw);
+        dfree(ctx, m->d_bleaf);
     }
     delete m;
     return PYG_OK;
@@ -844,6 +851,139 @@ __global__ void cdf_split_kernel(SplitArgs a)
         a.out[j - 1] = key;
         a.inside[j] = in;
     }
+}
+
+// ---------------------------------------------------------------------------
+// The model's own bins (rj_model_bin): partitions computed from the key by
+// the model instead of searched among splitters.
+
+// Leaf of key k on the host, with the device's operations (correctly
+// rounded fp64 / fp32 steps give the same results on both sides).
+static int bin_leaf_host(const pyg_cdf* m, int64_t k)
+{
+    const float x = (float)(((double)k - m->key_lo) * m->key_scale);
+    const float lr = fmaf(m->a0, x, m->b0) * (float)m->L;
+    const float fl = floorf(lr);
+    return fl < 0.f ? 0 : (fl > (float)(m->L - 1) ? m->L - 1 : (int)fl);
+}
+
+int cdf_bin_model(pyg_ctx* ctx, const pyg_cdf* m, int fbits, RJModel* out)
+{
+    if (!m || m->L < 1 || fbits < 1 || fbits > 24) {
+        set_error("cdf bins: no usable model for 2^%d bins", fbits);
+        return PYG_ERR_ARG;
+    }
+    const int L = m->L, H = (int)m->heavy_key.size();
+    if (!m->d_bleaf) {
+        // g = base_l + span_l t (+ the leaf's heavy masses below the key),
+        // capped at top_l; base_{l+1} >= top_l keeps bins ordered across
+        // leaves.  The heavy masses below a leaf are part of its base.
+        const double cont = 1.0 - m->wheavy;
+        std::vector<RJLeaf> lv(L);
+        std::vector<float> hw(H);
+        int h = 0;
+        double below = 0.0;  // heavy mass of the leaves so far
+        float prev_top = 0.f;
+        for (int l = 0; l < L; ++l) {
+            RJLeaf& p = lv[l];
+            const double ylo = m->ylo[l], yhi = m->yhi[l];
+            const bool ok = std::isfinite(ylo) && std::isfinite(yhi) && yhi > ylo;
+            p.base = std::max(prev_top, (float)(cont * (ok ? ylo : 0.0) + below));
+            p.span = ok ? (float)(cont * (yhi - ylo)) : 0.f;
+            p.slope = std::isfinite(m->la[l]) ? std::max(0.f, m->la[l]) : 0.f;
+            p.icpt = std::isfinite(m->lb[l]) ? m->lb[l] : 0.f;
+            p.h0 = h;
+            float top = fmaf(p.span, 1.f, p.base);
+            while (h < H && bin_leaf_host(m, m->heavy_key[h]) <= l) {
+                hw[h] = (float)m->heavy_w[h];
+                top = top + hw[h];
+                below += m->heavy_w[h];
+                ++h;
+            }
+            p.hn = h - p.h0;
+            p.top = top;
+            p.pad = 0;
+            prev_top = top;
+        }
+        char* buf = nullptr;
+        const size_t bytes = (size_t)L * sizeof(RJLeaf) + (size_t)H * 8 + (size_t)H * 4 + 16;
+        int rc = dalloc(ctx, (void**)&buf, bytes);
+        if (rc) return rc;
+        m->d_bleaf = (RJLeaf*)buf;
+        m->d_bhkey = (long long*)(buf + (size_t)L * sizeof(RJLeaf));
+        m->d_bhw = (float*)(m->d_bhkey + H);
+        PYG_CUDA(cudaMemcpyAsync(m->d_bleaf, lv.data(), (size_t)L * sizeof(RJLeaf), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        if (H) {
+            PYG_CUDA(cudaMemcpyAsync(m->d_bhkey, m->heavy_key.data(), (size_t)H * 8, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+            PYG_CUDA(cudaMemcpyAsync(m->d_bhw, hw.data(), (size_t)H * 4, cudaMemcpyHostToDevice, ctx->stream));
+        }
+        // The staged host vectors must outlive the copies.
+        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    RJModel r;
+    r.leaf = m->d_bleaf;
+    r.hkey = m->d_bhkey;
+    r.hw = m->d_bhw;
+    r.key_lo = m->key_lo;
+    // A sample of one key value has no scale: every key then has x = 0 (a
+    // constant is monotone too; the bins hold keys below, at and above it).
+    r.key_scale = std::isfinite(m->key_scale) && m->key_scale > 0 ? m->key_scale : 0.0;
+    r.kmin = m->kmin;
+    r.kmax = m->kmax;
+    // Bin 0 holds the keys <= kmin and the last bin those >= kmax; keep
+    // kmin < kmax so that both ends exist.
+    if (r.kmax <= r.kmin) {
+        if (r.kmin < INT64_MAX) r.kmax = r.kmin + 1;
+        else r.kmin = r.kmax - 1;
+    }
+    r.a0 = std::max(0.f, m->a0);
+    r.b0 = m->b0;
+    r.L = L;
+    r.fbits = fbits;
+    *out = r;
+    return PYG_OK;
+}
+
+// Splitter j (1 <= j < 2^fbits) = the first key whose bin is >= j, by
+// bisection over [kmin, kmax] (bin(kmin) = 0 < j <= bin(kmax)); since the
+// bins never decrease with the key, bin(k) = number of splitters <= k.
+__global__ void bin_splitters_kernel(RJModel m, int64_t* __restrict__ out)
+{
+    const int F = 1 << m.fbits;
+    for (int j = 1 + blockIdx.x * blockDim.x + threadIdx.x; j < F; j += gridDim.x * blockDim.x) {
+        // Keys as order-preserving unsigned words (sign bit flipped).
+        unsigned long long lo = to_sortable(m.kmin), hi = to_sortable(m.kmax);
+        while (hi - lo > 1) {
+            const unsigned long long mid = lo + ((hi - lo) >> 1);
+            if (rj_model_bin(m, from_sortable(mid)) >= (unsigned)j) hi = mid;
+            else lo = mid;
+        }
+        out[j - 1] = from_sortable(hi);
+    }
+}
+
+__global__ void model_bins_kernel(RJModel m, const int64_t* __restrict__ keys, int64_t n, uint32_t* __restrict__ out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = rj_model_bin(m, keys[i]);
+}
+
+int model_splitters(pyg_ctx* ctx, const RJModel& m, int64_t* out)
+{
+    const int F = 1 << m.fbits;
+    if (F < 2) return PYG_OK;
+    int64_t* d = nullptr;
+    int rc = dalloc(ctx, (void**)&d, (size_t)(F - 1) * 8);
+    if (rc) return rc;
+    bin_splitters_kernel<<<grid_for(ctx, F - 1, 128, 1, 8), 128, 0, ctx->stream>>>(m, d);
+    cudaError_t e = cudaGetLastError();
+    ctx->launches++;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, (size_t)(F - 1) * 8, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    dfree(ctx, d);
+    return e == cudaSuccess ? PYG_OK : cuda_status(e, "model splitters");
 }
 
 }  // namespace pyg
@@ -981,6 +1121,35 @@ int pyg_cdf_predict(pyg_ctx* ctx, const pyg_cdf* m, const int64_t* keys, int64_t
         (int)m->heavy_key.size(), m->wheavy, out);
     PYG_LAUNCHED(ctx);
     return PYG_OK;
+}
+
+int pyg_cdf_bins(pyg_ctx* ctx, const pyg_cdf* m, int32_t fbits, const int64_t* keys, int64_t n, uint32_t* out)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!m || n < 0 || (n > 0 && (!keys || !out))) {
+        set_error("pyg_cdf_bins: bad arguments");
+        return PYG_ERR_ARG;
+    }
+    RJModel bm;
+    if ((rc = cdf_bin_model(ctx, m, fbits, &bm))) return rc;
+    if (n == 0) return PYG_OK;
+    model_bins_kernel<<<grid_for(ctx, n, 256, 4, 8), 256, 0, ctx->stream>>>(bm, keys, n, out);
+    PYG_LAUNCHED(ctx);
+    return PYG_OK;
+}
+
+int pyg_cdf_bin_splitters(pyg_ctx* ctx, const pyg_cdf* m, int32_t fbits, int64_t* out)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!m || !out) {
+        set_error("pyg_cdf_bin_splitters: bad arguments");
+        return PYG_ERR_ARG;
+    }
+    RJModel bm;
+    if ((rc = cdf_bin_model(ctx, m, fbits, &bm))) return rc;
+    return model_splitters(ctx, bm, out);
 }
 
 int pyg_cdf_params(pyg_ctx* ctx, const pyg_cdf* m, float* params, int32_t cap, double* key_lo, double* key_scale)

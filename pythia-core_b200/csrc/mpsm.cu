@@ -28,6 +28,7 @@
 #include "mpsm16.cuh"
 #include "partition.cuh"
 #include "primitives.cuh"
+#include "radixpart.cuh"
 
 namespace pyg {
 
@@ -468,6 +469,16 @@ static int mpsm_run(pyg_ctx* ctx, const pyg_rel* build, int32_t bkey, const pyg_
 
     // ---- 1. splitters
     std::vector<int64_t> spl(Fs > 1 ? Fs - 1 : 0);
+    // Learned splitters on the 16-byte path: the model's own bins
+    // (rj_model_bin) partition both relations, and its splitters (the first
+    // key of each bin) bound the ranges; the model lives until the join.
+    pyg_cdf* model = nullptr;
+    RJModel bins;
+    bool use_bins = false;
+    auto done = [&](int code) {
+        pyg_cdf_free(ctx, model);
+        return fail(code);
+    };
     unsigned long long* h = (unsigned long long*)ctx->pinned + 256;
     if (Fs > 1 && nR + nS > 0) {
         if (o->splitter_kind == PYG_MPSM_SPLIT_EXACTRANGE || nS == 0) {
@@ -524,11 +535,17 @@ static int mpsm_run(pyg_ctx* ctx, const pyg_rel* build, int32_t bkey, const pyg_
                 to.epochs = 1;
                 to.lr = 0.002f;
                 to.seed = o->seed;
-                pyg_cdf* model = nullptr;
-                if ((rc = pyg_cdf_train(ctx, sample, ns, &to, &model))) return fail(rc);
-                rc = pyg_cdf_splitters(ctx, model, Fs, spl.data());
-                pyg_cdf_free(ctx, model);
-                if (rc) return fail(rc);
+                if ((rc = pyg_cdf_train(ctx, sample, ns, &to, &model))) return done(rc);
+                if (fast) {
+                    if ((rc = cdf_bin_model(ctx, model, FBf, &bins)) || (rc = model_splitters(ctx, bins, spl.data())))
+                        return done(rc);
+                    use_bins = true;
+                } else {
+                    rc = pyg_cdf_splitters(ctx, model, Fs, spl.data());
+                    pyg_cdf_free(ctx, model);
+                    model = nullptr;
+                    if (rc) return fail(rc);
+                }
             }
         }
     }
@@ -537,7 +554,9 @@ static int mpsm_run(pyg_ctx* ctx, const pyg_rel* build, int32_t bkey, const pyg_
         unsigned long long o3[3];
         std::vector<unsigned long long> sizes;
         float part_ms = 0.f, join_ms = 0.f;
-        if ((rc = mpsm16_agg(ctx, Ri, nR, Si, nS, spl.data(), FBf, o3, &sizes, &part_ms, &join_ms))) return fail(rc);
+        if ((rc = mpsm16_agg(ctx, Ri, nR, Si, nS, spl.data(), FBf, o3, &sizes, &part_ms, &join_ms,
+                             use_bins ? &bins : nullptr)))
+            return done(rc);
         memset(res, 0, sizeof(*res));
         res->count = (int64_t)o3[0];
         for (int p = 0; p < nproj; ++p) res->sums[p] = (int64_t)(proj[p].side ? o3[2] : o3[1]);
@@ -562,7 +581,7 @@ static int mpsm_run(pyg_ctx* ctx, const pyg_rel* build, int32_t bkey, const pyg_
             stats->sort_ms = 0;  // the sort runs inside the merge kernel
             stats->merge_ms = join_ms;
         }
-        return fail(0);
+        return done(0);
     }
 
     // ---- 2. range partition both sides

@@ -6,7 +6,11 @@
 //                  range holds a few thousand probe tuples.
 //   2. partition   both relations range-partitioned by those splitters with
 //                  the radix operators' bulk-copy partitioner (radixpart.cu,
-//                  splitter-search bins; two passes above 2^8 ranges).
+//                  two passes above 2^8 ranges): splitter-search bins, or,
+//                  for a learned model, the model's own bins (rj_model_bin,
+//                  the same ranges without a search), whose intermediates
+//                  are packed 8-byte words when the key and payload ranges
+//                  allow; the merge decodes them on load.
 //   3. sort+merge  persistent CTAs take (range, build chunk, probe chunk)
 //                  items.  A range whose splitters bound it to at most
 //                  MP16_DSPAN key values is sorted by counting: the build
@@ -51,8 +55,9 @@ struct Mp16Item {
 };
 
 struct Mp16Args {
-    const longlong2* R;
-    const longlong2* S;
+    const void* R;  // 16-byte tuples, or packed 8-byte words (frame rk / rp, sk / sp)
+    const void* S;
+    unsigned long long rk, rp, sk, sp;
     const Mp16Item* items;
     long long nitems;
     unsigned* next;
@@ -60,6 +65,24 @@ struct Mp16Args {
     unsigned* bad;            // a key outside its range's span (never set by a correct partition)
 };
 
+// Element i of a partitioned relation: a 16-byte tuple, or a packed word
+// (key - kb) | (payload - pb) << 32 decoded back to the tuple (exact).
+// CS: a streamed read (evict first).
+template <bool P, bool CS>
+__device__ __forceinline__ longlong2 mp16_elem(const void* base, unsigned long long i, unsigned long long kb,
+                                               unsigned long long pb)
+{
+    if constexpr (P) {
+        const unsigned long long* q = reinterpret_cast<const unsigned long long*>(base) + i;
+        const unsigned long long w = CS ? __ldcs(q) : *q;
+        return make_longlong2((long long)(kb + (w & 0xFFFFFFFFULL)), (long long)(pb + (w >> 32)));
+    } else {
+        const longlong2* q = reinterpret_cast<const longlong2*>(base) + i;
+        return CS ? __ldcs(q) : *q;
+    }
+}
+
+template <bool RP, bool SP>
 __global__ void __launch_bounds__(MP16_THREADS, 2) mp16_join_kernel(Mp16Args a)
 {
     extern __shared__ __align__(16) unsigned char mp16_smem[];
@@ -92,7 +115,7 @@ __global__ void __launch_bounds__(MP16_THREADS, 2) mp16_join_kernel(Mp16Args a)
             __syncthreads();
             bool out_of_span = false;
             for (unsigned i = tid; i < m.rn; i += MP16_THREADS) {
-                const longlong2 t = a.R[m.r0 + i];
+                const longlong2 t = mp16_elem<RP, false>(a.R, m.r0 + i, a.rk, a.rp);
                 const unsigned long long o = (unsigned long long)t.x - (unsigned long long)m.lo;
                 if (o < m.span) {
                     atomicAdd(&bc[o], 1u);
@@ -103,7 +126,6 @@ __global__ void __launch_bounds__(MP16_THREADS, 2) mp16_join_kernel(Mp16Args a)
             }
             if (out_of_span) atomicOr(a.bad, 1u);
             __syncthreads();
-            const longlong2* S = a.S + m.s0;
             auto probe_bin = [&](const longlong2 t) {
                 const unsigned long long o = (unsigned long long)t.x - (unsigned long long)m.lo;
                 if (o >= m.span) return;
@@ -119,11 +141,11 @@ __global__ void __launch_bounds__(MP16_THREADS, 2) mp16_join_kernel(Mp16Args a)
             for (; i + (U - 1) * MP16_THREADS < m.sn; i += U * MP16_THREADS) {
                 longlong2 t[U];
 #pragma unroll
-                for (int u = 0; u < U; ++u) t[u] = __ldcs(&S[i + u * MP16_THREADS]);
+                for (int u = 0; u < U; ++u) t[u] = mp16_elem<SP, true>(a.S, m.s0 + i + u * MP16_THREADS, a.sk, a.sp);
 #pragma unroll
                 for (int u = 0; u < U; ++u) probe_bin(t[u]);
             }
-            for (; i < m.sn; i += MP16_THREADS) probe_bin(__ldcs(&S[i]));
+            for (; i < m.sn; i += MP16_THREADS) probe_bin(mp16_elem<SP, true>(a.S, m.s0 + i, a.sk, a.sp));
             __syncthreads();  // the bins are reused by the next item
             continue;
         }
@@ -135,7 +157,7 @@ __global__ void __launch_bounds__(MP16_THREADS, 2) mp16_join_kernel(Mp16Args a)
             long long k = kPadKey;
             unsigned long long p = 0;
             if (i < (int)m.rn) {
-                const longlong2 t = a.R[m.r0 + i];
+                const longlong2 t = mp16_elem<RP, false>(a.R, m.r0 + i, a.rk, a.rp);
                 if (t.x == kPadKey) {
                     atomicAdd(&side_cnt, 1ULL);
                     atomicAdd(&side_sum, (unsigned long long)t.y);
@@ -202,7 +224,6 @@ __global__ void __launch_bounds__(MP16_THREADS, 2) mp16_join_kernel(Mp16Args a)
         const int rv = (int)m.rn - (int)side_cnt;  // real (non-padding) keys, sorted first
         const uint64_t scnt = side_cnt, ssum = side_sum;
         // Merge the probe chunk into the sorted run.
-        const longlong2* S = a.S + m.s0;
         auto probe = [&](const longlong2 t) {
             if (t.x == kPadKey) {
                 cnt += scnt;
@@ -244,11 +265,11 @@ __global__ void __launch_bounds__(MP16_THREADS, 2) mp16_join_kernel(Mp16Args a)
         for (; i + (U - 1) * MP16_THREADS < m.sn; i += U * MP16_THREADS) {
             longlong2 t[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) t[u] = __ldcs(&S[i + u * MP16_THREADS]);
+            for (int u = 0; u < U; ++u) t[u] = mp16_elem<SP, true>(a.S, m.s0 + i + u * MP16_THREADS, a.sk, a.sp);
 #pragma unroll
             for (int u = 0; u < U; ++u) probe(t[u]);
         }
-        for (; i < m.sn; i += MP16_THREADS) probe(__ldcs(&S[i]));
+        for (; i < m.sn; i += MP16_THREADS) probe(mp16_elem<SP, true>(a.S, m.s0 + i, a.sk, a.sp));
         __syncthreads();  // the run and the side counters are reused by the next item
     }
     cnt = warp_sum_u64(cnt);
@@ -271,7 +292,8 @@ int mpsm16_fine_bits(int64_t nR, int64_t nS)
 }
 
 int mpsm16_agg(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t nS, const int64_t* splitters, int FB,
-               unsigned long long out[3], std::vector<unsigned long long>* sizes, float* part_ms, float* join_ms)
+               unsigned long long out[3], std::vector<unsigned long long>* sizes, float* part_ms, float* join_ms,
+               const RJModel* model)
 {
     const longlong2* R = (const longlong2*)Rv;
     const longlong2* S = (const longlong2*)Sv;
@@ -299,8 +321,30 @@ int mpsm16_agg(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t
         unsigned* flags = (unsigned*)(ctx->dcounters + 208);
         unsigned* hflags = (unsigned*)ctx->pinned + 96;
         RJLayout LR, LS;
-        if ((rc = rp_partition(ctx, R, nR, FB, two, true, cs, fs, LR, &R1, &R2, flags, hflags))) break;
-        if ((rc = rp_partition(ctx, S, nS, FB, two, true, cs, fs, LS, &S1, &S2, flags, hflags))) break;
+        if (model) {
+            // Bins from the model: no splitter search in the histograms or
+            // passes, and both relations' histograms in one round trip.
+            RPSide sd[2];
+            sd[0].in = R;
+            sd[0].n = nR;
+            sd[1].in = S;
+            sd[1].n = nS;
+            sd[0].model = sd[1].model = model;
+            // One bin function for both passes: the intermediates can be
+            // packed words whatever split of bits the passes take.
+            sd[0].allow_pack = sd[1].allow_pack = true;
+            rc = rp_partition_sides(ctx, sd, 2, FB, two, flags, hflags, nullptr);
+            R1 = sd[0].P1;
+            R2 = sd[0].P2;
+            S1 = sd[1].P1;
+            S2 = sd[1].P2;
+            if (rc) break;
+            LR = std::move(sd[0].L);
+            LS = std::move(sd[1].L);
+        } else {
+            if ((rc = rp_partition(ctx, R, nR, FB, two, true, cs, fs, LR, &R1, &R2, flags, hflags))) break;
+            if ((rc = rp_partition(ctx, S, nS, FB, two, true, cs, fs, LS, &S1, &S2, flags, hflags))) break;
+        }
         cudaEventRecord(ev[1], ctx->stream);
         if (sizes) *sizes = LS.count;
         // Items: every (build chunk, probe chunk) pair of each range.  Range
@@ -342,16 +386,22 @@ int mpsm16_agg(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t
             PYG_CUDA(cudaMemcpyAsync(ditems, items.data(), items.size() * sizeof(Mp16Item), cudaMemcpyHostToDevice,
                                      ctx->stream));
             Mp16Args ja;
-            ja.R = (const longlong2*)(two ? R2 : R1);
-            ja.S = (const longlong2*)(two ? S2 : S1);
+            ja.R = two ? R2 : R1;
+            ja.S = two ? S2 : S1;
+            ja.rk = LR.kbase;
+            ja.rp = LR.pbase;
+            ja.sk = LS.kbase;
+            ja.sp = LS.pbase;
             ja.items = ditems;
             ja.nitems = (long long)items.size();
             ja.next = next;
             ja.acc = acc;
             ja.bad = bad;
-            PYG_CUDA(cudaFuncSetAttribute(mp16_join_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MP16_SMEM));
+            auto kern = LR.packed ? (LS.packed ? mp16_join_kernel<true, true> : mp16_join_kernel<true, false>)
+                                  : (LS.packed ? mp16_join_kernel<false, true> : mp16_join_kernel<false, false>);
+            PYG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, MP16_SMEM));
             const unsigned grid = (unsigned)std::min<long long>(2LL * ctx->sm_count, ja.nitems);
-            mp16_join_kernel<<<grid, MP16_THREADS, MP16_SMEM, ctx->stream>>>(ja);
+            kern<<<grid, MP16_THREADS, MP16_SMEM, ctx->stream>>>(ja);
             PYG_LAUNCHED(ctx);
         }
         cudaEventRecord(ev[2], ctx->stream);

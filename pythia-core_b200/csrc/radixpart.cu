@@ -35,14 +35,16 @@ __device__ __forceinline__ unsigned rj_bin(uint64_t h, int shift, unsigned mask)
 // 1. Histogram of the top `bits` hash bits (bits <= 15: 128 KB of shared
 // counters per CTA).
 
+template <bool MODEL>
 __global__ void __launch_bounds__(1024) rj_hist_kernel(const longlong2* __restrict__ in, int64_t n, int64_t step,
                                                        int bits, int base, int span, unsigned* __restrict__ part,
-                                                       long long* __restrict__ mm)
+                                                       long long* __restrict__ mm, RJModel model)
 {
     // Counts the bins [base, base + span) of in[0], in[step], in[2 step],
     // ... (step 1: every tuple); span 32-bit counters in shared memory,
     // stored to this CTA's row of part (rj_hist_sum_kernel adds the rows).
-    // With mm: also the key and payload ranges of the tuples read.
+    // With mm: also the key and payload ranges of the tuples read.  MODEL:
+    // the bins are the learned model's (rj_model_bin) instead of hash bits.
     extern __shared__ unsigned rj_sh_hist[];
     __shared__ long long sh_mm[4];
     const int P = 1 << bits;
@@ -55,7 +57,8 @@ __global__ void __launch_bounds__(1024) rj_hist_kernel(const longlong2* __restri
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     long long kmin = LLONG_MAX, kmax = LLONG_MIN, pmin = LLONG_MAX, pmax = LLONG_MIN;
     auto count = [&](const longlong2 t) {
-        const unsigned r = rj_bin(rj_hash((uint64_t)t.x), shift, P - 1) - (unsigned)base;
+        const uint64_t code = MODEL ? rj_model_code(model, t.x) : rj_hash((uint64_t)t.x);
+        const unsigned r = rj_bin(code, shift, P - 1) - (unsigned)base;
         if (r < (unsigned)span) atomicAdd(&rj_sh_hist[r], 1u);
         kmin = min(kmin, t.x);
         kmax = max(kmax, t.x);
@@ -165,6 +168,9 @@ struct RJPass {
     // 16-byte input tuple falls outside it.
     unsigned long long kbase, pbase;
     unsigned* frame;
+    // Model mode (the kernel's MODEL instances): the bin bits come from the
+    // learned model's code (rj_model_code) instead of the key's hash.
+    RJModel model;
 };
 
 // Element formats: a pass reads 16-byte tuples (the relation, or unpacked
@@ -295,7 +301,7 @@ __device__ __forceinline__ void rj_issue_tile(const RJPass& a, RJPartSmem<IN8, O
     bulk_load(sm.in[slot], reinterpret_cast<const typename F::In*>(a.in) + r.begin, bytes, &sm.bar[slot]);
 }
 
-template <bool IN8, bool OUT8>
+template <bool IN8, bool OUT8, bool MODEL>
 __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_kernel(RJPass a, long long ntiles)
 {
     using F = RJFmt<IN8, OUT8>;
@@ -352,8 +358,11 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
                     miss |= ((dk | dp) >> 32) != 0;
                     t[j] = (dk & 0xFFFFFFFFULL) | (dp << 32);
                 }
-                bin[j] = a.nsplit ? rj_range_bin(sm.split[a.nseg > 1 ? (k & 1) : 0], a.nsplit, key)
-                                  : rj_bin(rj_hash((uint64_t)key), a.shift, a.mask);
+                if constexpr (MODEL)
+                    bin[j] = rj_bin(rj_model_code(a.model, key), a.shift, a.mask);
+                else
+                    bin[j] = a.nsplit ? rj_range_bin(sm.split[a.nseg > 1 ? (k & 1) : 0], a.nsplit, key)
+                                      : rj_bin(rj_hash((uint64_t)key), a.shift, a.mask);
             }
             // Skewed keys put many lanes of a warp into one bin: when at
             // least 8 lanes share lane 0's bin, they take their ranks from
@@ -451,10 +460,10 @@ __global__ void __launch_bounds__(RJ_PT_THREADS, PYG_RJ_PT_MINB) rj_partition_ke
 
 namespace {
 
-template <bool IN8, bool OUT8>
+template <bool IN8, bool OUT8, bool MODEL>
 int launch_pass_t(pyg_ctx* ctx, const RJPass& p, long long ntiles)
 {
-    auto fn = rj_partition_kernel<IN8, OUT8>;
+    auto fn = rj_partition_kernel<IN8, OUT8, MODEL>;
     const size_t smem = sizeof(RJPartSmem<IN8, OUT8>);
     PYG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -471,9 +480,14 @@ int launch_pass_t(pyg_ctx* ctx, const RJPass& p, long long ntiles)
 int launch_pass(pyg_ctx* ctx, const RJPass& p, long long ntiles, bool in8, bool out8)
 {
     if (ntiles <= 0) return PYG_OK;
-    if (in8) return launch_pass_t<true, true>(ctx, p, ntiles);
-    if (out8) return launch_pass_t<false, true>(ctx, p, ntiles);
-    return launch_pass_t<false, false>(ctx, p, ntiles);
+    if (p.model.leaf) {
+        if (in8) return launch_pass_t<true, true, true>(ctx, p, ntiles);
+        if (out8) return launch_pass_t<false, true, true>(ctx, p, ntiles);
+        return launch_pass_t<false, false, true>(ctx, p, ntiles);
+    }
+    if (in8) return launch_pass_t<true, true, false>(ctx, p, ntiles);
+    if (out8) return launch_pass_t<false, true, false>(ctx, p, ntiles);
+    return launch_pass_t<false, false, false>(ctx, p, ntiles);
 }
 
 // Host-side layout of one relation's partitions.  Exact layouts come from a
@@ -606,7 +620,7 @@ int upload_layout(pyg_ctx* ctx, const RJLayout& L, const RJSideDev& d, int F, in
 // Runs the partition pass(es) of one relation into P1 (and P2).
 int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, const RJSideDev& d, bool two, int FB,
                int CB, void* P1, void* P2, unsigned* err, unsigned* ovf, const long long* csplit,
-               const long long* fsplit, unsigned* frame, cudaEvent_t between)
+               const long long* fsplit, unsigned* frame, cudaEvent_t between, const RJModel* model)
 {
     const int C = 1 << CB, sub = FB - CB;
     if (L.packed && (!frame || csplit || (two && sub > 8))) {
@@ -631,6 +645,7 @@ int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, 
     p.kbase = L.kbase;
     p.pbase = L.pbase;
     p.frame = frame;
+    if (model) p.model = *model;
     if (csplit) {
         p.split = csplit;
         p.nsplit = C - 1;
@@ -670,14 +685,16 @@ int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, 
 }
 
 int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int FB, unsigned long long* hist,
-                long long* mm)
+                long long* mm, const RJModel* model)
 {
     // At most 2^15 counters (128 KB) per launch: 2^16 bins take two.
     const int F = 1 << FB, span = F < (1 << 15) ? F : (1 << 15);
     const size_t hsm = (size_t)4 * span;
-    PYG_CUDA(cudaFuncSetAttribute(rj_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
+    auto kern = model ? rj_hist_kernel<true> : rj_hist_kernel<false>;
+    const RJModel none;
+    PYG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
     int per = 0;
-    PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rj_hist_kernel, 1024, hsm));
+    PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 1024, hsm));
     if (per < 1) per = 1;
     const int64_t m = (n + step - 1) / step;
     const int64_t want = (m + 1024 * 8 - 1) / (1024 * 8);
@@ -691,7 +708,8 @@ int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int 
     }
     for (int base = 0; base < F; base += span) {
         // The key and payload ranges are taken in the first launch only.
-        rj_hist_kernel<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, FB, base, span, part, base ? nullptr : mm);
+        kern<<<grid, 1024, hsm, ctx->stream>>>(in, n, step, FB, base, span, part, base ? nullptr : mm,
+                                                model ? *model : none);
         PYG_LAUNCHED(ctx);
         rj_hist_sum_kernel<<<(span + 255) / 256, 256, 0, ctx->stream>>>(part, grid, span, hist + base);
         PYG_LAUNCHED(ctx);
@@ -757,7 +775,7 @@ int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsig
             return hist_launch_range(ctx, sd[s].in, sd[s].n, st, cb, FB - cb, sd[s].csplit, sd[s].fsplit, hist_at(s));
         }
         return hist_launch(ctx, sd[s].in, sd[s].n, st, FB, hist_at(s),
-                           sd[s].allow_pack ? (long long*)(hist_at(s) + F) : nullptr);
+                           sd[s].allow_pack ? (long long*)(hist_at(s) + F) : nullptr, sd[s].model);
     };
     // Layout of relation s from host counts h (F counts, then the key and
     // payload ranges): packed when the caller allows it and a frame fits.
@@ -784,7 +802,8 @@ int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsig
         if (two && (r = dalloc(ctx, &sd[s].P2, pass_bytes(L, L.p2)))) return r;
         if (sd[s].begin) cudaEventRecord(sd[s].begin, ctx->stream);
         if ((r = run_passes(ctx, sd[s].in, sd[s].n, L, d[s], two, FB, CBs[s], sd[s].P1, sd[s].P2, flags + 4 * s,
-                            flags + 4 * s + 1, sd[s].csplit, sd[s].fsplit, flags + 4 * s + 2, sd[s].mid)))
+                            flags + 4 * s + 1, sd[s].csplit, sd[s].fsplit, flags + 4 * s + 2, sd[s].mid,
+                            sd[s].model)))
             return r;
         if (sd[s].done) cudaEventRecord(sd[s].done, ctx->stream);
         return PYG_OK;

@@ -30,6 +30,8 @@
 
 #include "pyg_internal.cuh"
 
+typedef struct pyg_cdf pyg_cdf;
+
 namespace pyg {
 
 #ifndef PYG_RJ_TILE
@@ -55,6 +57,72 @@ constexpr int RJ_MAX_RANGE_BITS = 15;  // range mode (one 2^15-counter histogram
 // at most 0.2 ms for two relations; regions get more slack than with a
 // larger sample, which costs device memory, not traffic).
 constexpr int RJ_SAMPLE_LOG2 = PYG_RJ_SAMPLE_LOG2;
+
+// Partition bins computed by a learned CDF model instead of a search
+// (range partitioning without splitters in the passes).  For a model with
+// L leaves over keys (kmin, kmax) and 2^fbits bins:
+//   x = (float)(((double)k - key_lo) * key_scale)     normalised key
+//   r = a0 x + b0, l = clamp(floor(L r), 0, L - 1)     root line -> leaf
+//   u = clamp(L r - l, 0, 1)                           leaf-local coordinate
+//   t = clamp(slope_l u + icpt_l, 0, 1)
+//   g = min(base_l + span_l t + (heavy keys of leaf l below k), top_l)
+//   bin(k) = min(2^fbits - 1, trunc(g 2^fbits))
+// with bin 0 for k <= kmin and the last bin for k >= kmax.  Every step is a
+// correctly rounded fp32 / fp64 operation that does not decrease when its
+// input grows (slopes, spans and masses are >= 0), and top_l <= base_{l+1},
+// so bin(k) never decreases with k: the bins are key ranges, and their
+// splitters (the first key of each bin, found by bisection over the same
+// function) reproduce them exactly.  The model's accuracy only decides how
+// even the bins are.
+struct RJLeaf {
+    float base, span, slope, icpt;  // g = base + span * t
+    float top;                      // the leaf's largest g
+    int h0, hn;                     // heavy keys of the leaf: hkey[h0 .. h0 + hn)
+    int pad;
+};
+struct RJModel {
+    const RJLeaf* leaf = nullptr;  // device, L leaves (null: no model)
+    const long long* hkey = nullptr;  // device, heavy keys ascending
+    const float* hw = nullptr;        // device, their masses
+    double key_lo = 0, key_scale = 0;
+    long long kmin = 0, kmax = 0;
+    float a0 = 0, b0 = 0;
+    int L = 0;
+    int fbits = 0;
+};
+
+__device__ __forceinline__ unsigned rj_model_bin(const RJModel& m, long long k)
+{
+    const unsigned last = (1u << m.fbits) - 1u;
+    if (k <= m.kmin) return 0u;
+    if (k >= m.kmax) return last;
+    const float x = __double2float_rn(__dmul_rn(__dsub_rn((double)k, m.key_lo), m.key_scale));
+    const float lr = __fmul_rn(__fmaf_rn(m.a0, x, m.b0), (float)m.L);
+    const float fl = floorf(lr);
+    int l = fl < 0.f ? 0 : (fl > (float)(m.L - 1) ? m.L - 1 : (int)fl);
+    const float u = fminf(1.f, fmaxf(0.f, __fsub_rn(lr, (float)l)));
+    const RJLeaf p = m.leaf[l];
+    const float t = fminf(1.f, fmaxf(0.f, __fmaf_rn(p.slope, u, p.icpt)));
+    float g = __fmaf_rn(p.span, t, p.base);
+    for (int h = p.h0; h < p.h0 + p.hn && m.hkey[h] < k; ++h) g = __fadd_rn(g, m.hw[h]);
+    g = fminf(g, p.top);
+    const float b = __fmul_rn(g, (float)(1u << m.fbits));
+    return b >= (float)last ? last : (unsigned)b;
+}
+
+// Bins of a trained CDF model (cdf.cu): *out refers to device tables the
+// model keeps until pyg_cdf_free.  model_splitters: the 2^fbits - 1
+// splitters of those bins into host array out (bin(k) = number of
+// splitters <= k).
+int cdf_bin_model(pyg_ctx* ctx, const pyg_cdf* m, int fbits, RJModel* out);
+int model_splitters(pyg_ctx* ctx, const RJModel& m, int64_t* out);
+
+// The 64-bit code whose top fbits bits are the model's bin (the hash
+// operators take their partition bits from the top of such a word).
+__device__ __forceinline__ uint64_t rj_model_code(const RJModel& m, long long k)
+{
+    return (uint64_t)rj_model_bin(m, k) << (64 - m.fbits);
+}
 
 // Host-side layout of one relation's partitions.
 struct RJLayout {
@@ -121,7 +189,7 @@ int upload_layout(pyg_ctx* ctx, const RJLayout& L, const RJSideDev& d, int F, in
 // minimum and maximum key and payload of the tuples read, as signed
 // {kmin, kmax, pmin, pmax}.
 int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int FB, unsigned long long* hist,
-                long long* mm = nullptr);
+                long long* mm = nullptr, const RJModel* model = nullptr);
 // Partition pass(es) of one relation into P1 (and P2 when two): *err is set
 // if a tile's bulk copy never landed, *ovf if a sampled region overflowed,
 // *frame if a tuple fell outside a packed layout's frame.  Afterwards
@@ -131,7 +199,8 @@ int hist_launch(pyg_ctx* ctx, const longlong2* in, int64_t n, int64_t step, int 
 // splitter i = fine splitter (i + 1) * 2^(FB - CB) - 1).
 int run_passes(pyg_ctx* ctx, const longlong2* in, int64_t n, const RJLayout& L, const RJSideDev& d, bool two, int FB,
                int CB, void* P1, void* P2, unsigned* err, unsigned* ovf, const long long* csplit = nullptr,
-               const long long* fsplit = nullptr, unsigned* frame = nullptr, cudaEvent_t between = nullptr);
+               const long long* fsplit = nullptr, unsigned* frame = nullptr, cudaEvent_t between = nullptr,
+               const RJModel* model = nullptr);
 // Device bytes of a layout's pass buffers (packed buffers get 16 bytes of
 // tail so that the last tile's 16-byte-rounded copy stays inside).
 inline size_t pass_bytes(const RJLayout& L, unsigned long long words)
@@ -153,6 +222,9 @@ struct RPSide {
     bool allow_pack = false;  // the caller reads packed intermediates (L.packed tells)
     const long long* csplit = nullptr;
     const long long* fsplit = nullptr;
+    // Learned-model bins (rj_model_bin) instead of hash bits; model->fbits
+    // must equal the partition bits.
+    const RJModel* model = nullptr;
     cudaEvent_t begin = nullptr;  // recorded before the first pass (optional)
     cudaEvent_t mid = nullptr;    // between the two passes (optional)
     cudaEvent_t done = nullptr;

@@ -13,6 +13,7 @@ device.  Cases and the kernels they launch:
   radix      R 2^24 x S 2^27 PK-FK radix join      rj_hist, rj_partition, rj_join
   direct     R 2^20 x S 2^24 join, one HBM table    dj_clear, dj_build, dj_probe
   groupby16  2^26 (int64, int64), G = 16 / 1024 / 2^16   gbr_tiny / gbr_direct / gbr_part
+  groupby-zipf  2^26 tuples, G = 2^16, Zipf(1.0) ids     rj_hist, rj_partition, gbr_part
   composite  2^25 (int32, int32, int64), G = 2^16    groupby_kernel
   partition  2^25 tuples, exactrange, fan-out 64     pt_hist, pt_scatter
   sort       2^24 tuples                            rs_hist, rs_scatter
@@ -67,6 +68,19 @@ def case_groupby16(torch, ctx, a):
         for _ in range(a.reps):
             rc, g = ctx.groupby(pyg.Rel(A, n, [I64, I64]), [0], 3, 1, True, G, out, G)
             assert rc == 0 and int(out[: 3 * g].view(g, 3)[:, 2].sum().item()) == n
+
+
+def case_groupby_zipf(torch, ctx, a):
+    """2^26 (int64 id, int64 value), ids Zipf(1.0) over G = 2^16."""
+    n, G = (1 << 26) >> a.shift, 1 << 16
+    w = torch.arange(1, G + 1, dtype=torch.float64, device="cuda").pow(-1.0)
+    ids = torch.cat([torch.multinomial(w / w.sum(), min(n, 1 << 24), replacement=True)
+                     for _ in range(max(1, n >> 24))])[:n]
+    A = torch.stack([ids, torch.randint(0, 1 << 20, (n,), device="cuda")], 1).contiguous().view(-1)
+    out = torch.empty(G * 3, dtype=torch.int64, device="cuda")
+    for _ in range(a.reps):
+        rc, g = ctx.groupby(pyg.Rel(A, n, [I64, I64]), [0], 3, 1, True, G, out, G)
+        assert rc == 0 and int(out[: 3 * g].view(g, 3)[:, 2].sum().item()) == n
 
 
 def case_composite(torch, ctx, a):
@@ -156,7 +170,7 @@ def case_batch(torch, ctx, a):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["radix", "direct", "groupby16", "composite", "partition", "sort", "mpsm",
+    ap.add_argument("case", choices=["radix", "direct", "groupby16", "groupby-zipf", "composite", "partition", "sort", "mpsm",
                                      "mpsm-mat", "cdf", "batch"])
     ap.add_argument("--shift", type=int, default=0, help="shrink the inputs by 2^shift")
     ap.add_argument("--reps", type=int, default=2)
@@ -174,6 +188,8 @@ def main():
             case_join(torch, ctx, a, pyg.JOIN_DIRECT, (1 << 20) >> a.shift, (1 << 24) >> a.shift)
         elif a.case == "groupby16":
             case_groupby16(torch, ctx, a)
+        elif a.case == "groupby-zipf":
+            case_groupby_zipf(torch, ctx, a)
         elif a.case == "composite":
             case_composite(torch, ctx, a)
         elif a.case == "partition":

@@ -166,6 +166,8 @@ SIGNATURES = [
     ("pyg_cdf_free", C.c_int, [_P, _P]),
     ("pyg_cdf_splitters", C.c_int, [_P, _P, _I32, _PI64]),
     ("pyg_cdf_predict", C.c_int, [_P, _P, _P, _I64, _P]),
+    ("pyg_cdf_bins", C.c_int, [_P, _P, _I32, _P, _I64, _P]),
+    ("pyg_cdf_bin_splitters", C.c_int, [_P, _P, _I32, C.POINTER(C.c_int64)]),
     ("pyg_cdf_params", C.c_int, [_P, _P, C.POINTER(C.c_float), _I32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("pyg_cdf_loss_grad", C.c_int, [_P, _P, _I64, _I32, C.POINTER(C.c_float), C.c_double, C.c_double,
                                     C.POINTER(C.c_double), C.POINTER(C.c_float)]),

@@ -161,3 +161,74 @@ def test_learned_vs_sampled_splitters_on_mpsm_join(ctx, torch_cuda, theta):
     assert res[pyg.MPSM_LEARNED][0] == nS
     assert res[pyg.MPSM_LEARNED][2] <= 1.05 * res[pyg.MPSM_SAMPLED][2] + 0.1
     assert res[pyg.MPSM_LEARNED][3] < 5.0, res
+
+
+def model_bins(ctx, torch, model, fbits, keys):
+    d = torch.from_numpy(np.ascontiguousarray(keys)).cuda()
+    out = torch.empty(max(1, keys.shape[0]), dtype=torch.int32, device="cuda")
+    pyg.check(pyg.lib().pyg_cdf_bins(ctx.h, model, fbits, d.data_ptr(), keys.shape[0], out.data_ptr()))
+    ctx.sync()
+    return out[: keys.shape[0]].cpu().numpy().view(np.uint32)
+
+
+def model_bin_splitters(ctx, model, fbits):
+    out = np.zeros((1 << fbits) - 1, dtype=np.int64)
+    pyg.check(pyg.lib().pyg_cdf_bin_splitters(ctx.h, model, fbits, out.ctypes.data_as(C.POINTER(C.c_int64))))
+    return out
+
+
+def bin_sample(rng, dist):
+    mn, mx = np.iinfo(np.int64).min, np.iinfo(np.int64).max
+    if dist == "dense":
+        return rng.permutation(1 << 20)[: 1 << 16].astype(np.int64) + 1
+    if dist == "zipf":  # heavy keys scattered over a permuted domain
+        return zipf_sample(rng, 1 << 17, 1 << 20, 1.2, rng.permutation(1 << 20).astype(np.int64) * 5)
+    if dist == "wide":
+        return rng.integers(-(1 << 62), 1 << 62, 1 << 16)
+    if dist == "heavy":  # one key holds half the sample
+        k = rng.integers(0, 1 << 30, 1 << 16)
+        k[::2] = 777
+        return k
+    if dist == "tiny":
+        return np.array([9, -3, 100, 4, 4], dtype=np.int64)
+    if dist == "equal":
+        return np.full(1000, 42, dtype=np.int64)
+    # extremes: both ends of the int64 range in the sample
+    k = rng.integers(-1000, 1000, 5000)
+    k[:3] = [mn, mx, mn]
+    return k
+
+
+@pytest.mark.parametrize("fbits", [1, 7, 15])
+@pytest.mark.parametrize("dist", ["dense", "zipf", "wide", "heavy", "tiny", "equal", "extremes"])
+def test_model_bins_equal_a_search_of_their_splitters(ctx, torch_cuda, dist, fbits):
+    """The MPSM join's learned partitioning computes each key's range from
+    the model (pyg_cdf_bins) instead of searching splitters.  It must place
+    every key exactly where a search of the model's splitters
+    (pyg_cdf_bin_splitters) places it -- bin(k) = number of splitters <= k,
+    the rule of the splitter-search path -- for the sample, its neighbours,
+    keys outside the sample's range and the int64 extremes."""
+    rng = np.random.default_rng(fbits * 7 + len(dist))
+    sample = bin_sample(rng, dist).astype(np.int64)
+    model = train(ctx, torch_cuda, sample, leaves=1024, epochs=1, lr=0.002)
+    try:
+        mn, mx = np.iinfo(np.int64).min, np.iinfo(np.int64).max
+        lo, hi = int(sample.min()), int(sample.max())
+        probe = [sample, np.array([mn, mx, mn + 1, mx - 1, 0, -1, 1], dtype=np.int64),
+                 np.array([v for v in (lo - 1, lo, lo + 1, hi - 1, hi, hi + 1) if mn <= v <= mx], dtype=np.int64)]
+        sub = sample[: 1 << 14]
+        probe += [sub[sub < mx] + 1, sub[sub > mn] - 1]
+        if hi - lo > 2:
+            probe.append(rng.integers(lo, hi, 1 << 16, dtype=np.int64, endpoint=True))
+        keys = np.concatenate(probe)
+        spl = model_bin_splitters(ctx, model, fbits)
+        assert np.all(np.diff(spl) >= 0)
+        got = model_bins(ctx, torch_cuda, model, fbits, keys)
+        want = np.searchsorted(spl, keys, side="right")
+        assert np.array_equal(got, want), np.nonzero(got != want)[0][:10]
+        if dist == "dense" and fbits == 7:
+            # a model of a dense key range spreads the sample evenly
+            counts = np.bincount(model_bins(ctx, torch_cuda, model, fbits, sample), minlength=1 << fbits)
+            assert counts.max() <= 1.5 * sample.shape[0] / (1 << fbits)
+    finally:
+        pyg.lib().pyg_cdf_free(ctx.h, model)
