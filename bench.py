@@ -479,7 +479,9 @@ def join_roofline(pyg, phase, nR, nS, step_ms, hbm, peak_kind, theta):
                                              packed)
         eR = 8 if int(phase[0].build_packed) else 16
         eS = 8 if int(phase[0].probe_packed) else 16
-        launches["join"] = ("rj_join_kernel", mean("probe_ms"), (nR + nS) * 16, nR * eR + nS * eS, None)
+        jk = mean("join_kernel_ms")
+        launches["join"] = ("rj_join32_kernel" if jk > 0 else "rj_join_kernel", jk if jk > 0 else mean("probe_ms"),
+                            (nR + nS) * 16, nR * eR + nS * eS, None)
     else:
         launches["build"] = ("ht_build16_kernel", mean("build_ms"), nR * 16, nR * 16, None)
         launches["probe"] = ("probe_agg16_kernel", mean("probe_ms"), nS * 16, nS * 16, None)
@@ -499,6 +501,12 @@ def join_roofline(pyg, phase, nR, nS, step_ms, hbm, peak_kind, theta):
                 "launches": ph, "algorithm": int(phase[0].algorithm), "radix_bits": int(phase[0].radix_bits),
                 "histogram_ms": round(mean("histogram_ms"), 3) if radix else None,
                 "histogram_tuples": int(phase[0].histogram_tuples) if radix else None,
+                # Host round trips inside the step: the layouts formed from the
+                # histograms (before the build side's passes), and the work
+                # items formed from the partition counts (before the join).
+                "host_layout_ms": round(mean("build_partition_ms") - mean2("build_pass_ms", 0)
+                                        - mean2("build_pass_ms", 1), 3) if radix else None,
+                "host_items_ms": round(mean("probe_ms") - mean("join_kernel_ms"), 3) if radix else None,
                 "step_achieved_gbs": round(step_bytes / (step_ms / 1e3) / 1e9, 1),
                 "step_frac": round(step_bytes / (step_ms / 1e3) / 1e9 / hbm, 4)}
     # DRAM traffic of the dominant launch from an ncu capture of the same

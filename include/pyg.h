@@ -201,6 +201,9 @@ typedef struct pyg_join_stats {
     double probe_pass_ms[2];
     int32_t build_packed;       /* 8-byte packed intermediates (RADIX)  */
     int32_t probe_packed;
+    /* RADIX: the join kernel alone; probe_ms also holds the host round trip
+     * that reads the partition counts and uploads the work items. */
+    double join_kernel_ms;
 } pyg_join_stats;
 
 int pyg_hashjoin_agg(pyg_ctx* ctx, const pyg_rel* build, const int32_t* build_keys,

@@ -49,6 +49,7 @@ struct pyg_cdf {
     // Device tables of the model's own bins (pyg::cdf_bin_model), built on
     // first use: L leaves, then the heavy keys and their masses.
     mutable pyg::RJLeaf* d_bleaf = nullptr;
+    mutable int2* d_bhinfo = nullptr;
     mutable long long* d_bhkey = nullptr;
     mutable float* d_bhw = nullptr;
 };
@@ -857,11 +858,18 @@ __global__ void cdf_split_kernel(SplitArgs a)
 // The model's own bins (rj_model_bin): partitions computed from the key by
 // the model instead of searched among splitters.
 
+// Normalisation of the model's bins: x = (float)(k - kmin) * scale.
+static float bin_scale(const pyg_cdf* m)
+{
+    const double s = m->key_scale;
+    return std::isfinite(s) && s > 0 ? (float)s : 0.f;
+}
+
 // Leaf of key k on the host, with the device's operations (correctly
-// rounded fp64 / fp32 steps give the same results on both sides).
+// rounded fp32 steps give the same results on both sides).
 static int bin_leaf_host(const pyg_cdf* m, int64_t k)
 {
-    const float x = (float)(((double)k - m->key_lo) * m->key_scale);
+    const float x = (float)((unsigned long long)k - (unsigned long long)m->kmin) * bin_scale(m);
     const float lr = fmaf(m->a0, x, m->b0) * (float)m->L;
     const float fl = floorf(lr);
     return fl < 0.f ? 0 : (fl > (float)(m->L - 1) ? m->L - 1 : (int)fl);
@@ -875,69 +883,71 @@ int cdf_bin_model(pyg_ctx* ctx, const pyg_cdf* m, int fbits, RJModel* out)
     }
     const int L = m->L, H = (int)m->heavy_key.size();
     if (!m->d_bleaf) {
-        // g = base_l + span_l t (+ the leaf's heavy masses below the key),
-        // capped at top_l; base_{l+1} >= top_l keeps bins ordered across
-        // leaves.  The heavy masses below a leaf are part of its base.
+        // Leaf l's line over u: g = base + span * clamp(slope u + icpt, 0,
+        // 1), as A u + B clamped to [base, base + span]; its heavy keys
+        // add their masses above that, capped at hi_l.  The heavy masses
+        // below a leaf are part of its base, and lo_{l+1} >= hi_l keeps the
+        // bins ordered across leaves.
         const double cont = 1.0 - m->wheavy;
         std::vector<RJLeaf> lv(L);
+        std::vector<int2> hinfo(L);
         std::vector<float> hw(H);
         int h = 0;
         double below = 0.0;  // heavy mass of the leaves so far
-        float prev_top = 0.f;
+        float prev_hi = 0.f;
         for (int l = 0; l < L; ++l) {
             RJLeaf& p = lv[l];
             const double ylo = m->ylo[l], yhi = m->yhi[l];
             const bool ok = std::isfinite(ylo) && std::isfinite(yhi) && yhi > ylo;
-            p.base = std::max(prev_top, (float)(cont * (ok ? ylo : 0.0) + below));
-            p.span = ok ? (float)(cont * (yhi - ylo)) : 0.f;
-            p.slope = std::isfinite(m->la[l]) ? std::max(0.f, m->la[l]) : 0.f;
-            p.icpt = std::isfinite(m->lb[l]) ? m->lb[l] : 0.f;
-            p.h0 = h;
-            float top = fmaf(p.span, 1.f, p.base);
+            const float base = std::max(prev_hi, (float)(cont * (ok ? ylo : 0.0) + below));
+            const float span = ok ? (float)(cont * (yhi - ylo)) : 0.f;
+            const float slope = std::isfinite(m->la[l]) ? std::max(0.f, m->la[l]) : 0.f;
+            const float icpt = std::isfinite(m->lb[l]) ? m->lb[l] : 0.f;
+            p.A = span * slope;
+            p.B = base + span * icpt;
+            p.lo = base;
+            float top = base + span;
+            hinfo[l].x = h;
             while (h < H && bin_leaf_host(m, m->heavy_key[h]) <= l) {
                 hw[h] = (float)m->heavy_w[h];
                 top = top + hw[h];
                 below += m->heavy_w[h];
                 ++h;
             }
-            p.hn = h - p.h0;
-            p.top = top;
-            p.pad = 0;
-            prev_top = top;
+            hinfo[l].y = h - hinfo[l].x;
+            p.hi = std::max(top, base);
+            prev_hi = p.hi;
         }
         char* buf = nullptr;
-        const size_t bytes = (size_t)L * sizeof(RJLeaf) + (size_t)H * 8 + (size_t)H * 4 + 16;
+        const size_t bytes = (size_t)L * sizeof(RJLeaf) + (size_t)L * sizeof(int2) + (size_t)H * 8 + (size_t)H * 4 + 16;
         int rc = dalloc(ctx, (void**)&buf, bytes);
         if (rc) return rc;
         m->d_bleaf = (RJLeaf*)buf;
-        m->d_bhkey = (long long*)(buf + (size_t)L * sizeof(RJLeaf));
+        m->d_bhinfo = (int2*)(m->d_bleaf + L);
+        m->d_bhkey = (long long*)(m->d_bhinfo + L);
         m->d_bhw = (float*)(m->d_bhkey + H);
-        PYG_CUDA(cudaMemcpyAsync(m->d_bleaf, lv.data(), (size_t)L * sizeof(RJLeaf), cudaMemcpyHostToDevice,
-                                 ctx->stream));
+        if ((rc = stage_h2d(ctx, m->d_bleaf, lv.data(), (size_t)L * sizeof(RJLeaf)))) return rc;
         if (H) {
-            PYG_CUDA(cudaMemcpyAsync(m->d_bhkey, m->heavy_key.data(), (size_t)H * 8, cudaMemcpyHostToDevice,
-                                     ctx->stream));
-            PYG_CUDA(cudaMemcpyAsync(m->d_bhw, hw.data(), (size_t)H * 4, cudaMemcpyHostToDevice, ctx->stream));
+            if ((rc = stage_h2d(ctx, m->d_bhinfo, hinfo.data(), (size_t)L * sizeof(int2)))) return rc;
+            if ((rc = stage_h2d(ctx, m->d_bhkey, m->heavy_key.data(), (size_t)H * 8))) return rc;
+            if ((rc = stage_h2d(ctx, m->d_bhw, hw.data(), (size_t)H * 4))) return rc;
         }
-        // The staged host vectors must outlive the copies.
-        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
     }
     RJModel r;
     r.leaf = m->d_bleaf;
+    r.hinfo = H ? m->d_bhinfo : nullptr;
     r.hkey = m->d_bhkey;
     r.hw = m->d_bhw;
-    r.key_lo = m->key_lo;
-    // A sample of one key value has no scale: every key then has x = 0 (a
-    // constant is monotone too; the bins hold keys below, at and above it).
-    r.key_scale = std::isfinite(m->key_scale) && m->key_scale > 0 ? m->key_scale : 0.0;
     r.kmin = m->kmin;
     r.kmax = m->kmax;
     // Bin 0 holds the keys <= kmin and the last bin those >= kmax; keep
-    // kmin < kmax so that both ends exist.
+    // kmin < kmax so that both ends exist.  A sample of one key value has
+    // no scale: x = 0 for every key then (a constant is monotone too).
     if (r.kmax <= r.kmin) {
         if (r.kmin < INT64_MAX) r.kmax = r.kmin + 1;
         else r.kmin = r.kmax - 1;
     }
+    r.scale = bin_scale(m);
     r.a0 = std::max(0.f, m->a0);
     r.b0 = m->b0;
     r.L = L;

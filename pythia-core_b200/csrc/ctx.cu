@@ -61,6 +61,25 @@ int check_rel(const pyg_rel* r, const char* name)
     return PYG_OK;
 }
 
+int stage_h2d(pyg_ctx* ctx, void* dst, const void* src, size_t bytes)
+{
+    if (bytes == 0) return PYG_OK;
+    if (bytes > kPinnedUploadBytes) {
+        PYG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        return PYG_OK;
+    }
+    size_t at = (ctx->up_cursor + 255) & ~(size_t)255;
+    if (at + bytes > kPinnedUploadBytes) {
+        PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        at = 0;
+    }
+    unsigned char* area = (unsigned char*)ctx->pinned + kPinnedScalarBytes + kPinnedStageBytes;
+    memcpy(area + at, src, bytes);
+    ctx->up_cursor = at + bytes;
+    PYG_CUDA(cudaMemcpyAsync(dst, area + at, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    return PYG_OK;
+}
+
 int dalloc(pyg_ctx* ctx, void** p, size_t bytes)
 {
     *p = nullptr;
@@ -174,7 +193,7 @@ int pyg_ctx_create(int device, pyg_ctx** out)
         return cuda_status(e, "cudaStreamCreate");
     }
     c->stream = c->own_stream;
-    c->pinned_bytes = kPinnedScalarBytes + kPinnedStageBytes;
+    c->pinned_bytes = kPinnedScalarBytes + kPinnedStageBytes + kPinnedUploadBytes;
     e = cudaMallocHost(&c->pinned, c->pinned_bytes);
     if (e == cudaSuccess) e = cudaMalloc((void**)&c->dcounters, 4096);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);

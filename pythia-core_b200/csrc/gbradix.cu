@@ -100,6 +100,25 @@ __device__ __forceinline__ bool gbr_fold(const GbrTable& t, uint64_t k, uint64_t
     return false;
 }
 
+// Folds (sum, cnt) for key k into the shared table, else into the HBM
+// table; false if both are full.
+__device__ __forceinline__ bool gbr_fold_n(const GbrArgs& a, const GbrTable& t, uint64_t k, uint64_t sum, unsigned cnt,
+                                           unsigned long long& fresh)
+{
+    unsigned pos = rj_slot(k, a.fine_bits, GBR_SLOTS);
+    for (unsigned steps = 0; steps < GBR_SLOTS; ++steps) {
+        unsigned long long prev = t.key[pos];
+        if (prev == kEmptyKey) prev = atomicCAS(&t.key[pos], kEmptyKey, (unsigned long long)k);
+        if (prev == kEmptyKey || prev == k) {
+            if (a.want_sum) atomicAdd(&t.sum[pos], (unsigned long long)sum);
+            atomicAdd(&t.cnt[pos], cnt);
+            return true;
+        }
+        pos = pos + 1 == GBR_SLOTS ? 0 : pos + 1;
+    }
+    return gbr_global_add(a, k, sum, cnt, fresh);
+}
+
 // Folds tuples [0, n) of p into the shared table.
 // Lane combining in gbr_fold_range: never, always, or adaptive (a warp
 // stops combining after four batches in a row whose rounds found no key
@@ -114,6 +133,13 @@ __device__ void gbr_fold_range(const GbrArgs& a, const GbrTable& t, const longlo
     const int lane = threadIdx.x & 31;
     bool comb = MODE != kFoldPlain, hit = false;
     int cool = 0, miss = 0;
+    // The warp's hot key: combined groups of it are added to these
+    // registers (the same values in every lane) instead of the shared
+    // table, where every warp's groups of that key would meet on one slot;
+    // they are folded in when another key of a large group takes its
+    // place, and at the end.
+    uint64_t hot_k = kEmptyKey, hot_s = 0;
+    unsigned hot_c = 0;
     // While combining, the lanes holding the key of a leader lane are combined
     // with one shuffle reduction and folded once, for up to two leaders per
     // warp; each round takes the larger key group of two candidates (the
@@ -145,20 +171,17 @@ __device__ void gbr_fold_range(const GbrArgs& a, const GbrTable& t, const longlo
             uint64_t sv = ((m >> lane) & 1) ? v : 0;
 #pragma unroll
             for (int o = 16; o; o >>= 1) sv += __shfl_xor_sync(0xffffffffu, sv, o);
-            if (lane == leader) {
-                unsigned pos = rj_slot(kl, a.fine_bits, GBR_SLOTS);
-                bool done = false;
-                for (unsigned steps = 0; steps < GBR_SLOTS && !done; ++steps) {
-                    unsigned long long prev = t.key[pos];
-                    if (prev == kEmptyKey) prev = atomicCAS(&t.key[pos], kEmptyKey, (unsigned long long)kl);
-                    if (prev == kEmptyKey || prev == kl) {
-                        if (a.want_sum) atomicAdd(&t.sum[pos], (unsigned long long)sv);
-                        atomicAdd(&t.cnt[pos], (unsigned)c);
-                        done = true;
-                    }
-                    pos = pos + 1 == GBR_SLOTS ? 0 : pos + 1;
-                }
-                if (!done && !gbr_global_add(a, kl, sv, (uint64_t)c, fresh)) full = true;
+            if (kl == hot_k) {
+                hot_s += sv;
+                hot_c += (unsigned)c;
+            } else if (c >= 8) {
+                // A large group: its key becomes the warp's hot key.
+                if (lane == leader && hot_c && !gbr_fold_n(a, t, hot_k, hot_s, hot_c, fresh)) full = true;
+                hot_k = kl;
+                hot_s = sv;
+                hot_c = (unsigned)c;
+            } else if (lane == leader && !gbr_fold_n(a, t, kl, sv, (unsigned)c, fresh)) {
+                full = true;
             }
             rem &= ~m;
         }
@@ -194,6 +217,7 @@ __device__ void gbr_fold_range(const GbrArgs& a, const GbrTable& t, const longlo
         const bool valid = j < n;
         one(valid ? __ldcs(&p[j]) : make_longlong2((long long)kEmptyKey, 0), valid);
     }
+    if (lane == 0 && hot_c && !gbr_fold_n(a, t, hot_k, hot_s, hot_c, fresh)) full = true;
 }
 
 __device__ void gbr_clear(const GbrTable& t)
@@ -472,8 +496,7 @@ int groupby16_fill(pyg_ctx* ctx, const void* in, int64_t n, int want_sum, int64_
         const size_t ni = istart.size();
         if ((rc = dalloc(ctx, (void**)&dstart, ni * 12 + 16))) break;
         unsigned* dlen = (unsigned*)(dstart + ni);
-        PYG_CUDA(cudaMemcpyAsync(dstart, istart.data(), ni * 8, cudaMemcpyHostToDevice, ctx->stream));
-        PYG_CUDA(cudaMemcpyAsync(dlen, ilen.data(), ni * 4, cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = stage_h2d(ctx, dstart, istart.data(), ni * 8)) || (rc = stage_h2d(ctx, dlen, ilen.data(), ni * 4))) break;
         unsigned* next = (unsigned*)(ctx->dcounters + 206);
         PYG_CUDA(cudaMemsetAsync(next, 0, 8, ctx->stream));
         a.in = (const longlong2*)(two ? P2 : P1);

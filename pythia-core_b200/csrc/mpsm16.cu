@@ -315,7 +315,7 @@ int mpsm16_agg(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t
         for (int i = 0; i < F - 1; ++i) sp[i] = (long long)splitters[i];
         for (int i = 0; i < C - 1; ++i) sp[F - 1 + i] = (long long)splitters[(size_t)(i + 1) * L - 1];
         if ((rc = dalloc(ctx, (void**)&dsplit, sp.size() * 8 + 8))) break;
-        PYG_CUDA(cudaMemcpyAsync(dsplit, sp.data(), sp.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = stage_h2d(ctx, dsplit, sp.data(), sp.size() * 8))) break;
         const long long* fs = dsplit;
         const long long* cs = two ? dsplit + (F - 1) : dsplit;
         unsigned* flags = (unsigned*)(ctx->dcounters + 208);
@@ -383,8 +383,7 @@ int mpsm16_agg(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t
         PYG_CUDA(cudaMemsetAsync(acc, 0, 32, ctx->stream));
         if (!items.empty()) {
             if ((rc = dalloc(ctx, (void**)&ditems, items.size() * sizeof(Mp16Item)))) break;
-            PYG_CUDA(cudaMemcpyAsync(ditems, items.data(), items.size() * sizeof(Mp16Item), cudaMemcpyHostToDevice,
-                                     ctx->stream));
+            if ((rc = stage_h2d(ctx, ditems, items.data(), items.size() * sizeof(Mp16Item)))) break;
             Mp16Args ja;
             ja.R = two ? R2 : R1;
             ja.S = two ? S2 : S1;

@@ -43,7 +43,7 @@ __host__ __device__ __forceinline__ uint64_t packed_to_sortable(uint64_t k, int 
 // (cdf.cu).  Sizes hash tables when a caller gives no group estimate.
 constexpr int64_t CDF_ESTIMATE_SAMPLE = (int64_t)1 << 18;
 // Largest key sample the MPSM join draws for its learned splitters.
-constexpr int64_t CDF_MPSM_SAMPLE = (int64_t)1 << 18;
+constexpr int64_t CDF_MPSM_SAMPLE = (int64_t)1 << 21;
 int estimate_distinct_keys(pyg_ctx* ctx, const uint8_t* base, int64_t n, int32_t tb, const KeySpec& ks,
                            int64_t* out);
 

@@ -10,6 +10,7 @@
 
 constexpr size_t kPinnedScalarBytes = (size_t)1 << 16;  // scalar read-backs (fixed word offsets)
 constexpr size_t kPinnedStageBytes = (size_t)1 << 21;   // two relations x 2^16 partition counts x 8 B, x2
+constexpr size_t kPinnedUploadBytes = (size_t)1 << 23;  // host arrays staged for device copies (stage_h2d)
 
 struct pyg_ctx {
     int device;
@@ -32,6 +33,9 @@ struct pyg_ctx {
     // freed with the context).
     void* join_arena;
     size_t join_arena_bytes;
+    // Bump cursor into the pinned upload area (after the scalar and stage
+    // areas) used by stage_h2d.
+    size_t up_cursor;
 };
 
 namespace pyg {
@@ -56,6 +60,18 @@ int cuda_status(cudaError_t e, const char* what);
 
 int check_ctx(pyg_ctx* ctx);
 int check_rel(const pyg_rel* r, const char* name);
+
+// Host -> device copy on ctx->stream through the context's pinned upload
+// area: src is copied into pinned memory first, so the asynchronous copy
+// neither blocks on pageable staging nor depends on src afterwards.  The
+// area is used as a bump allocator; when it is full, the stream is
+// synchronised (every earlier copy out of it has then completed) and it
+// starts over.  Copies larger than the area go directly from src
+// (pageable, synchronously staged by the driver).
+int stage_h2d(pyg_ctx* ctx, void* dst, const void* src, size_t bytes);
+// Marks the upload area free; call only right after ctx->stream was
+// synchronised.
+inline void stage_reset(pyg_ctx* ctx) { ctx->up_cursor = 0; }
 
 // Device memory from the stream-ordered pool.
 int dalloc(pyg_ctx* ctx, void** p, size_t bytes);

@@ -390,8 +390,9 @@ namespace {
 
 struct RJEvents {
     // 0 start, 1 histograms, 2 / 3 build / probe passes done, 4 join done,
-    // 5 / 6 build first pass begins / ends, 7 / 8 the same for the probe side.
-    static constexpr int N = 9;
+    // 5 / 6 build first pass begins / ends, 7 / 8 the same for the probe side,
+    // 9 the join kernel begins.
+    static constexpr int N = 10;
     cudaEvent_t ev[N] = {};
     bool on = false;
     void start(pyg_ctx* ctx, bool enable)
@@ -529,8 +530,7 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
             dfree(ctx, ditems);
             ditems = nullptr;
             if ((rc = dalloc(ctx, (void**)&ditems, items.size() * sizeof(RJItem)))) break;
-            PYG_CUDA(cudaMemcpyAsync(ditems, items.data(), items.size() * sizeof(RJItem), cudaMemcpyHostToDevice,
-                                     ctx->stream));
+            if ((rc = stage_h2d(ctx, ditems, items.data(), items.size() * sizeof(RJItem)))) break;
             void* fn = j32 ? (void*)rj_join32_kernel
                            : (unique ? join_fn<true>(LR.packed, LS.packed) : join_fn<false>(LR.packed, LS.packed));
             const int smem = j32 ? RJ32_TABLE_BYTES : RJ_TABLE_BYTES;
@@ -553,6 +553,7 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
             ja.sk = LS.kbase;
             ja.sp = LS.pbase;
             const unsigned grid = (unsigned)std::min<long long>((long long)ctx->sm_count * per_sm, ja.nitems);
+            if (unique) tm.mark(ctx, 9);
             void* args[] = {&ja};
             PYG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, smem, ctx->stream));
             PYG_LAUNCHED(ctx);
@@ -577,6 +578,7 @@ int radix_join16(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64
             stats->build_ms = 0;
             stats->probe_partition_ms = tm.ms(2, 3);
             stats->probe_ms = tm.ms(3, 4);
+            stats->join_kernel_ms = tm.ms(9, 4);
             for (int s = 0; s < 2; ++s) {
                 double* pm = s ? stats->probe_pass_ms : stats->build_pass_ms;
                 pm[0] = pm[1] = 0;

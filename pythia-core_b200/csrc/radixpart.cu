@@ -604,17 +604,18 @@ bool common_key_frame(const long long* mm0, bool exact0, const long long* mm1, b
 
 int upload_layout(pyg_ctx* ctx, const RJLayout& L, const RJSideDev& d, int F, int C, int64_t n)
 {
-    PYG_CUDA(cudaMemcpyAsync(d.fstart, L.fstart.data(), (size_t)(F + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
-    PYG_CUDA(cudaMemcpyAsync(d.cstart, L.cstart.data(), (size_t)(C + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
-    if (L.sampled) PYG_CUDA(cudaMemcpyAsync(d.fcap, L.fcap.data(), (size_t)F * 8, cudaMemcpyHostToDevice, ctx->stream));
-    if (L.sampled || L.packed)
-        PYG_CUDA(cudaMemcpyAsync(d.ccap, L.ccap.data(), (size_t)C * 8, cudaMemcpyHostToDevice, ctx->stream));
-    else
-        PYG_CUDA(cudaMemcpyAsync(d.tiles2, L.tiles2.data(), (size_t)(C + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    int rc;
+    if ((rc = stage_h2d(ctx, d.fstart, L.fstart.data(), (size_t)(F + 1) * 8))) return rc;
+    if ((rc = stage_h2d(ctx, d.cstart, L.cstart.data(), (size_t)(C + 1) * 8))) return rc;
+    if (L.sampled && (rc = stage_h2d(ctx, d.fcap, L.fcap.data(), (size_t)F * 8))) return rc;
+    if (L.sampled || L.packed) {
+        if ((rc = stage_h2d(ctx, d.ccap, L.ccap.data(), (size_t)C * 8))) return rc;
+    } else if ((rc = stage_h2d(ctx, d.tiles2, L.tiles2.data(), (size_t)(C + 1) * 8))) {
+        return rc;
+    }
     PYG_CUDA(cudaMemsetAsync(d.cur1, 0, (size_t)(C + F) * 8, ctx->stream));  // cur1 and cur2 are adjacent
     const unsigned long long w[4] = {0, (unsigned long long)n, 0, (unsigned long long)((n + RJ_TILE - 1) / RJ_TILE)};
-    PYG_CUDA(cudaMemcpyAsync(d.whole, w, sizeof(w), cudaMemcpyHostToDevice, ctx->stream));
-    return PYG_OK;
+    return stage_h2d(ctx, d.whole, w, sizeof(w));
 }
 
 // Runs the partition pass(es) of one relation into P1 (and P2).
@@ -753,7 +754,7 @@ int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsig
     const int F = 1 << FB;
     const size_t side = RJSideDev::words(F, 1 << coarse_bits(false));
     const size_t per = side + F + 4;  // metadata, histogram, {kmin, kmax, pmin, pmax}
-    if (ns < 1 || ns > 2 || (size_t)ns * (F + 4) * 8 > ctx->pinned_bytes - kPinnedScalarBytes) {
+    if (ns < 1 || ns > 2 || (size_t)ns * (F + 4) * 8 > kPinnedStageBytes) {
         set_error("partition: %d relations of 2^%d partitions exceed the staging area", ns, FB);
         return PYG_ERR_ARG;
     }
@@ -823,6 +824,7 @@ int rp_partition_sides(pyg_ctx* ctx, RPSide* sd, int ns, int FB, bool two, unsig
         for (int s = 0; s < ns; ++s)
             PYG_CUDA(cudaMemcpyAsync(hh_at(s), hist_at(s), (size_t)(F + 4) * 8, cudaMemcpyDeviceToHost, ctx->stream));
         PYG_CUDA(cudaStreamSynchronize(ctx->stream));
+        stage_reset(ctx);
         // One key frame for both relations when asked and both ranges fit
         // in it, so that their packed words compare by key offset.
         unsigned long long ckb = 0;

@@ -61,31 +61,31 @@ constexpr int RJ_SAMPLE_LOG2 = PYG_RJ_SAMPLE_LOG2;
 // Partition bins computed by a learned CDF model instead of a search
 // (range partitioning without splitters in the passes).  For a model with
 // L leaves over keys (kmin, kmax) and 2^fbits bins:
-//   x = (float)(((double)k - key_lo) * key_scale)     normalised key
+//   x = (float)(k - kmin) * scale                     normalised key (the
+//                                                     offset as unsigned)
 //   r = a0 x + b0, l = clamp(floor(L r), 0, L - 1)     root line -> leaf
 //   u = clamp(L r - l, 0, 1)                           leaf-local coordinate
-//   t = clamp(slope_l u + icpt_l, 0, 1)
-//   g = min(base_l + span_l t + (heavy keys of leaf l below k), top_l)
+//   g = clamp(A_l u + B_l, lo_l, hi_l)                 the leaf's line
+//   g = min(g + (masses of the leaf's heavy keys below k), hi_l)
 //   bin(k) = min(2^fbits - 1, trunc(g 2^fbits))
 // with bin 0 for k <= kmin and the last bin for k >= kmax.  Every step is a
-// correctly rounded fp32 / fp64 operation that does not decrease when its
-// input grows (slopes, spans and masses are >= 0), and top_l <= base_{l+1},
-// so bin(k) never decreases with k: the bins are key ranges, and their
-// splitters (the first key of each bin, found by bisection over the same
-// function) reproduce them exactly.  The model's accuracy only decides how
-// even the bins are.
+// correctly rounded fp32 operation that does not decrease when its input
+// grows (A_l and the masses are >= 0), and hi_l <= lo_{l+1}, so bin(k)
+// never decreases with k: the bins are key ranges, and their splitters
+// (the first key of each bin, found by bisection over the same function)
+// reproduce them exactly.  The model's accuracy only decides how even the
+// bins are.
 struct RJLeaf {
-    float base, span, slope, icpt;  // g = base + span * t
-    float top;                      // the leaf's largest g
-    int h0, hn;                     // heavy keys of the leaf: hkey[h0 .. h0 + hn)
-    int pad;
+    float A, B;    // the leaf's line over u
+    float lo, hi;  // its range of g
 };
 struct RJModel {
     const RJLeaf* leaf = nullptr;  // device, L leaves (null: no model)
+    const int2* hinfo = nullptr;   // device, per leaf {first heavy key, count}; null without heavy keys
     const long long* hkey = nullptr;  // device, heavy keys ascending
     const float* hw = nullptr;        // device, their masses
-    double key_lo = 0, key_scale = 0;
     long long kmin = 0, kmax = 0;
+    float scale = 0;
     float a0 = 0, b0 = 0;
     int L = 0;
     int fbits = 0;
@@ -96,16 +96,18 @@ __device__ __forceinline__ unsigned rj_model_bin(const RJModel& m, long long k)
     const unsigned last = (1u << m.fbits) - 1u;
     if (k <= m.kmin) return 0u;
     if (k >= m.kmax) return last;
-    const float x = __double2float_rn(__dmul_rn(__dsub_rn((double)k, m.key_lo), m.key_scale));
+    const float x = __fmul_rn(__ull2float_rn((unsigned long long)k - (unsigned long long)m.kmin), m.scale);
     const float lr = __fmul_rn(__fmaf_rn(m.a0, x, m.b0), (float)m.L);
     const float fl = floorf(lr);
-    int l = fl < 0.f ? 0 : (fl > (float)(m.L - 1) ? m.L - 1 : (int)fl);
+    const int l = fl < 0.f ? 0 : (fl > (float)(m.L - 1) ? m.L - 1 : (int)fl);
     const float u = fminf(1.f, fmaxf(0.f, __fsub_rn(lr, (float)l)));
     const RJLeaf p = m.leaf[l];
-    const float t = fminf(1.f, fmaxf(0.f, __fmaf_rn(p.slope, u, p.icpt)));
-    float g = __fmaf_rn(p.span, t, p.base);
-    for (int h = p.h0; h < p.h0 + p.hn && m.hkey[h] < k; ++h) g = __fadd_rn(g, m.hw[h]);
-    g = fminf(g, p.top);
+    float g = fminf(p.hi, fmaxf(p.lo, __fmaf_rn(p.A, u, p.B)));
+    if (m.hinfo) {
+        const int2 hi = m.hinfo[l];
+        for (int h = hi.x; h < hi.x + hi.y && m.hkey[h] < k; ++h) g = __fadd_rn(g, m.hw[h]);
+        g = fminf(g, p.hi);
+    }
     const float b = __fmul_rn(g, (float)(1u << m.fbits));
     return b >= (float)last ? last : (unsigned)b;
 }

@@ -81,7 +81,7 @@ class pyg_join_stats(C.Structure):
                 ("build_ms", C.c_double), ("probe_partition_ms", C.c_double), ("probe_ms", C.c_double), ("overflow_tuples", C.c_int64),
                 ("padded_tuples", C.c_int64), ("histogram_ms", C.c_double), ("histogram_tuples", C.c_int64),
                 ("build_pass_ms", C.c_double * 2), ("probe_pass_ms", C.c_double * 2), ("build_packed", C.c_int32),
-                ("probe_packed", C.c_int32)]
+                ("probe_packed", C.c_int32), ("join_kernel_ms", C.c_double)]
 
 
 class pyg_splitter(C.Structure):

@@ -162,3 +162,25 @@ def test_groupby_full_size_property(ctx, torch_cuda):
     assert int(o[:, 1].sum().item()) == int(S.view(n, 2)[:, 1].sum().item())
     assert bool((o[1:, 0] > o[:-1, 0]).all().item())
     assert int(torch.unique(S.view(n, 2)[:, 0]).numel()) == g
+
+
+@pytest.mark.parametrize("case", ["zipf1.0", "zipf1.5", "alternating"])
+def test_groupby_hot_keys_in_warp_registers(ctx, torch_cuda, case):
+    """Skewed 16-byte tuples through the partitioned shared-memory fold,
+    where each warp keeps its hot key's combined sum and count in registers
+    and folds them when another large group's key takes its place: Zipf ids
+    (theta 1.0 and 1.5), and runs of 64 tuples alternating between two hot
+    keys with a third spread among them, so the hot key changes every few
+    batches.  Values near 2^62 make the int64 sums wrap."""
+    rng = np.random.default_rng(len(case))
+    G, n = 1 << 16, (1 << 22) + 333
+    if case == "alternating":
+        run = (np.arange(n) // 64) % 3
+        gid = np.where(run == 0, 5, np.where(run == 1, 77, rng.integers(0, G, n)))
+        gid[rng.random(n) < 0.2] = 1234
+    else:
+        gid = zipf_ranks(rng, n, G, float(case[4:]))
+    perm = rng.permutation(G).astype(np.int64) * 104729 + (1 << 45)
+    A = struct([perm[gid], rng.integers((1 << 62) - (1 << 40), 1 << 62, n)], [I64, I64])
+    out = run_groupby(ctx, torch_cuda, A, [I64, I64], [0], 3, 1, G)
+    assert rows(out) == rows(O.groupby(A, [I64, I64], [0], 3, 1, buckets=G))
