@@ -14,9 +14,13 @@
  * Fragments whose build side has at least `large_build` tuples are not
  * queued: their tables would not stay in L2 beside the others', and their
  * work dwarfs a call's fixed cost, so after the graph they run one by one
- * through the partitioned join (pyg_hashjoin_agg).  The persistent kernel
- * takes the many small and medium fragments, whose separate calls would be
- * dominated by launches and host synchronisations.
+ * with the algorithm pyg_hashjoin_agg would pick.  Those that take the
+ * direct join are enqueued back to back with no host synchronisation
+ * between them (their counters stay on the device until the run's single
+ * synchronisation; a build side with a repeated key is answered by the
+ * general path after it); the partitioned joins follow.  The persistent
+ * kernel takes the many small and medium fragments, whose separate calls
+ * would be dominated by launches and host synchronisations.
  */
 #ifndef PYG_BATCH_H
 #define PYG_BATCH_H
@@ -45,7 +49,7 @@ typedef struct pyg_tuning {
     float load_factor;           /* per-fragment table load factor           */
     int32_t chunk_tuples;        /* work-item grain in tuples                */
     int32_t large_build;         /* build tuples from which a fragment runs
-                                    as its own partitioned join (0: 2^20) */
+                                    as its own join (0: 2^16)             */
 } pyg_tuning;
 
 /* Plans n fragments (tuning NULL: the autotuner's cached choice, else

@@ -16,6 +16,7 @@
 
 #include "../../include/pyg_batch.h"
 #include "pyg_internal.cuh"
+#include "radixjoin.cuh"
 
 namespace pyg {
 
@@ -263,9 +264,12 @@ struct pyg_batch {
     cudaGraphExec_t exec = nullptr;
     std::vector<int32_t> order;  // fragments with no work item (empty) still report results
     std::vector<char> empty_frag;
-    // Fragments run after the graph as their own partitioned joins.
+    // Fragments run after the graph as their own joins: the direct join,
+    // enqueued without waiting (its counters in 16 device words each of
+    // large_words), or a partitioned join through pyg_hashjoin_agg.
     std::vector<int32_t> large;
     std::vector<pyg_fragment> large_frag;
+    unsigned long long* large_words = nullptr;
 };
 
 namespace pyg {
@@ -294,6 +298,16 @@ static std::string signature(const pyg_fragment* fr, int n)
     std::ostringstream os;
     os << "n" << n << "_b" << (int)(b > 0 ? log2(b) : 0) << "_p" << (int)(p > 0 ? log2(p) : 0);
     return os.str();
+}
+
+// The automatic algorithm's choice for a fragment (pyg_hashjoin_agg): the
+// direct join while its table (16-byte slots at load factor 0.5) fits well
+// inside L2 or the probe side is small, else the partitioned join.
+static bool fragment_direct(const pyg_fragment& f)
+{
+    const double table_bytes = 16.0 * (double)f.nbuild / 0.5;
+    return !(table_bytes > 64.0 * 1024 * 1024 && f.nprobe >= ((int64_t)1 << 22)) && (uintptr_t)f.build % 16 == 0 &&
+           (uintptr_t)f.probe % 16 == 0;
 }
 
 // One fragment through pyg_hashjoin_agg with the automatic algorithm (the
@@ -391,6 +405,13 @@ int pyg_batch_create(pyg_ctx* ctx, const pyg_fragment* frags, int32_t n, const p
             b->large.push_back(i);
             b->large_frag.push_back(frags[i]);
         }
+    if (!b->large.empty()) {
+        int rc = batch_alloc(ctx, b, (void**)&b->large_words, b->large.size() * 16 * sizeof(unsigned long long));
+        if (rc) {
+            pyg_batch_free(ctx, b);
+            return rc;
+        }
+    }
     // Tables: one arena of 16-byte slots and one of extra-copy counters,
     // per-fragment capacity nbuild / load factor (queued fragments only).
     std::vector<FragDesc> fd(n);
@@ -507,11 +528,35 @@ int pyg_batch_run(pyg_ctx* ctx, pyg_batch* b, int64_t* counts, int64_t* sums, do
     std::vector<unsigned char> st(b->state_bytes);
     PYG_CUDA(cudaMemcpyAsync(st.data(), b->state, b->state_bytes, cudaMemcpyDeviceToHost, ctx->stream));
     std::vector<int64_t> lc(nl), ls(nl);
-    for (size_t j = 0; j < nl && !rc; ++j) {
-        rc = join_fragment(ctx, b->large_frag[j], &lc[j], &ls[j]);
-        cudaEventRecord(ev[j + 1], ctx->stream);
-    }
+    // Direct joins first, one after another on the stream with no wait
+    // between them; the partitioned joins after them.
+    std::vector<char> direct(nl, 0);
+    for (size_t j = 0; j < nl; ++j) direct[j] = fragment_direct(b->large_frag[j]) ? 1 : 0;
+    for (int pass = 0; pass < 2 && !rc; ++pass)
+        for (size_t j = 0; j < nl && !rc; ++j) {
+            if (direct[j] != (pass == 0)) continue;
+            const pyg_fragment& f = b->large_frag[j];
+            if (direct[j]) rc = direct_join16_enqueue(ctx, f.build, f.nbuild, f.probe, f.nprobe, 0.5f,
+                                                      b->large_words + 16 * j);
+            else rc = join_fragment(ctx, f, &lc[j], &ls[j]);
+            cudaEventRecord(ev[j + 1], ctx->stream);
+        }
+    std::vector<unsigned long long> lw(nl * 16);
+    if (nl && !rc)
+        PYG_CUDA(cudaMemcpyAsync(lw.data(), b->large_words, lw.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    // A direct join whose build repeated a key stood down: the general
+    // path answers for it now.
+    for (size_t j = 0; j < nl && !rc && e == cudaSuccess; ++j) {
+        if (!direct[j]) continue;
+        unsigned long long r3[3];
+        if (direct_join16_result(lw.data() + 16 * j, b->large_frag[j].nbuild, r3)) {
+            lc[j] = (int64_t)r3[0];
+            ls[j] = (int64_t)(r3[1] + r3[2]);
+        } else {
+            rc = join_fragment(ctx, b->large_frag[j], &lc[j], &ls[j]);
+        }
+    }
     std::vector<float> lat_large(nl, 0.f);
     for (size_t j = 0; j < nl && !rc && e == cudaSuccess; ++j) cudaEventElapsedTime(&lat_large[j], ev[0], ev[j + 1]);
     for (auto& x : ev) cudaEventDestroy(x);

@@ -770,6 +770,62 @@ __global__ void __launch_bounds__(DJ_THREADS) dj_probe_kernel(const longlong2* _
     block_flush(acc, 3, out);
 }
 
+// Side-list capacity of the direct join (build keys equal to kEmptyKey).
+static int64_t direct_side_cap(int64_t nR) { return nR < 1024 ? (nR > 0 ? nR : 1) : 1024; }
+
+int direct_join16_enqueue(pyg_ctx* ctx, const void* Rv, int64_t nR, const void* Sv, int64_t nS, float lf,
+                          unsigned long long* words, PhaseTimer* tm)
+{
+    const longlong2* R = (const longlong2*)Rv;
+    const longlong2* S = (const longlong2*)Sv;
+    // 2^bits slots, more than nR / lf (so at least one slot stays free).
+    int bits = 6;
+    while (bits < 62 && (double)((uint64_t)1 << bits) * (double)lf <= (double)nR) ++bits;
+    const uint64_t cap = (uint64_t)1 << bits;
+    const int64_t side_cap = direct_side_cap(nR);
+    const size_t need = (size_t)cap * 16 + (size_t)side_cap * 16;
+    if (ctx->join_arena_bytes < need) {
+        // Stream-ordered: earlier joins on the stream finish with the old
+        // arena before its memory is reused.
+        dfree(ctx, ctx->join_arena);
+        ctx->join_arena = nullptr;
+        ctx->join_arena_bytes = 0;
+        int rc = dalloc(ctx, &ctx->join_arena, need);
+        if (rc) return rc;
+        ctx->join_arena_bytes = need;
+    }
+    ulonglong2* slots = (ulonglong2*)ctx->join_arena;
+    uint64_t* side = (uint64_t*)(slots + cap);
+    dj_clear_kernel<<<grid_for(ctx, (int64_t)cap, 256, 4, 8), 256, 0, ctx->stream>>>(slots, cap, words, 11);
+    PYG_LAUNCHED(ctx);
+    if (tm) tm->mark(ctx, 1);
+    if (nR > 0) {
+        dj_build_kernel<<<grid_for(ctx, nR, DJ_THREADS, DJ_U, 8), DJ_THREADS, 0, ctx->stream>>>(
+            R, nR, slots, cap - 1, 64 - bits, side, side_cap, words);
+        PYG_LAUNCHED(ctx);
+    }
+    if (tm) {
+        tm->mark(ctx, 2);
+        tm->mark(ctx, 3);
+    }
+    if (nS > 0) {
+        dj_probe_kernel<<<grid_for(ctx, nS, DJ_THREADS, DJ_U, 8), DJ_THREADS, 0, ctx->stream>>>(
+            S, nS, slots, cap - 1, 64 - bits, side, side_cap, words, words + 8);
+        PYG_LAUNCHED(ctx);
+    }
+    if (tm) tm->mark(ctx, 4);
+    return PYG_OK;
+}
+
+bool direct_join16_result(const unsigned long long* w, int64_t nR, unsigned long long res[3])
+{
+    if (w[0] || w[1] || w[2] > (unsigned long long)direct_side_cap(nR)) return false;
+    res[0] = w[8];
+    res[1] = w[9];
+    res[2] = w[10];
+    return true;
+}
+
 // One-shot join + sum of 16-byte (int64 key @0, int64 payload @8) device
 // relations through one table in HBM (L2-resident for build sides up to a
 // few million tuples): clear, build, probe as three launches, one copy of
@@ -783,50 +839,13 @@ __global__ void __launch_bounds__(DJ_THREADS) dj_probe_kernel(const longlong2* _
 static int direct_join16(pyg_ctx* ctx, const longlong2* R, int64_t nR, const longlong2* S, int64_t nS, float lf,
                          unsigned long long res[3], bool* fallback, PhaseTimer* tm)
 {
-    *fallback = false;
-    // 2^bits slots, more than nR / lf (so at least one slot stays free).
-    int bits = 6;
-    while (bits < 62 && (double)((uint64_t)1 << bits) * (double)lf <= (double)nR) ++bits;
-    const uint64_t cap = (uint64_t)1 << bits;
-    const int64_t side_cap = nR < 1024 ? (nR > 0 ? nR : 1) : 1024;
-    const size_t need = (size_t)cap * 16 + (size_t)side_cap * 16;
-    if (ctx->join_arena_bytes < need) {
-        dfree(ctx, ctx->join_arena);
-        ctx->join_arena = nullptr;
-        ctx->join_arena_bytes = 0;
-        int rc = dalloc(ctx, &ctx->join_arena, need);
-        if (rc) return rc;
-        ctx->join_arena_bytes = need;
-    }
-    ulonglong2* slots = (ulonglong2*)ctx->join_arena;
-    uint64_t* side = (uint64_t*)(slots + cap);
     unsigned long long* words = ctx->dcounters;  // [0..2] build flags, [8..10] probe sums
-    dj_clear_kernel<<<grid_for(ctx, (int64_t)cap, 256, 4, 8), 256, 0, ctx->stream>>>(slots, cap, words, 11);
-    PYG_LAUNCHED(ctx);
-    tm->mark(ctx, 1);
-    if (nR > 0) {
-        dj_build_kernel<<<grid_for(ctx, nR, DJ_THREADS, DJ_U, 8), DJ_THREADS, 0, ctx->stream>>>(
-            R, nR, slots, cap - 1, 64 - bits, side, side_cap, words);
-        PYG_LAUNCHED(ctx);
-    }
-    tm->mark(ctx, 2);
-    tm->mark(ctx, 3);
-    if (nS > 0) {
-        dj_probe_kernel<<<grid_for(ctx, nS, DJ_THREADS, DJ_U, 8), DJ_THREADS, 0, ctx->stream>>>(
-            S, nS, slots, cap - 1, 64 - bits, side, side_cap, words, words + 8);
-        PYG_LAUNCHED(ctx);
-    }
-    tm->mark(ctx, 4);
+    int rc = direct_join16_enqueue(ctx, R, nR, S, nS, lf, words, tm);
+    if (rc) return rc;
     unsigned long long* h = (unsigned long long*)ctx->pinned;
     PYG_CUDA(cudaMemcpyAsync(h, words, 11 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
     PYG_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (h[0] || h[1] || h[2] > (unsigned long long)side_cap) {
-        *fallback = true;
-        return PYG_OK;
-    }
-    res[0] = h[8];
-    res[1] = h[9];
-    res[2] = h[10];
+    *fallback = !direct_join16_result(h, nR, res);
     return PYG_OK;
 }
 

@@ -17,7 +17,7 @@ device.  Cases and the kernels they launch:
   composite  2^25 (int32, int32, int64), G = 2^16    groupby_kernel
   partition  2^25 tuples, exactrange, fan-out 64     pt_hist, pt_scatter
   sort       2^24 tuples                            rs_hist, rs_scatter
-  mpsm       R 2^22 x S 2^24, sampled splitters     mp16 path (aggregate sink)
+  mpsm       R 2^22 x S 2^24, sampled or learned splitters   mp16 path (aggregate sink)
   mpsm-mat   R 2^20 x S 2^22, materialised          mp_tile_sort, mp_merge, mp_join
   cdf        2^21-key sample, 1024 leaves           cdf training kernels
   batch      64 fragments, builds 2^12..2^18        batch_kernel
@@ -123,7 +123,8 @@ def case_mpsm(torch, ctx, a, materialize):
     nR, nS = nR >> a.shift, nS >> a.shift
     R, S = pkfk(torch, ctx, nR, nS, a.theta)
     Rr, Sr = pyg.Rel(R, nR, [I64, I64]), pyg.Rel(S, nS, [I64, I64])
-    opts = ctx.mpsm_opts(pyg.MPSM_SAMPLED, 1024, 0.01, 1024)
+    kind = pyg.MPSM_LEARNED if a.splitter == "learned" else pyg.MPSM_SAMPLED
+    opts = ctx.mpsm_opts(kind, 1024, 0.01, 1024)
     if materialize:
         out = torch.empty(nS * 2, dtype=torch.int64, device="cuda")
         for _ in range(a.reps):
@@ -176,6 +177,8 @@ def main():
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--theta", type=float, default=0.0)
     ap.add_argument("--bits", type=int, default=0, help="radix: log2 partition fan-out (0 = automatic)")
+    ap.add_argument("--splitter", default="sampled", choices=["sampled", "learned"],
+                    help="mpsm: range splitters (learned: the model's own bins)")
     a = ap.parse_args()
     import torch
 
