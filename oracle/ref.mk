@@ -69,10 +69,12 @@ BZ_OBJS := $(addprefix $(OBJ)/bz/,$(addsuffix .o,$(BZ_SRCS)))
 
 all: $(OUT)/executequery $(OUT)/executemultiplequery
 
-$(OUT)/include/libconfig.h++ $(OUT)/include/libconfig.h $(OUT)/include/bzlib.h:
+# One recipe run makes all three headers (grouped target): with plain
+# targets a parallel make ran the copy once per header and the runs raced.
+$(OUT)/include/libconfig.h++ $(OUT)/include/libconfig.h $(OUT)/include/bzlib.h &:
 	mkdir -p $(OUT)/include
-	cp $(LIBCONFIG)/libconfig.h $(LIBCONFIG)/libconfig.h++ $(OUT)/include/
-	cp $(BZIP2)/bzlib.h $(OUT)/include/
+	cp -f $(LIBCONFIG)/libconfig.h $(LIBCONFIG)/libconfig.h++ $(OUT)/include/
+	cp -f $(BZIP2)/bzlib.h $(OUT)/include/
 
 HDRS := $(OUT)/include/libconfig.h++ $(OUT)/include/libconfig.h $(OUT)/include/bzlib.h
 
