@@ -59,9 +59,11 @@ def parse():
                          "independent replicas")
     ap.add_argument("--no-secondary", action="store_true",
                     help="join: skip the other configurations measured after the headline")
-    ap.add_argument("--workload", default="join", choices=["join", "join-small", "groupby", "mpsm", "batch"],
-                    help="join: the headline configuration (default); the others measure the small join, "
-                         "group-by, MPSM sort-merge join and batched-fragment configurations")
+    ap.add_argument("--workload", default="join", choices=["join", "join-radix", "join-small", "groupby", "mpsm",
+                                                          "batch"],
+                    help="join: the headline configuration (default); join-radix: the same join at --theta as a "
+                         "secondary line; the others measure the small join, group-by, MPSM sort-merge join and "
+                         "batched-fragment configurations")
     ap.add_argument("--groups", type=int, default=1 << 16, help="groupby: group cardinality G")
     ap.add_argument("--zipf", action="store_true", help="groupby: Zipf(1.0) group ids instead of uniform")
     ap.add_argument("--splitter", default="learned", choices=["learned", "sampled", "exactrange"],
@@ -99,8 +101,7 @@ class Clocks:
         except Exception:
             return None
 
-    def _run(self):
-        nv = self._handle()
+    def _run(self, nv):
         while not self._stop.is_set():
             try:
                 if nv:
@@ -121,7 +122,12 @@ class Clocks:
             self._stop.wait(0.02 if nv else 0.2)
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
+        # NVML is imported and opened here, before the caller's timed region
+        # starts: an import on the sampling thread holds the interpreter
+        # lock in the middle of the timed steps (measured: 3.5 ms per step of
+        # idle GPU over 20 steps of the headline join).
+        nv = self._handle()
+        self._t = threading.Thread(target=self._run, args=(nv,), daemon=True)
         self._t.start()
         return self
 
@@ -676,6 +682,31 @@ def workload_line(args, torch, pyg, ctx, rank, world, local, dist, stream):
             if r:
                 cpu = {"value": units * len(r[1]) / sum(r[1]), "unit": UNIT, "cores": r[0], "kind": "reference",
                        "sample": f"the whole workload, executequery ResponseTimeInSec, {r[0]} threads"}
+    elif args.workload == "join-radix":
+        # The headline radix join (R 2^27 PK, S 2^30 FK, count + checksum)
+        # with the fks Zipf(theta) over R's keys: the configuration's other
+        # skews.  Checked like the headline: count == |S| and checksum ==
+        # sum(7 fk + val).
+        nR, nS = N_BUILD >> sh, N_PROBE >> sh
+        R = torch.empty(nR * 2, dtype=torch.int64, device="cuda")
+        S = torch.empty(nS * 2, dtype=torch.int64, device="cuda")
+        ctx.gen_pk(R, nR, 7, SEED_KEYS)
+        ctx.gen_fk(S, nS, nR, args.theta, SEED_KEYS, VMAX, SEED_PROBE + rank)
+        Rr, Sr = pyg.Rel(R, nR, [I64, I64]), pyg.Rel(S, nS, [I64, I64])
+
+        def fn():
+            cnt, sums = ctx.hashjoin_agg(Rr, [0], Sr, [0], [(0, 1), (1, 1)], pyg.JOIN_RADIX, args.radix_bits,
+                                         args.load_factor)
+            return cnt, (sums[0] + sums[1]) & 0xFFFFFFFFFFFFFFFF
+
+        cnt, chk = fn()
+        Sv = S.view(nS, 2)
+        expect = int((Sv[:, 0] * 7 + Sv[:, 1]).sum().item()) & 0xFFFFFFFFFFFFFFFF
+        assert cnt == nS and chk == expect, (cnt, chk, expect)
+        units, abytes = nR + nS, (nR + nS) * 16
+        metric = METRIC
+        workload = {"workload": "radix-scale PK-FK hash join + count + checksum", "build_tuples": nR,
+                    "probe_tuples": nS, "theta": args.theta, "l2": "inputs larger than L2; no flush needed"}
     elif args.workload == "groupby":
         # N = 2^28 (int64 group id, int64 value); ids ~ U[0, G) or Zipf(1.0); sum and count per group, sorted.
         N, G = (1 << 28) >> sh, args.groups
@@ -814,10 +845,13 @@ def workload_line(args, torch, pyg, ctx, rank, world, local, dist, stream):
 
 
 # Configurations measured beside the headline in the default run, with the
-# bench options that select each: the small join, group-by at three
+# bench options that select each: the headline join at the other two fk
+# skews, the small join, group-by at three
 # cardinalities, the MPSM join with both splitters on skewed keys, and the
 # batched fragments.
 SECONDARY = [
+    ("join_theta0.75", dict(workload="join-radix", theta=0.75)),
+    ("join_theta1.25", dict(workload="join-radix", theta=1.25)),
     ("join_small", dict(workload="join-small")),
     ("groupby_G16", dict(workload="groupby", groups=16)),
     ("groupby_G2p16", dict(workload="groupby", groups=1 << 16)),
