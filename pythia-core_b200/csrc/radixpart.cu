@@ -183,7 +183,6 @@ struct RJFmt {
     using Out = typename std::conditional<OUT8, unsigned long long, longlong2>::type;
     using Bin = typename std::conditional<IN8, unsigned char, unsigned short>::type;
     static constexpr int TILE = IN8 ? RJ_TILE8 : RJ_TILE;
-    static constexpr int THREADS = IN8 ? RJ_PT_THREADS8 : RJ_PT_THREADS16;
 };
 
 __device__ __forceinline__ long long rj_key(const longlong2& t, unsigned long long) { return t.x; }
@@ -323,15 +322,26 @@ __device__ __forceinline__ void rj_issue_tile(const RJPass& a, RJPartSmem<IN8, O
 // per-tuple branch chooses it.
 enum RJMode { RJ_MODE_HASH = 0, RJ_MODE_MODEL = 1, RJ_MODE_RANGE = 2 };
 
+// Threads of a partition CTA: 256 for hash bins of 16-byte tuples, 512
+// otherwise.  The learned model's bins and splitter searches wait on loads
+// (the key's leaf, the splitters) and measured faster with the larger CTA:
+// MPSM partition phase at theta 1.0, 8.05 against 7.18 ms (model) and 10.59
+// against 10.14 ms (sampled splitters) with 256 threads.
+template <bool IN8, int MODE>
+constexpr int rj_pt_threads()
+{
+    return (IN8 || MODE != RJ_MODE_HASH) ? RJ_PT_THREADS8 : RJ_PT_THREADS16;
+}
+
 template <bool IN8, bool OUT8, int MODE>
-__global__ void __launch_bounds__(RJFmt<IN8, OUT8>::THREADS, PYG_RJ_PT_MINB) rj_partition_kernel(RJPass a, long long ntiles)
+__global__ void __launch_bounds__(rj_pt_threads<IN8, MODE>(), PYG_RJ_PT_MINB) rj_partition_kernel(RJPass a, long long ntiles)
 {
     using F = RJFmt<IN8, OUT8>;
     using Out = typename F::Out;
     if (a.ntiles_dev) ntiles = (long long)*a.ntiles_dev;
     extern __shared__ __align__(128) unsigned char rj_pt_raw[];
     RJPartSmem<IN8, OUT8>& sm = *reinterpret_cast<RJPartSmem<IN8, OUT8>*>(rj_pt_raw);
-    constexpr int T = F::THREADS;
+    constexpr int T = rj_pt_threads<IN8, MODE>();
     constexpr int PER = F::TILE / T;
     const int L = 1 << a.lbits;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -381,9 +391,10 @@ __global__ void __launch_bounds__(RJFmt<IN8, OUT8>::THREADS, PYG_RJ_PT_MINB) rj_
                     miss |= ((dk | dp) >> 32) != 0;
                     t[j] = (dk & 0xFFFFFFFFULL) | (dp << 32);
                 }
-                // 16-byte passes choose hash or range bins at run time: with
-                // the choice fixed at compile time the first pass of the
-                // 2^30-tuple probe side measured 7.51 against 6.95 ms.
+                // 16-byte passes test nsplit at run time, the hash instance
+                // too (it never has splitters): compiled without the test,
+                // the first pass of the 2^30-tuple probe side measured 7.51
+                // against 6.95 ms.
                 if constexpr (MODE == RJ_MODE_MODEL)
                     bin[j] = rj_bin(rj_model_code(a.model, key), a.shift, a.mask);
                 else if constexpr (!IN8)
@@ -565,7 +576,7 @@ int launch_pass_t(pyg_ctx* ctx, const RJPass& p, long long ntiles)
     const size_t smem = sizeof(RJPartSmem<IN8, OUT8>);
     PYG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    constexpr int T = RJFmt<IN8, OUT8>::THREADS;
+    constexpr int T = rj_pt_threads<IN8, MODE>();
     PYG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, smem));
     if (per_sm < 1) per_sm = 1;
     long long grid = std::min<long long>(ntiles, (long long)ctx->sm_count * per_sm);
@@ -579,12 +590,9 @@ int launch_pass_t(pyg_ctx* ctx, const RJPass& p, long long ntiles)
 template <int MODE>
 int launch_pass_m(pyg_ctx* ctx, const RJPass& p, long long ntiles, bool in8, bool out8)
 {
-    // 16-byte passes have one instance for hash and range bins (the kernel
-    // tests nsplit at run time).
-    constexpr int M16 = MODE == RJ_MODE_MODEL ? RJ_MODE_MODEL : RJ_MODE_HASH;
     if (in8) return launch_pass_t<true, true, MODE>(ctx, p, ntiles);
-    if (out8) return launch_pass_t<false, true, M16>(ctx, p, ntiles);
-    return launch_pass_t<false, false, M16>(ctx, p, ntiles);
+    if (out8) return launch_pass_t<false, true, MODE>(ctx, p, ntiles);
+    return launch_pass_t<false, false, MODE>(ctx, p, ntiles);
 }
 
 int launch_pass(pyg_ctx* ctx, const RJPass& p, long long ntiles, bool in8, bool out8)
